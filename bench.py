@@ -1,0 +1,367 @@
+#!/usr/bin/env python
+"""Benchmark of the PHG assembly + Jacobi-PCG hot path on B200.
+
+Workload (one "step"): P2 Poisson on the unit cube split into 64^3 subcubes
+x 6 Kuhn tetrahedra (1,572,864 elements, 129^3 = 2,146,689 DOFs), kappa = 1,
+f = 3 pi^2 sin(pi x) sin(pi y) sin(pi z), homogeneous Dirichlet BC on all
+faces; element assembly into CSR (order-2 stiffness rule, order-4 RHS rule),
+boundary elimination, then Jacobi-PCG from x = 0 to relative residual 1e-8.
+Inputs are synthetic (generated here), not a dataset.
+
+Metric: time to tolerance of one step in ms (lower is better).
+  value  inputs already resident in HBM (mesh, element->DOF map, Dirichlet
+         flags, f): SetMesh + SetDofMap + BuildLinearSystem + SolverPCG.
+  e2e    the same calls with HOST (pinned) input buffers: the host->device
+         copies of the inputs and the device->host copy of the solution are
+         inside the timed region.
+The dominant kernel is the CSR SpMV inside PCG; its roofline is reported
+against the measured HBM copy bandwidth.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With --gpus N > 1 (launched by torch.distributed.run, one process per GPU)
+every rank solves its own copy of the problem (replicas: the path runs on
+one GPU), value = max over ranks of the step time.  --impl reference times
+the reference's own CPU build (oracle/_ref/phg_dump_omp, all host threads)
+on the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "P2 Poisson assembly+PCG time to 1e-8 rel. resid (64^3 Kuhn cube, 2.15M DOF), 1 B200"
+REF_DUMP_OMP = os.path.join(ROOT, "oracle", "_ref", "phg_dump_omp")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--m", type=int, default=64, help=argparse.SUPPRESS)
+    ap.add_argument("--no-cpu-baseline", action="store_true", help=argparse.SUPPRESS)
+    return ap.parse_args()
+
+
+def workload(m):
+    return {"workload": "P2 Poisson, %d^3 subcubes x 6 Kuhn tets, kappa=1, sine RHS, "
+                        "Dirichlet 0, Jacobi-PCG to rtol 1e-8 (btol=atol=0) from x=0" % m,
+            "elements": 6 * m ** 3, "dofs": (2 * m + 1) ** 3, "order": 2, "rtol": 1e-8,
+            "l2_flush": "inputs and CSR exceed the 126 MB L2"}
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[3:7]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(path))["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def committed_traffic(kernel_key):
+    """dram bytes per launch of the dominant kernel from the committed ncu
+    summary (profiles/traffic.json), or None."""
+    try:
+        return json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))[kernel_key]
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+# ---------------------------------------------------------------------------
+def write_mesh(m, path):
+    from phg_b200.mesh import kuhn_cube, write_medit
+    v, e = kuhn_cube(m)
+    write_medit(path, v, e)
+
+
+def run_reference(args, m, reps, sample_maxit):
+    """Runs the reference's OpenMP build on the workload; returns the JSON
+    lines of its repetitions (rep 0 runs to tolerance, later reps stop
+    after `sample_maxit` PCG iterations)."""
+    if not os.path.exists(REF_DUMP_OMP):
+        raise RuntimeError("reference build missing (oracle/_ref/phg_dump_omp)")
+    with tempfile.TemporaryDirectory() as d:
+        mesh = os.path.join(d, "cube.mesh")
+        write_mesh(m, mesh)
+        env = dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count()), OMP_PROC_BIND="false")
+        cmd = [REF_DUMP_OMP, "-mesh_file", mesh, "-dof_type", "P2", "-solver", "pcg",
+               "-pcg_pc_type", "jacobi", "-solver_rtol", "1e-8", "-solver_btol", "0",
+               "-solver_atol", "0", "-solver_maxit", "100000", "-map_reorder", "no",
+               "-repeat", str(reps), "-sample_maxit", str(sample_maxit)]
+        out = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=3600, check=True)
+    return [json.loads(l) for l in out.stdout.splitlines() if l.startswith("{")]
+
+
+def reference_step_ms(rec, nits_full):
+    """Stage times of one repetition; a capped solve is scaled to the full
+    iteration count."""
+    solve = rec["t_solve"] * (nits_full / max(rec["nits"], 1))
+    return 1e3 * (rec["t_build"] + rec["t_assemble"] + solve)
+
+
+def impl_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    m = args.m
+    sample = 20
+    recs = run_reference(args, m, max(args.warmup, 1) + args.steps, sample)
+    nits_full = recs[0]["nits"]
+    timed = recs[-args.steps:]
+    vals = [reference_step_ms(r, nits_full) for r in timed]
+    v = statistics.mean(vals)
+    threads = recs[0]["threads"]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "ms",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(v, 3), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload(m),
+        "cpu_baseline": {"value": round(v, 3), "unit": "ms", "cores": threads, "kind": "reference",
+                         "sample": "reference OpenMP build (oracle/_ref/phg_dump_omp), full element "
+                                   "loop + phgSolverAssemble each step; PCG capped at %d iterations "
+                                   "per timed step and scaled to the %d iterations of its own "
+                                   "full solve (rep 0)" % (sample, nits_full)},
+        "e2e": {"value": round(v, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_nits": nits_full,
+        "reference_full_solve_ms": round(1e3 * (recs[0]["t_build"] + recs[0]["t_assemble"] +
+                                                recs[0]["t_solve"]), 1),
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+def impl_ours(args):
+    import torch
+    import phg_b200 as pb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    m, p = args.m, 2
+    v, e = pb.kuhn_cube(m)
+    e2l, bdry, nodes = pb.lagrange_dofs(v, e, p)
+    f = pb.sine_source(nodes)
+    ndof = len(bdry)
+    host = {"verts": v, "elems": e, "e2l": e2l, "bdry": bdry, "f": f}
+    pinned = {k: torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for k, a in host.items()}
+    d = {k: t.to(dev) for k, t in pinned.items()}
+    x_dev = torch.zeros(ndof, dtype=torch.float64, device=dev)
+    x_host = torch.zeros(ndof, dtype=torch.float64).pin_memory()
+    rtol = 1e-8
+
+    stream = torch.cuda.Stream(dev)
+    s = pb.Solver(local, stream.cuda_stream)
+
+    def step(inp, x):
+        s.set_mesh(inp["verts"], inp["elems"])
+        s.set_dof_map(p, inp["e2l"], inp["bdry"])
+        s.build_linear_system(f=inp["f"])
+        x.zero_()
+        _, nits, res = s.solve_pcg(out=x, rtol=rtol, btol=0.0, atol=0.0)
+        return nits, res
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(val):
+        if dist is None:
+            return val
+        t = torch.tensor([val], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(inp, x, k):
+        barrier()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = s.launch_count()
+        with torch.cuda.stream(stream):
+            a.record(stream)
+            for _ in range(k):
+                out = step(inp, x)
+            b.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        return a.elapsed_time(b) / k, out, s.launch_count() - l0
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step(d, x_dev)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms, (nits, res), launches = timed(d, x_dev, args.steps)
+    clock_info = clocks.stop()
+    ms = max_over_ranks(ms)
+
+    # end to end through the C ABI with host buffers
+    with torch.cuda.stream(stream):
+        step(pinned, x_host)
+    e2e_ms, _, _ = timed(pinned, x_host, max(1, args.steps))
+    e2e_ms = max_over_ranks(e2e_ms)
+    h2d = sum(t.numel() * t.element_size() for t in pinned.values())
+    d2h = x_host.numel() * x_host.element_size()
+
+    # accuracy of the solution against the exact sine solution (discretisation)
+    u = np.sin(np.pi * nodes[:, 0]) * np.sin(np.pi * nodes[:, 1]) * np.sin(np.pi * nodes[:, 2])
+    err = float(np.max(np.abs(x_dev.cpu().numpy() - u)))
+
+    # phase breakdown of one step
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    with torch.cuda.stream(stream):
+        ev[0].record(stream)
+        s.set_mesh(d["verts"], d["elems"])
+        ev[1].record(stream)
+        s.set_dof_map(p, d["e2l"], d["bdry"])
+        ev[2].record(stream)
+        s.build_linear_system(f=d["f"])
+        ev[3].record(stream)
+        x_dev.zero_()
+        s.solve_pcg(out=x_dev, rtol=rtol, btol=0.0, atol=0.0)
+        ev[4].record(stream)
+    torch.cuda.synchronize()
+    phases = [ev[i].elapsed_time(ev[i + 1]) for i in range(4)]
+    n, nnz, _ = s.sizes()
+
+    # dominant kernel: the CSR SpMV, timed alone on the launching stream
+    xs = torch.randn(n, dtype=torch.float64, device=dev)
+    ys = torch.empty_like(xs)
+    reps = 50
+    with torch.cuda.stream(stream):
+        for _ in range(5):
+            s.mat_vec(xs, ys)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            s.mat_vec(xs, ys)
+        b.record(stream)
+    torch.cuda.synchronize()
+    spmv_ms = a.elapsed_time(b) / reps
+    spmv_bytes = 12 * nnz + 4 * (n + 1) + 16 * n
+    peak, peak_kind = measured_hbm_peak()
+    achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9
+    # per PCG iteration: SpMV + 88 bytes/row of vector traffic
+    it_bytes = spmv_bytes + 88 * n
+    solve_ms = phases[3]
+
+    line = {
+        "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": dict(workload(m), parallelism="replicas x%d" % world,
+                                            path="fp64"),
+        "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "hbm", "kernel": "spmv_kernel (CSR, fp64)", "achieved": round(achieved, 1),
+                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": committed_traffic("spmv_p2_m64_fp64"),
+                     "algorithmic_bytes": int(spmv_bytes), "launch_ms": round(spmv_ms, 5)},
+        "gpu_launches": int(launches),
+        "clocks": clock_info,
+        "pcg": {"nits": int(nits), "residual": res, "max_err_vs_exact": err,
+                "ms_per_iteration": round(solve_ms / max(nits, 1), 4),
+                "iteration_gbs": round(it_bytes * nits / (solve_ms * 1e-3) / 1e9, 1)},
+        "phases_ms": {"set_mesh": round(phases[0], 3), "set_dof_map": round(phases[1], 3),
+                      "assemble": round(phases[2], 3), "pcg": round(phases[3], 3)},
+        "assembly_melem_s": round(6 * m ** 3 / (phases[2] * 1e-3) / 1e6, 1),
+        "n": int(n), "nnz": int(nnz),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            recs = run_reference(args, m, 1, 0)
+            r0 = recs[0]
+            line["cpu_baseline"] = {
+                "value": round(reference_step_ms(r0, r0["nits"]), 1), "unit": "ms",
+                "cores": r0["threads"], "kind": "reference",
+                "sample": "the full workload once: reference OpenMP build (oracle/_ref/phg_dump_omp), "
+                          "element loop + phgSolverAssemble + PCG (%d its)" % r0["nits"]}
+        except Exception as ex:  # report, never fail the GPU measurement
+            line["cpu_baseline"] = {"value": None, "unit": "ms", "cores": os.cpu_count(),
+                                    "kind": "reference", "sample": "failed: %s" % ex}
+    s.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        impl_reference(args)
+    else:
+        impl_ours(args)
+
+
+if __name__ == "__main__":
+    main()

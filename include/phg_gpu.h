@@ -1,0 +1,133 @@
+/*
+ * phg_gpu.h -- C ABI of the B200 (sm_100a) element-assembly + Jacobi-PCG
+ * path for PHG (Parallel Hierarchical Grid) tetrahedral Lagrange P1/P2/P3
+ * finite elements.
+ *
+ * The library stands in for the reference's element loop and linear-solver
+ * calls.  PHG keeps the mesh, refinement and DOF numbering on the host; the
+ * host hands the arrays PHG already holds to this ABI:
+ *
+ *   GRID  g->verts (FLOAT[nvert][3]), e->verts (INT[4] per element)
+ *   DOF   the vector index of every element basis function
+ *         (phgSolverMapE2L, include/phg/solver.h:297), the Dirichlet flag of
+ *         every DOF (what phgDofDirichletBC returns), f_h->data, and the
+ *         per-element coefficient (DOF_P0 data)
+ *
+ * and gets back the same CSR matrix, right-hand side and PCG solution the
+ * reference computes.  Types follow the reference's default build:
+ * FLOAT = double, INT = int (include/phg.h:88,97).
+ *
+ * Pointer arguments may be host or device memory (the library asks the CUDA
+ * runtime which); device pointers must be on the system's device.  All
+ * functions return PHG_GPU_OK (0) or a negative PHG_GPU_ERR_* code, and
+ * phgGpuLastError() describes the last failure of the calling thread.  One
+ * system is used from one host thread at a time; its work is issued in
+ * order on its stream.
+ */
+#ifndef PHG_GPU_H
+#define PHG_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PHG_GPU_OK		0
+#define PHG_GPU_ERR_ARG		(-1)	/* invalid argument / index */
+#define PHG_GPU_ERR_CUDA	(-2)	/* CUDA runtime error */
+#define PHG_GPU_ERR_STATE	(-3)	/* call out of order */
+#define PHG_GPU_ERR_LIMIT	(-4)	/* size beyond a documented limit */
+#define PHG_GPU_ERR_BREAKDOWN	(-5)	/* PCG breakdown: matrix not SPD */
+#define PHG_GPU_ERR_NAN		(-6)	/* non-finite value in the iteration */
+
+typedef struct phgGpuSystem_ phgGpuSystem;
+
+/* Text of the calling thread's last error ("" if none). */
+const char *phgGpuLastError(void);
+/* Library version, major * 10000 + minor * 100 + patch. */
+int phgGpuVersion(void);
+
+/* Creates a system on CUDA device `device`.  `stream` is a cudaStream_t
+ * (NULL: the library creates its own non-blocking stream). */
+int phgGpuCreate(int device, void *stream, phgGpuSystem **sys);
+int phgGpuDestroy(phgGpuSystem *sys);
+/* Re-targets later work to `stream` (cudaStream_t). */
+int phgGpuSetStream(phgGpuSystem *sys, void *stream);
+
+/* The mesh: replaces the reference's per-element reads of g->verts and
+ * e->verts (phgGeomGetJacobian_, src/geom.c:855-884, computed by
+ * compute_jacobian, src/geom.c:103-169, and phgGeomGetVolume, :809). */
+int phgGpuSetMesh(phgGpuSystem *sys, int64_t nvert, const double *verts,
+		  int64_t nelem, const int32_t *elem_verts);
+
+/* The DOF layout of a scalar Lagrange P`order` space (order 1, 2 or 3):
+ * e2l[e * nbas + k] = vector index of element basis k (phgSolverMapE2L,
+ * include/phg/solver.h:297 -> phgDofMapE2D_, src/dof.c:4821-4881), and
+ * bdry[i] != 0 for Dirichlet DOFs (phgDofDirichletBC__,
+ * src/dof-utils.c:1269-1392).  nbas = 4, 10, 20. */
+int phgGpuSetDofMap(phgGpuSystem *sys, int order, int64_t ndof,
+		    const int32_t *e2l, const uint8_t *bdry);
+
+/* The batched element loop of a reference user program plus assembly:
+ * for every element and basis pair phgQuadGradBasAGradBas (src/quad.c:
+ * 5260-5344; kappa == NULL is phgQuadGradBasDotGradBas), per basis
+ * phgDofDirichletBC (unit row, rhs = g) or phgQuadDofTimesBas (src/quad.c:
+ * 5481-5530), phgMatAddEntries_ (src/matvec.c:5348-5493, exact zeros
+ * dropped, rows in first-touch order), phgVecAddEntries_, then
+ * phgMatAssemble (src/matvec.c:4602-4671: boundary columns removed from the
+ * rows and saved) and phgSolverUpdateRHS (src/solver.c:508-754).
+ *   kappa  per-element coefficient (nelem) or NULL
+ *   f      f_h DOF values (ndof) or NULL (zero)
+ *   g      Dirichlet values at the DOFs (ndof) or NULL (zero)
+ * The matrix and RHS stay on the device for the solver calls below. */
+int phgGpuBuildLinearSystem(phgGpuSystem *sys, const double *kappa,
+			    const double *f, const double *g);
+
+/* Installs an already-assembled matrix instead (the rows PHG hands an OEM
+ * solver, src/solver.c:223-285): CSR with int64 row pointers (PHG's
+ * size_t packed_ind), int32 columns, and the right-hand side. */
+int phgGpuSetMatrix(phgGpuSystem *sys, int64_t n, const int64_t *ptr,
+		    const int32_t *cols, const double *vals, const double *rhs);
+
+/* Sizes of the assembled system: rows, matrix entries, saved boundary
+ * column entries. */
+int phgGpuGetSizes(phgGpuSystem *sys, int64_t *n, int64_t *nnz,
+		   int64_t *nnz_bdry);
+/* Copies out the matrix rows (phgMatPack layout, src/matvec.c:279-416:
+ * row order and in-row order kept), any argument may be NULL. */
+int phgGpuGetMatrix(phgGpuSystem *sys, int64_t *ptr, int32_t *cols,
+		    double *vals);
+/* Copies out the saved boundary columns (MAT.bdry_rows). */
+int phgGpuGetBdryColumns(phgGpuSystem *sys, int64_t *ptr, int32_t *cols,
+			 double *vals);
+/* Copies out the updated right-hand side / the Jacobi diagonal
+ * (phgMatSetupDiagonal, src/matvec.c:500-549). */
+int phgGpuGetRHS(phgGpuSystem *sys, double *rhs);
+int phgGpuGetDiagonal(phgGpuSystem *sys, double *diag);
+
+/* y = A x  (phgMatVec(MAT_OP_N, 1.0, A, x, 0.0, &y), src/matvec.c:552).
+ * When x and y are both device pointers the call is asynchronous on the
+ * system's stream; otherwise it returns with y written. */
+int phgGpuMatVec(phgGpuSystem *sys, const double *x, double *y);
+
+/* Jacobi-preconditioned CG on the assembled system, FP64 throughout
+ * (solver_pcg, src/solver-phg.c:485-604; jacobi_pc :207-245; stopping rule
+ * ||r|| <= max(rtol ||r0||, btol ||b||, atol), get_tol :104).
+ * x: initial guess in, solution out (n).  Returns the iteration count
+ * (>= 0) or a negative error code; *residual gets the final ||r||_2.
+ * hist (optional, maxit + 1 doubles) receives ||r|| after each
+ * iteration, hist[0] = ||r0||. */
+int phgGpuSolverPCG(phgGpuSystem *sys, double rtol, double btol,
+		    double atol, int maxit, double *x, double *residual,
+		    double *hist);
+
+/* Number of kernels this system has launched so far (the nodes of captured
+ * PCG graphs included): no counterpart in the reference, an aid for
+ * profiling. */
+int phgGpuGetLaunchCount(phgGpuSystem *sys, int64_t *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PHG_GPU_H */

@@ -34,6 +34,7 @@ static char *dump_dir = NULL;
 static char *kappa_file = NULL;
 static INT rhs_case = 0;		/* 0: sine (g = 0), 1: linear u=x+y+z */
 static INT repeat = 1;			/* repeat the whole pipeline (timing) */
+static INT sample_maxit = 0;		/* > 0: cap PCG iterations after rep 0 */
 static const char *rhs_case_names[] = {"sine", "linear", NULL};
 
 static void
@@ -123,6 +124,9 @@ main(int argc, char *argv[])
     phgOptionsRegisterKeyword("-rhs_case", "Right-hand side / BC case",
 		rhs_case_names, &rhs_case);
     phgOptionsRegisterInt("-repeat", "Repeat the pipeline (timing)", &repeat);
+    phgOptionsRegisterInt("-sample_maxit",
+		"PCG iteration cap for repetitions after the first (timing samples)",
+		&sample_maxit);
 
     phgInit(&argc, &argv);
     if (mesh_file == NULL)
@@ -154,6 +158,10 @@ main(int argc, char *argv[])
 	BOOLEAN last = (rep == repeat - 1);
 	phgDofSetDataByValue(u_h, 0.0);
 	solver = phgSolverCreate(SOLVER_DEFAULT, u_h, NULL);
+	if (rep > 0 && sample_maxit > 0) {
+	    solver->maxit = sample_maxit;
+	    solver->warn_maxit = FALSE;
+	}
 
 	if (dump && last) {
 	    e2l = phgAlloc(g->nelem * nbas * sizeof(*e2l));

@@ -1,0 +1,197 @@
+"""ctypes binding of libphg_b200.so (include/phg_gpu.h).
+
+`Solver` mirrors the reference's objects for this path: a GRID (set_mesh), a
+DOF layout (set_dof_map), the user element loop plus phgSolverAssemble
+(build_linear_system), phgMatVec (mat_vec) and phgSolverSolve with the PCG
+solver (solve_pcg).  Arrays may be numpy arrays (host memory) or torch CUDA
+tensors (device memory, used in place).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libphg_b200.so")
+
+ERRORS = {-1: "PHG_GPU_ERR_ARG", -2: "PHG_GPU_ERR_CUDA", -3: "PHG_GPU_ERR_STATE",
+          -4: "PHG_GPU_ERR_LIMIT", -5: "PHG_GPU_ERR_BREAKDOWN", -6: "PHG_GPU_ERR_NAN"}
+
+# name -> (restype, argtypes) of every entry point declared in phg_gpu.h
+_P = C.c_void_p
+_I64 = C.c_int64
+SIGNATURES = {
+    "phgGpuLastError": (C.c_char_p, []),
+    "phgGpuVersion": (C.c_int, []),
+    "phgGpuCreate": (C.c_int, [C.c_int, _P, C.POINTER(_P)]),
+    "phgGpuDestroy": (C.c_int, [_P]),
+    "phgGpuSetStream": (C.c_int, [_P, _P]),
+    "phgGpuSetMesh": (C.c_int, [_P, _I64, _P, _I64, _P]),
+    "phgGpuSetDofMap": (C.c_int, [_P, C.c_int, _I64, _P, _P]),
+    "phgGpuBuildLinearSystem": (C.c_int, [_P, _P, _P, _P]),
+    "phgGpuSetMatrix": (C.c_int, [_P, _I64, _P, _P, _P, _P]),
+    "phgGpuGetSizes": (C.c_int, [_P, C.POINTER(_I64), C.POINTER(_I64), C.POINTER(_I64)]),
+    "phgGpuGetMatrix": (C.c_int, [_P, _P, _P, _P]),
+    "phgGpuGetBdryColumns": (C.c_int, [_P, _P, _P, _P]),
+    "phgGpuGetRHS": (C.c_int, [_P, _P]),
+    "phgGpuGetDiagonal": (C.c_int, [_P, _P]),
+    "phgGpuMatVec": (C.c_int, [_P, _P, _P]),
+    "phgGpuSolverPCG": (C.c_int, [_P, C.c_double, C.c_double, C.c_double, C.c_int, _P,
+                                  C.POINTER(C.c_double), _P]),
+    "phgGpuGetLaunchCount": (C.c_int, [_P, C.POINTER(_I64)]),
+}
+
+_LIB = None
+
+
+class PhgGpuError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (ERRORS.get(code, "error"), code, msg))
+        self.code = code
+
+
+def load_library(path=LIB_PATH):
+    """Loads the library without touching the GPU (no CUDA calls)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(path):
+            raise RuntimeError("libphg_b200.so is not built (run __graft_entry__.build())")
+        L = C.CDLL(path)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def lib():
+    return load_library()
+
+
+def _check(rc):
+    if rc < 0:
+        raise PhgGpuError(rc, lib().phgGpuLastError().decode())
+    return rc
+
+
+def _ptr(a):
+    """Raw pointer of a numpy array or a torch tensor (None -> NULL)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("arrays must be C-contiguous")
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensors must be contiguous")
+        return a.data_ptr()
+    raise TypeError("expected a numpy array or a torch tensor, got %r" % type(a))
+
+
+def _np(a, dtype):
+    if a is None or hasattr(a, "data_ptr"):
+        return a
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+class Solver:
+    """One assembled linear system on one GPU (a phgGpuSystem)."""
+
+    def __init__(self, device=0, stream=None):
+        self._h = C.c_void_p()
+        _check(lib().phgGpuCreate(int(device), stream, C.byref(self._h)))
+        self._keep = []
+
+    def close(self):
+        if self._h:
+            lib().phgGpuDestroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_stream(self, stream):
+        _check(lib().phgGpuSetStream(self._h, stream))
+
+    def set_mesh(self, verts, elems):
+        verts, elems = _np(verts, np.float64), _np(elems, np.int32)
+        _check(lib().phgGpuSetMesh(self._h, len(verts), _ptr(verts), len(elems), _ptr(elems)))
+
+    def set_dof_map(self, order, e2l, bdry):
+        e2l, bdry = _np(e2l, np.int32), _np(bdry, np.uint8)
+        _check(lib().phgGpuSetDofMap(self._h, int(order), len(bdry), _ptr(e2l), _ptr(bdry)))
+
+    def build_linear_system(self, kappa=None, f=None, g=None):
+        kappa, f, g = _np(kappa, np.float64), _np(f, np.float64), _np(g, np.float64)
+        _check(lib().phgGpuBuildLinearSystem(self._h, _ptr(kappa), _ptr(f), _ptr(g)))
+
+    def set_matrix(self, ptr, cols, vals, rhs):
+        ptr, cols = _np(ptr, np.int64), _np(cols, np.int32)
+        vals, rhs = _np(vals, np.float64), _np(rhs, np.float64)
+        _check(lib().phgGpuSetMatrix(self._h, len(ptr) - 1, _ptr(ptr), _ptr(cols), _ptr(vals), _ptr(rhs)))
+
+    def sizes(self):
+        n, nnz, bnnz = _I64(), _I64(), _I64()
+        _check(lib().phgGpuGetSizes(self._h, C.byref(n), C.byref(nnz), C.byref(bnnz)))
+        return n.value, nnz.value, bnnz.value
+
+    def get_matrix(self):
+        n, nnz, _ = self.sizes()
+        ptr, cols, vals = np.empty(n + 1, np.int64), np.empty(nnz, np.int32), np.empty(nnz)
+        _check(lib().phgGpuGetMatrix(self._h, _ptr(ptr), _ptr(cols), _ptr(vals)))
+        return ptr, cols, vals
+
+    def get_bdry_columns(self):
+        n, _, bnnz = self.sizes()
+        ptr, cols, vals = np.empty(n + 1, np.int64), np.empty(bnnz, np.int32), np.empty(bnnz)
+        _check(lib().phgGpuGetBdryColumns(self._h, _ptr(ptr), _ptr(cols), _ptr(vals)))
+        return ptr, cols, vals
+
+    def get_rhs(self):
+        out = np.empty(self.sizes()[0])
+        _check(lib().phgGpuGetRHS(self._h, _ptr(out)))
+        return out
+
+    def get_diagonal(self):
+        out = np.empty(self.sizes()[0])
+        _check(lib().phgGpuGetDiagonal(self._h, _ptr(out)))
+        return out
+
+    def mat_vec(self, x, y=None):
+        x = _np(x, np.float64)
+        if y is None:
+            y = np.empty(self.sizes()[0])
+        _check(lib().phgGpuMatVec(self._h, _ptr(x), _ptr(y)))
+        return y
+
+    def launch_count(self):
+        c = _I64()
+        _check(lib().phgGpuGetLaunchCount(self._h, C.byref(c)))
+        return c.value
+
+    def solve_pcg(self, x0=None, rtol=1e-10, btol=1e-10, atol=0.0, maxit=10000, history=False, out=None):
+        """phgSolverSolve with -solver pcg -pcg_pc_type jacobi.  Returns
+        (x, nits, residual) or (x, nits, residual, history)."""
+        n = self.sizes()[0]
+        if out is not None:
+            x = out
+        else:
+            x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+        hist = np.empty(maxit + 1) if history else None
+        res = C.c_double()
+        nits = _check(lib().phgGpuSolverPCG(self._h, rtol, btol, atol, int(maxit), _ptr(x),
+                                            C.byref(res), _ptr(hist)))
+        if history:
+            return x, nits, res.value, hist[:nits + 1]
+        return x, nits, res.value

@@ -1,0 +1,587 @@
+// Element assembly on the device: element matrices and vectors, the DOF ->
+// element incidence lists, and the deterministic row-owner assembly into CSR.
+//
+// Data layout in HBM (one system):
+//   verts   f64 [nvert][3]           coordinates (PHG g->verts)
+//   elems   i32 [nelem][4]           element vertices (PHG e->verts)
+//   e2l     i32 [nelem][N]           vector index of each element basis
+//   bdry    u8  [ndof]               Dirichlet flag per DOF
+//   inc_ptr i32 [ndof+1], inc i32    per DOF, the incident (element, basis)
+//                                    pairs as keys e*N+a, ascending
+//   Ke      f64 [nelem][N][N]        element matrices (row a = basis a)
+//   Re      f64 [nelem][N]           element right-hand sides
+//   ptr/cols/vals                    CSR (rows in first-touch order)
+//   bptr/bcols/bvals                 saved boundary columns
+//   rhs, diag                        f64 [ndof]
+//
+// The element kernel repeats the reference's floating-point operations one by
+// one (explicit round-to-nearest intrinsics, no fused multiply-adds), so the
+// element entries -- and therefore which entries are exactly zero and get
+// dropped -- are identical to the reference's.  The row walk then visits each
+// row's contributions in element order, which is the order the reference's
+// element loop adds them in, so the assembled values are identical as well.
+#include "common.cuh"
+#include "assemble.h"
+
+namespace phgb {
+
+// ---------------------------------------------------------------------------
+// Geometry: compute_jacobian (geom.c:103-169) and the volume
+// (geom.c:46-78), operation for operation.
+__device__ __forceinline__ void jacobian_vol(const double *x, double *J, double &vol) {
+    double a[4][8];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+#pragma unroll
+        for (int i = 0; i < 3; i++) a[j][i] = x[3 * j + i];
+        a[j][3] = 1.0;
+#pragma unroll
+        for (int i = 0; i < 4; i++) a[j][4 + i] = (i == j) ? 1.0 : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        double d = fabs(a[j][j]);
+        int k = j;
+#pragma unroll
+        for (int i = j + 1; i < 4; i++) {
+            const double t = fabs(a[i][j]);
+            if (d < t) { d = t; k = i; }
+        }
+        // row swap, written as selects so the array stays in registers
+#pragma unroll
+        for (int r = j + 1; r < 4; r++) {
+            if (r == k) {
+#pragma unroll
+                for (int i = j; i < 8; i++) {
+                    const double t = a[j][i];
+                    a[j][i] = a[r][i];
+                    a[r][i] = t;
+                }
+            }
+        }
+        const double t = a[j][j];
+        d = __ddiv_rn(1.0, t == 0. ? 1. : t);
+#pragma unroll
+        for (int i = j + 1; i < 8; i++) a[j][i] = rn_mul(a[j][i], d);
+#pragma unroll
+        for (int i = j + 1; i < 4; i++) {
+            const double m = a[i][j];
+#pragma unroll
+            for (int c = j + 1; c < 8; c++) a[i][c] = rn_sub(a[i][c], rn_mul(m, a[j][c]));
+        }
+    }
+#pragma unroll
+    for (int j = 2; j >= 0; j--)
+#pragma unroll
+        for (int i = j + 1; i < 4; i++) {
+            const double d = a[j][i];
+#pragma unroll
+            for (int c = 4; c < 8; c++) a[j][c] = rn_sub(a[j][c], rn_mul(d, a[i][c]));
+        }
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+        for (int i = 0; i < 4; i++) J[4 * j + i] = a[i][j + 4];
+
+    const double x0 = x[0], y0 = x[1], z0 = x[2];
+    const double x1 = rn_sub(x[3], x0), y1 = rn_sub(x[4], y0), z1 = rn_sub(x[5], z0);
+    const double x2 = rn_sub(x[6], x0), y2 = rn_sub(x[7], y0), z2 = rn_sub(x[8], z0);
+    const double x3 = rn_sub(x[9], x0), y3 = rn_sub(x[10], y0), z3 = rn_sub(x[11], z0);
+    const double s1 = rn_add(rn_add(rn_mul(rn_mul(x1, y2), z3), rn_mul(rn_mul(x2, y3), z1)),
+                           rn_mul(rn_mul(y1, z2), x3));
+    const double s2 = rn_add(rn_add(rn_mul(rn_mul(z1, y2), x3), rn_mul(rn_mul(y1, x2), z3)),
+                           rn_mul(rn_mul(z2, y3), x1));
+    vol = rn_mul(fabs(rn_sub(s1, s2)), 0x1.5555555555555p-3 /* 1/6 */);
+}
+
+// ---------------------------------------------------------------------------
+// Element kernel: one warp per element.
+//   Ke[e] = N x N stiffness: integral of grad phi_b . kappa grad phi_a with the
+//           order-2(p-1) rule (phgQuadGradBasAGradBas, quad.c:5260-5344, basis
+//           gradients as phgQuadGetBasisGradient, quad.c:3314-3421)
+//   Re[e] = N right-hand side entries, integral of f_h phi_a with the order-2p
+//           rule (phgQuadDofTimesBas, quad.c:5481-5530; f_h at the points as
+//           phgDofEval_, dof-utils.c:59-300)
+template <int P>
+struct ElemDims {
+    static constexpr int N = P == 1 ? 4 : P == 2 ? 10 : 20;
+    static constexpr int QK = P == 1 ? 1 : P == 2 ? 4 : 14;
+    static constexpr int QR = P == 1 ? 4 : P == 2 ? 14 : 24;
+};
+
+constexpr int kElemWarps = 4;
+
+template <int P>
+__global__ void __launch_bounds__(kElemWarps * 32)
+element_kernel(int64_t nelem, int64_t nvert, int64_t ndof, const double *__restrict__ verts,
+               const int32_t *__restrict__ elems, const int32_t *__restrict__ e2l,
+               const double *__restrict__ kappa, const double *__restrict__ f,
+               const double *__restrict__ wk, const double *__restrict__ gk,
+               const double *__restrict__ wr, const double *__restrict__ br,
+               double *__restrict__ Ke, double *__restrict__ Re, int *status) {
+    using D = ElemDims<P>;
+    constexpr int N = D::N, QK = D::QK, QR = D::QR;
+    __shared__ double s_grad[kElemWarps][N * QK * 3];
+    __shared__ double s_K[kElemWarps][N * N];
+    __shared__ double s_f[kElemWarps][N];
+    __shared__ double s_fq[kElemWarps][QR];
+
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    double *grad = s_grad[w], *K = s_K[w], *fl = s_f[w], *fq = s_fq[w];
+
+    for (int64_t e = (int64_t)blockIdx.x * kElemWarps + w; e < nelem;
+         e += (int64_t)gridDim.x * kElemWarps) {
+        // vertex coordinates, broadcast to the whole warp
+        double cx = 0, cy = 0, cz = 0;
+        if (lane < 4) {
+            const int32_t v = elems[4 * e + lane];
+            if (v < 0 || v >= nvert) {
+                atomicExch(status, PHGB_DEV_BAD_INDEX);
+            } else {
+                cx = verts[3 * (int64_t)v];
+                cy = verts[3 * (int64_t)v + 1];
+                cz = verts[3 * (int64_t)v + 2];
+            }
+        }
+        double x[12];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            x[3 * j] = __shfl_sync(0xffffffffu, cx, j);
+            x[3 * j + 1] = __shfl_sync(0xffffffffu, cy, j);
+            x[3 * j + 2] = __shfl_sync(0xffffffffu, cz, j);
+        }
+        double J[16], vol;
+        jacobian_vol(x, J, vol);
+        const double kap = kappa != nullptr ? kappa[e] : 0.0;
+
+        // basis gradients at the stiffness points: grad[(k*QK + q)*3 + c]
+        for (int idx = lane; idx < N * QK; idx += 32) {
+            const int k = idx / QK, q = idx % QK;
+            double *o = grad + 3 * idx;
+            if (P == 1) {
+                o[0] = J[4 * k]; o[1] = J[4 * k + 1]; o[2] = J[4 * k + 2];
+            } else if (k < 4) {
+                const double d = gk[(q * N + k) * 4 + k];
+                o[0] = rn_mul(d, J[4 * k]);
+                o[1] = rn_mul(d, J[4 * k + 1]);
+                o[2] = rn_mul(d, J[4 * k + 2]);
+            } else {
+                const double *G = gk + (q * N + k) * 4;
+                const double g0 = G[0], g1 = G[1], g2 = G[2], g3 = G[3];
+#pragma unroll
+                for (int c = 0; c < 3; c++)
+                    o[c] = rn_add(rn_add(rn_add(rn_mul(g0, J[c]), rn_mul(g1, J[4 + c])),
+                                     rn_mul(g2, J[8 + c])),
+                                rn_mul(g3, J[12 + c]));
+            }
+        }
+        __syncwarp();
+
+        // symmetric pairs b <= a
+        for (int idx = lane; idx < N * (N + 1) / 2; idx += 32) {
+            int a = (int)((sqrtf(8.0f * idx + 1.0f) - 1.0f) * 0.5f);
+            while (a * (a + 1) / 2 > idx) a--;
+            while ((a + 1) * (a + 2) / 2 <= idx) a++;
+            const int b = idx - a * (a + 1) / 2;
+            double d = 0.;
+#pragma unroll 4
+            for (int q = 0; q < QK; q++) {
+                const double *g1 = grad + 3 * (b * QK + q);
+                const double *g2 = grad + 3 * (a * QK + q);
+                const double d0 = rn_add(0., rn_add(rn_add(rn_mul(g1[0], g2[0]), rn_mul(g1[1], g2[1])),
+                                                rn_mul(g1[2], g2[2])));
+                const double t = rn_mul(d0, wk[q]);
+                d = rn_add(d, kappa != nullptr ? rn_mul(t, kap) : t);
+            }
+            const double v = rn_mul(d, vol);
+            K[a * N + b] = v;
+            K[b * N + a] = v;
+        }
+        __syncwarp();
+        double *ke = Ke + (size_t)e * N * N;
+        for (int t = lane; t < N * N; t += 32) ke[t] = K[t];
+
+        // right-hand side
+        if (lane < N) {
+            double fv = 0.0;
+            if (f != nullptr) {
+                const int32_t d = e2l[(size_t)e * N + lane];
+                if (d < 0 || d >= ndof) atomicExch(status, PHGB_DEV_BAD_INDEX);
+                else fv = f[d];
+            }
+            fl[lane] = fv;
+        }
+        __syncwarp();
+        for (int q = lane; q < QR; q += 32) {
+            double v = 0.0;
+            for (int k = 0; k < N; k++) v = rn_add(v, rn_mul(br[q * N + k], fl[k]));
+            fq[q] = v;
+        }
+        __syncwarp();
+        if (lane < N) {
+            double d = 0.0;
+            for (int q = 0; q < QR; q++) d = rn_add(d, rn_mul(rn_mul(br[q * N + lane], wr[q]), fq[q]));
+            Re[(size_t)e * N + lane] = rn_mul(d, vol);
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// DOF -> (element, basis) incidence lists.
+
+__global__ void inc_count_kernel(int64_t nkeys, int N, int64_t ndof, const int32_t *__restrict__ e2l,
+                                 int32_t *__restrict__ cnt, int *status) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nkeys;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t d = e2l[t];
+        if (d < 0 || d >= ndof) { atomicExch(status, PHGB_DEV_BAD_INDEX); continue; }
+        atomicAdd(&cnt[d], 1);
+    }
+}
+
+__global__ void inc_fill_kernel(int64_t nkeys, int64_t ndof, const int32_t *__restrict__ e2l,
+                                const int32_t *__restrict__ inc_ptr, int32_t *__restrict__ cursor,
+                                int32_t *__restrict__ inc) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nkeys;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t d = e2l[t];
+        if (d < 0 || d >= ndof) continue;
+        const int32_t pos = atomicAdd(&cursor[d], 1);
+        inc[inc_ptr[d] + pos] = (int32_t)t;   // key = e * N + a
+    }
+}
+
+// Sorts each DOF's short incidence list ascending (element order).
+__global__ void inc_sort_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr,
+                                int32_t *__restrict__ inc) {
+    for (int64_t d = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; d < ndof;
+         d += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t b = inc_ptr[d], n = inc_ptr[d + 1] - b;
+        int32_t *v = inc + b;
+        for (int i = 1; i < n; i++) {
+            const int32_t key = v[i];
+            int j = i - 1;
+            while (j >= 0 && v[j] > key) { v[j + 1] = v[j]; j--; }
+            v[j + 1] = key;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Exclusive scan of int32 counts (three phases), with the total.
+constexpr int kScanBlock = 1024;
+
+__global__ void scan_local_kernel(int64_t n, const int32_t *__restrict__ in, int32_t *__restrict__ out,
+                                  int64_t *__restrict__ block_sums) {
+    __shared__ int64_t s[kScanBlock];
+    const int64_t i = (int64_t)blockIdx.x * kScanBlock + threadIdx.x;
+    const int64_t v = i < n ? in[i] : 0;
+    s[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = 1; o < kScanBlock; o <<= 1) {
+        const int64_t t = threadIdx.x >= o ? s[threadIdx.x - o] : 0;
+        __syncthreads();
+        s[threadIdx.x] += t;
+        __syncthreads();
+    }
+    if (i < n) out[i] = (int32_t)(s[threadIdx.x] - v);   // block-local exclusive
+    if (threadIdx.x == kScanBlock - 1) block_sums[blockIdx.x] = s[threadIdx.x];
+}
+
+__global__ void scan_blocks_kernel(int64_t nb, int64_t *__restrict__ block_sums, int64_t *__restrict__ total) {
+    // single block: serial per thread chunk, then across threads
+    __shared__ int64_t s[1024];
+    const int64_t chunk = (nb + blockDim.x - 1) / blockDim.x;
+    const int64_t b0 = threadIdx.x * chunk, b1 = min(nb, b0 + chunk);
+    int64_t acc = 0;
+    for (int64_t b = b0; b < b1; b++) acc += block_sums[b];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int64_t run = 0;
+        for (int t = 0; t < (int)blockDim.x; t++) { const int64_t c = s[t]; s[t] = run; run += c; }
+        *total = run;
+    }
+    __syncthreads();
+    acc = s[threadIdx.x];
+    for (int64_t b = b0; b < b1; b++) { const int64_t c = block_sums[b]; block_sums[b] = acc; acc += c; }
+}
+
+__global__ void scan_add_kernel(int64_t n, int32_t *__restrict__ out, const int64_t *__restrict__ block_sums,
+                                const int64_t *__restrict__ total) {
+    const int64_t i = (int64_t)blockIdx.x * kScanBlock + threadIdx.x;
+    if (i < n) out[i] = (int32_t)(out[i] + block_sums[blockIdx.x]);
+    if (i == n) out[n] = (int32_t)*total;
+}
+
+// ---------------------------------------------------------------------------
+// Row walk: one warp per row.  For an interior row the warp visits the row's
+// incidences in element order; lane j handles element column j, skips exact
+// zeros (phgMatAddEntries_, matvec.c:5459-5461), finds or appends the column
+// (add_columns_to_row, matvec.c:3286-3321: first-touch order) through a
+// per-warp open-addressing table in shared memory, and (pass 2) accumulates
+// the value.  Boundary columns are then separated from the row as
+// save_bdry_columns does (matvec.c:4430-4488) and lifted into the RHS as
+// update_rhs does (solver.c:707-725).  A Dirichlet row is the sum of the unit
+// rows of its elements (phgDofDirichletBC, dof-utils.c:1369-1392).
+template <int N, int HS>
+struct WalkCfg {
+    static constexpr int MAXROW = HS / 2;
+    static constexpr int WARPS = 4;
+};
+
+__device__ __forceinline__ unsigned hash32(int32_t c) { return (unsigned)c * 2654435761u; }
+
+// Sum of g_k added mult times (the Dirichlet row's RHS, phgVecAddEntries_).
+__device__ __forceinline__ double bdry_rhs(const double *g, int32_t k, int mult) {
+    if (g == nullptr) return 0.0;
+    const double v = g[k];
+    if (v == 0.0) return 0.0;
+    double s = 0.0;
+    for (int i = 0; i < mult; i++) s = rn_add(s, v);
+    return s;
+}
+
+template <int N, int HS, bool PASS2>
+__global__ void __launch_bounds__(WalkCfg<N, HS>::WARPS * 32)
+row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t *__restrict__ inc,
+                const int32_t *__restrict__ e2l, const uint8_t *__restrict__ bdry,
+                const double *__restrict__ Ke, const double *__restrict__ Re,
+                const double *__restrict__ g,
+                // pass 1 outputs
+                int32_t *__restrict__ cnt_keep, int32_t *__restrict__ cnt_bdry,
+                // pass 2 inputs / outputs
+                const int32_t *__restrict__ ptr, int32_t *__restrict__ cols, double *__restrict__ vals,
+                const int32_t *__restrict__ bptr, int32_t *__restrict__ bcols, double *__restrict__ bvals,
+                double *__restrict__ rhs, double *__restrict__ diag, int *status) {
+    using C = WalkCfg<N, HS>;
+    constexpr int MAXROW = C::MAXROW;
+    __shared__ int32_t s_key[C::WARPS][HS];
+    __shared__ int16_t s_pos[C::WARPS][HS];
+    __shared__ int32_t s_col[C::WARPS][PASS2 ? MAXROW : 1];
+    __shared__ double s_val[C::WARPS][PASS2 ? MAXROW : 1];
+
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    int32_t *key = s_key[w];
+    int16_t *hpos = s_pos[w];
+
+    for (int64_t d = (int64_t)blockIdx.x * C::WARPS + w; d < ndof; d += (int64_t)gridDim.x * C::WARPS) {
+        const int32_t i0 = inc_ptr[d], i1 = inc_ptr[d + 1];
+        if (bdry[d]) {
+            if (lane == 0) {
+                const int mult = i1 - i0;
+                if (!PASS2) {
+                    cnt_keep[d] = mult > 0 ? 1 : 0;
+                    cnt_bdry[d] = mult > 0 ? 1 : 0;
+                } else {
+                    double m = 0.0;
+                    for (int i = 0; i < mult; i++) m = rn_add(m, 1.0);
+                    if (mult > 0) {
+                        cols[ptr[d]] = (int32_t)d;
+                        vals[ptr[d]] = m;
+                        bcols[bptr[d]] = (int32_t)d;
+                        bvals[bptr[d]] = m;
+                    }
+                    diag[d] = m;
+                    rhs[d] = bdry_rhs(g, (int32_t)d, mult);
+                }
+            }
+            continue;
+        }
+
+        for (int t = lane; t < HS; t += 32) key[t] = -1;
+        __syncwarp();
+        int L = 0;
+        bool overflow = false;
+        for (int32_t ii = i0; ii < i1; ii++) {
+            const int32_t kk = inc[ii];
+            const int32_t e = kk / N, a = kk - e * N;
+            int32_t col = -1;
+            double v = 0.0;
+            bool nz = false;
+            if (lane < N) {
+                col = e2l[(size_t)e * N + lane];
+                v = Ke[((size_t)e * N + a) * N + lane];
+                nz = (v != 0.0);
+            }
+            // look up
+            int pos = -1;
+            if (nz) {
+                unsigned h = hash32(col) & (HS - 1);
+                for (int probe = 0; probe < HS; probe++) {
+                    const int32_t k = key[h];
+                    if (k == col) { pos = hpos[h]; break; }
+                    if (k == -1) break;
+                    h = (h + 1) & (HS - 1);
+                }
+            }
+            const unsigned newm = __ballot_sync(0xffffffffu, nz && pos < 0);
+            if (nz && pos < 0) {
+                pos = L + __popc(newm & lt_mask);
+                if (pos < MAXROW) {
+                    unsigned h = hash32(col) & (HS - 1);
+                    for (int probe = 0; probe < HS; probe++) {
+                        if (atomicCAS(&key[h], -1, col) == -1) { hpos[h] = (int16_t)pos; break; }
+                        h = (h + 1) & (HS - 1);
+                    }
+                    if (PASS2) { s_col[w][pos] = col; s_val[w][pos] = v; }
+                } else {
+                    overflow = true;
+                }
+            } else if (nz && PASS2) {
+                s_val[w][pos] = rn_add(s_val[w][pos], v);
+            }
+            L += __popc(newm);
+            __syncwarp();
+        }
+        if (__any_sync(0xffffffffu, overflow) || L > MAXROW) {
+            if (lane == 0) atomicExch(status, PHGB_DEV_ROW_OVERFLOW);
+            continue;
+        }
+
+        if (!PASS2) {
+            int nk = 0, nb = 0;
+            for (int t = lane; t < HS; t += 32) {
+                const int32_t c = key[t];
+                if (c < 0) continue;
+                if (c != d && bdry[c]) nb++; else nk++;
+            }
+            nk = warp_sumi(nk);
+            nb = warp_sumi(nb);
+            if (lane == 0) { cnt_keep[d] = nk; cnt_bdry[d] = nb; }
+            __syncwarp();
+            continue;
+        }
+
+        // pass 2: emit kept columns and saved boundary columns, in order
+        const int32_t p0 = ptr[d], b0 = bptr[d];
+        int nk = 0, nb = 0;
+        double dg = 0.0;
+        for (int base = 0; base < L; base += 32) {
+            const int t = base + lane;
+            bool isb = false, valid = t < L;
+            int32_t c = 0;
+            double v = 0.0;
+            if (valid) {
+                c = s_col[w][t];
+                v = s_val[w][t];
+                isb = (c != d) && bdry[c];
+                if (c == d) dg = v;
+            }
+            const unsigned km = __ballot_sync(0xffffffffu, valid && !isb);
+            const unsigned bm = __ballot_sync(0xffffffffu, valid && isb);
+            if (valid && !isb) {
+                const int r = nk + __popc(km & lt_mask);
+                cols[p0 + r] = c;
+                vals[p0 + r] = v;
+            }
+            if (valid && isb) {
+                const int r = nb + __popc(bm & lt_mask);
+                bcols[b0 + r] = c;
+                bvals[b0 + r] = v;
+            }
+            nk += __popc(km);
+            nb += __popc(bm);
+        }
+        dg = warp_sum(dg);   // exactly one lane holds the diagonal
+        if (lane == 0) {
+            if (p0 + nk != ptr[d + 1] || b0 + nb != bptr[d + 1])
+                atomicExch(status, PHGB_DEV_COUNT_MISMATCH);
+            diag[d] = dg;
+            // rhs: element contributions in element order, zeros skipped
+            double r = 0.0;
+            for (int32_t ii = i0; ii < i1; ii++) {
+                const double b = Re[inc[ii]];
+                if (b != 0.0) r = rn_add(r, b);
+            }
+            // lift the boundary columns: r -= 1.0 * rhs_k * a_dk / D_kk
+            for (int t = 0; t < L; t++) {
+                const int32_t c = s_col[w][t];
+                if (c == d || !bdry[c]) continue;
+                const int mult = inc_ptr[c + 1] - inc_ptr[c];
+                double Dk = 0.0;
+                for (int m = 0; m < mult; m++) Dk = rn_add(Dk, 1.0);
+                const double rk = bdry_rhs(g, c, mult);
+                r = rn_sub(r, __ddiv_rn(rn_mul(rn_mul(1.0, rk), s_val[w][t]), Dk));
+            }
+            rhs[d] = r;
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host-side launchers.
+
+static int grid_for(int64_t work, int per_block, int max_blocks) {
+    int64_t b = ceil_div(work, per_block);
+    if (b < 1) b = 1;
+    if (b > max_blocks) b = max_blocks;
+    return (int)b;
+}
+
+cudaError_t launch_element_kernel(int p, const ElemArgs &A, cudaStream_t s) {
+    const int blocks = grid_for(A.nelem, kElemWarps, 148 * 64);
+#define PHGB_ELEM(P)                                                                       \
+    element_kernel<P><<<blocks, kElemWarps * 32, 0, s>>>(A.nelem, A.nvert, A.ndof, A.verts, \
+        A.elems, A.e2l, A.kappa, A.f, A.wk, A.gk, A.wr, A.br, A.Ke, A.Re, A.status)
+    if (p == 1) PHGB_ELEM(1);
+    else if (p == 2) PHGB_ELEM(2);
+    else PHGB_ELEM(3);
+#undef PHGB_ELEM
+    return cudaGetLastError();
+}
+
+cudaError_t launch_incidence(int N, int64_t nelem, int64_t ndof, const int32_t *e2l, int32_t *cnt,
+                             int32_t *inc_ptr, int32_t *cursor, int32_t *inc, int64_t *scan_ws,
+                             int *status, cudaStream_t s) {
+    const int64_t nkeys = nelem * N;
+    cudaMemsetAsync(cnt, 0, sizeof(int32_t) * ndof, s);
+    cudaMemsetAsync(cursor, 0, sizeof(int32_t) * ndof, s);
+    const int bl = grid_for(nkeys, 256, 148 * 16);
+    inc_count_kernel<<<bl, 256, 0, s>>>(nkeys, N, ndof, e2l, cnt, status);
+    cudaError_t err = launch_scan(ndof, cnt, inc_ptr, scan_ws, s);
+    if (err != cudaSuccess) return err;
+    inc_fill_kernel<<<bl, 256, 0, s>>>(nkeys, ndof, e2l, inc_ptr, cursor, inc);
+    inc_sort_kernel<<<grid_for(ndof, 128, 148 * 16), 128, 0, s>>>(ndof, inc_ptr, inc);
+    return cudaGetLastError();
+}
+
+int64_t scan_workspace_elems(int64_t n) { return ceil_div(n + 1, kScanBlock) + 2; }
+
+cudaError_t launch_scan(int64_t n, const int32_t *in, int32_t *out, int64_t *ws, cudaStream_t s) {
+    // ws: block sums (nb) + total; out has n + 1 entries
+    const int64_t nb = ceil_div(n + 1, kScanBlock);
+    int64_t *total = ws + nb;
+    scan_local_kernel<<<(unsigned)nb, kScanBlock, 0, s>>>(n, in, out, ws);
+    scan_blocks_kernel<<<1, 1024, 0, s>>>(nb, ws, total);
+    scan_add_kernel<<<(unsigned)nb, kScanBlock, 0, s>>>(n, out, ws, total);
+    return cudaGetLastError();
+}
+
+template <int N, int HS>
+static cudaError_t walk(bool pass2, const WalkArgs &A, cudaStream_t s) {
+    constexpr int W = WalkCfg<N, HS>::WARPS;
+    const int blocks = grid_for(A.ndof, W, 148 * 32);
+    if (!pass2)
+        row_walk_kernel<N, HS, false><<<blocks, W * 32, 0, s>>>(
+            A.ndof, A.inc_ptr, A.inc, A.e2l, A.bdry, A.Ke, A.Re, A.g, A.cnt_keep, A.cnt_bdry,
+            nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, A.status);
+    else
+        row_walk_kernel<N, HS, true><<<blocks, W * 32, 0, s>>>(
+            A.ndof, A.inc_ptr, A.inc, A.e2l, A.bdry, A.Ke, A.Re, A.g, nullptr, nullptr, A.ptr,
+            A.cols, A.vals, A.bptr, A.bcols, A.bvals, A.rhs, A.diag, A.status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_row_walk(int p, bool pass2, const WalkArgs &A, cudaStream_t s) {
+    if (p == 1) return walk<4, 128>(pass2, A, s);
+    if (p == 2) return walk<10, 256>(pass2, A, s);
+    return walk<20, 512>(pass2, A, s);
+}
+
+int row_walk_max_row(int p) { return p == 1 ? 64 : p == 2 ? 128 : 256; }
+
+}  // namespace phgb

@@ -1,0 +1,40 @@
+// Launch interfaces of the assembly kernels (assemble.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace phgb {
+
+struct ElemArgs {
+    int64_t nelem, nvert, ndof;
+    const double *verts;
+    const int32_t *elems, *e2l;
+    const double *kappa, *f;                 // may be null
+    const double *wk, *gk, *wr, *br;         // element tables
+    double *Ke, *Re;
+    int *status;
+};
+
+struct WalkArgs {
+    int64_t ndof;
+    const int32_t *inc_ptr, *inc, *e2l;
+    const uint8_t *bdry;
+    const double *Ke, *Re, *g;
+    int32_t *cnt_keep, *cnt_bdry;            // pass 1
+    const int32_t *ptr, *bptr;               // pass 2
+    int32_t *cols, *bcols;
+    double *vals, *bvals, *rhs, *diag;
+    int *status;
+};
+
+cudaError_t launch_element_kernel(int p, const ElemArgs &a, cudaStream_t s);
+cudaError_t launch_incidence(int N, int64_t nelem, int64_t ndof, const int32_t *e2l, int32_t *cnt,
+                             int32_t *inc_ptr, int32_t *cursor, int32_t *inc, int64_t *scan_ws,
+                             int *status, cudaStream_t s);
+int64_t scan_workspace_elems(int64_t n);
+// out[0..n] = exclusive prefix sums of in[0..n-1], out[n] = total (int32).
+cudaError_t launch_scan(int64_t n, const int32_t *in, int32_t *out, int64_t *ws, cudaStream_t s);
+cudaError_t launch_row_walk(int p, bool pass2, const WalkArgs &a, cudaStream_t s);
+int row_walk_max_row(int p);
+
+}  // namespace phgb

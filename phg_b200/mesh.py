@@ -57,3 +57,91 @@ def write_medit(path, verts, elems):
             [elems.astype(np.int64) + 1,
              np.ones((len(elems), 1), dtype=np.int64)], 1), fmt="%d")
         fp.write("End\n")
+
+
+# local edge k of a tetrahedron joins local vertices EDGES[k]; local face k is
+# opposite local vertex k (the reference's conventions, lagrange.c P2/P3 bases)
+EDGES = ((0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3))
+FACES = ((1, 2, 3), (0, 2, 3), (0, 1, 3), (0, 1, 2))
+
+
+def lagrange_dofs(verts, elems, p):
+    """Numbers the DOFs of a continuous Lagrange P`p` space (p = 1, 2, 3) the
+    way PHG lays out a DOF object: vertex DOFs first (by vertex index), then
+    edge DOFs (p - 1 per edge), then face DOFs (one per face for P3).
+
+    Returns (e2l int32 [nelem, N], bdry uint8 [ndof], nodes float64 [ndof, 3]):
+    the vector index of each element basis function (local order: vertices,
+    edges -- for P3 the node nearer the edge's first local vertex first --,
+    faces), the Dirichlet flag (DOF on a boundary face, i.e. a face that
+    belongs to one element), and the Lagrange node of each DOF.  On an edge
+    with two DOFs, slot 0 is the node nearer the lower-numbered vertex.
+    """
+    verts = np.asarray(verts, np.float64)
+    elems = np.asarray(elems, np.int64)
+    ne, nv = len(elems), len(verts)
+    N = {1: 4, 2: 10, 3: 20}[p]
+    e2l = np.empty((ne, N), np.int64)
+    e2l[:, :4] = elems
+    ndof = nv
+
+    # boundary faces: faces owned by exactly one element
+    fv = np.sort(elems[:, FACES], axis=2).reshape(-1, 3)
+    fkey = (fv[:, 0] * nv + fv[:, 1]) * nv + fv[:, 2]
+    fu, finv, fcnt = np.unique(fkey, return_inverse=True, return_counts=True)
+    bface = (fcnt == 1)[finv].reshape(ne, 4)
+
+    bdry_v = np.zeros(nv, bool)
+    for k in range(4):
+        for v in FACES[k]:
+            bdry_v[elems[bface[:, k], v]] = True
+    nodes = [verts]
+    bflags = [bdry_v]
+
+    if p >= 2:
+        ev = elems[:, EDGES]                           # ne x 6 x 2
+        lo, hi = ev.min(axis=2), ev.max(axis=2)
+        ekey = lo * nv + hi
+        eu, einv = np.unique(ekey.reshape(-1), return_inverse=True)
+        einv = einv.reshape(ne, 6)
+        nedge = len(eu)
+        elo, ehi = eu // nv, eu % nv
+        # an edge is on the boundary iff it lies in a boundary face
+        bedge = np.zeros(nedge, bool)
+        for k in range(4):
+            f = FACES[k]
+            for a, b in ((f[0], f[1]), (f[0], f[2]), (f[1], f[2])):
+                j = EDGES.index((a, b))
+                bedge[einv[bface[:, k], j]] = True
+        if p == 2:
+            e2l[:, 4:10] = ndof + einv
+            nodes.append(0.5 * (verts[elo] + verts[ehi]))
+            bflags.append(bedge)
+            ndof += nedge
+        else:
+            first_is_low = ev[:, :, 0] < ev[:, :, 1]       # local first vertex is the lower one
+            slot_a = np.where(first_is_low, 0, 1)
+            e2l[:, 4:16:2] = ndof + 2 * einv + slot_a
+            e2l[:, 5:16:2] = ndof + 2 * einv + (1 - slot_a)
+            enodes = np.empty((2 * nedge, 3))
+            enodes[0::2] = (2.0 * verts[elo] + verts[ehi]) / 3.0
+            enodes[1::2] = (verts[elo] + 2.0 * verts[ehi]) / 3.0
+            nodes.append(enodes)
+            bflags.append(np.repeat(bedge, 2))
+            ndof += 2 * nedge
+    if p == 3:
+        e2l[:, 16:20] = ndof + finv.reshape(ne, 4)
+        fa, fb, fc = fu // (nv * nv), (fu // nv) % nv, fu % nv
+        nodes.append((verts[fa] + verts[fb] + verts[fc]) / 3.0)
+        bflags.append(fcnt == 1)
+        ndof += len(fu)
+    return (e2l.astype(np.int32), np.concatenate(bflags).astype(np.uint8),
+            np.concatenate(nodes))
+
+
+def sine_source(nodes):
+    """f = 3 pi^2 sin(pi x) sin(pi y) sin(pi z) at the given nodes; the exact
+    solution of -Laplace u = f with u = 0 on the unit cube's boundary is
+    sin(pi x) sin(pi y) sin(pi z)."""
+    x, y, z = nodes[:, 0], nodes[:, 1], nodes[:, 2]
+    return 3.0 * np.pi ** 2 * np.sin(np.pi * x) * np.sin(np.pi * y) * np.sin(np.pi * z)

@@ -1,0 +1,100 @@
+"""Generates the parity fixtures in tests/golden/ from the UNMODIFIED
+reference (PHG 0.9.7) built from its own sources by `make -C oracle ref`.
+
+For every case it writes the mesh as Medit, runs oracle/_ref/phg_dump (the
+reference's element loop + phgSolverAssemble + phgSolverUpdateRHS +
+phgSolverSolve with -solver pcg, see oracle/ref_driver/phg_dump.c) and stores
+the reference's own inputs (coordinates, element vertices and element->DOF
+maps as PHG numbered them, f and g at the DOF nodes, Dirichlet flags, kappa)
+and outputs (matrix rows before and after boundary elimination, saved
+boundary columns, RHS before/after update_rhs, Jacobi diagonal, solution,
+iteration count, residual) in one compressed .npz per case, plus the
+reference's quadrature rules (quad_rules.npz).
+
+Run here, where the reference is available:  python tests/golden/make_golden.py
+"""
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+from phg_b200.mesh import kuhn_cube, write_medit  # noqa: E402
+
+DUMP = os.path.join(ROOT, "oracle", "_ref", "phg_dump")
+QDUMP = os.path.join(ROOT, "oracle", "_ref", "quad_dump")
+
+# name: (m, P, rhs case, kappa seed or None, rtol)
+CASES = {
+    "p1_m4_sine": (4, 1, "sine", None, 1e-10),
+    "p1_m5_kappa": (5, 1, "sine", 11, 1e-10),
+    "p2_m3_sine": (3, 2, "sine", None, 1e-10),
+    "p2_m5_kappa": (5, 2, "sine", 12, 1e-8),
+    "p2_m6_sine": (6, 2, "sine", None, 1e-8),
+    "p3_m2_sine": (2, 3, "sine", None, 1e-10),
+    "p3_m3_linear": (3, 3, "linear", None, 1e-10),
+    "p3_m3_kappa": (3, 3, "sine", 13, 1e-10),
+}
+
+
+def run_case(name, m, P, case, kseed, rtol):
+    with tempfile.TemporaryDirectory() as d:
+        v, e = kuhn_cube(m)
+        write_medit(os.path.join(d, "m.mesh"), v, e)
+        args = [DUMP, "-mesh_file", os.path.join(d, "m.mesh"), "-dof_type", "P%d" % P,
+                "-solver", "pcg", "-pcg_pc_type", "jacobi", "-solver_rtol", repr(rtol),
+                "-solver_btol", "0", "-solver_atol", "0", "-solver_maxit", "10000",
+                "-map_reorder", "no", "-dump_dir", d, "-rhs_case", case]
+        kappa = None
+        if kseed is not None:
+            kappa = np.exp(np.random.default_rng(kseed).standard_normal(len(e)))
+            kappa.tofile(os.path.join(d, "kappa.in"))
+            args += ["-kappa_file", os.path.join(d, "kappa.in")]
+        subprocess.run(args, check=True, capture_output=True)
+        meta = dict(l.split() for l in open(os.path.join(d, "meta.txt")))
+
+        def L(n, t):
+            return np.fromfile(os.path.join(d, n), t)
+        N = int(meta["nbas"])
+        out = dict(
+            order=P, m=m, rtol=rtol, nits=int(meta["nits"]),
+            residual=float(meta["residual"]),
+            verts=L("verts.f64", np.float64).reshape(-1, 3),
+            elems=L("elems.i32", np.int32).reshape(-1, 4),
+            e2l=L("e2l.i32", np.int32).reshape(-1, N),
+            bdry=L("bdry.u8", np.uint8), f=L("f.f64", np.float64), g=L("g.f64", np.float64),
+            rhs_raw=L("rhs_raw.f64", np.float64), rhs=L("rhs.f64", np.float64),
+            diag=L("diag.f64", np.float64), x=L("x.f64", np.float64))
+        if kappa is not None:
+            out["kappa"] = L("kappa.f64", np.float64)
+        for pre in ("rows_raw", "rows", "bdry_rows"):
+            out[pre + "_ptr"] = L(pre + "_ptr.i64", np.int64)
+            out[pre + "_cols"] = L(pre + "_cols.i32", np.int32)
+            out[pre + "_vals"] = L(pre + "_vals.f64", np.float64)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, "ndof", len(out["bdry"]), "nnz", len(out["rows_cols"]), "nits", out["nits"])
+
+
+def quad_rules():
+    txt = subprocess.run([QDUMP], check=True, capture_output=True, text=True).stdout
+    rules = {}
+    cur = None
+    for line in txt.splitlines():
+        if line.startswith("order"):
+            cur = int(line.split()[1])
+            rules[cur] = []
+        elif cur is not None and line.strip():
+            rules[cur].append([float.fromhex(t) for t in line.split()])
+    np.savez_compressed(os.path.join(HERE, "quad_rules.npz"),
+                        **{"order%d" % k: np.array(v) for k, v in rules.items()})
+    print("quad rules:", {k: len(v) for k, v in rules.items()})
+
+
+if __name__ == "__main__":
+    quad_rules()
+    for name, args in CASES.items():
+        run_case(name, *args)

@@ -1,0 +1,184 @@
+"""Parity of the CUDA path (through the C ABI) with the reference.
+
+* Golden cases (tests/golden/, outputs of the unmodified reference): matrix
+  rows, saved boundary columns, RHS and Jacobi diagonal must match BIT FOR BIT
+  -- the element kernel repeats the reference's floating-point operations and
+  the row walk adds contributions in the reference's element order.
+* Larger meshes: the same, against the CPU oracle on identical inputs.
+* PCG: the device reductions sum in a different order than the reference's
+  sequential loops, so iterates differ by rounding.  Tolerances: iteration
+  count within 2 of the reference; relative L2 distance of the solution to
+  the reference's at most 1e-6 * rtol^(1/2)... written per test below.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def build(pb, order, verts, elems, e2l, bdry, f, g=None, kappa=None):
+    s = pb.Solver(0)
+    s.set_mesh(verts, elems)
+    s.set_dof_map(order, e2l, bdry)
+    s.build_linear_system(kappa=kappa, f=f, g=g)
+    return s
+
+
+def solution_tol(rtol):
+    # two PCG runs to relative residual rtol that differ only in rounding
+    return 1e3 * rtol
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_golden_assembly_bitexact(gpu, name):
+    G = load_golden(name)
+    s = build(gpu, int(G["order"]), G["verts"], G["elems"], G["e2l"], G["bdry"], G["f"], G["g"],
+              G.get("kappa"))
+    ptr, cols, vals = s.get_matrix()
+    assert np.array_equal(ptr, G["rows_ptr"])
+    assert np.array_equal(cols, G["rows_cols"])
+    assert np.array_equal(vals, G["rows_vals"])
+    bptr, bcols, bvals = s.get_bdry_columns()
+    assert np.array_equal(bptr, G["bdry_rows_ptr"])
+    assert np.array_equal(bcols, G["bdry_rows_cols"])
+    assert np.array_equal(bvals, G["bdry_rows_vals"])
+    assert np.array_equal(s.get_rhs(), G["rhs"])
+    assert np.array_equal(s.get_diagonal(), G["diag"])
+    s.close()
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_golden_pcg(gpu, name):
+    G = load_golden(name)
+    s = build(gpu, int(G["order"]), G["verts"], G["elems"], G["e2l"], G["bdry"], G["f"], G["g"],
+              G.get("kappa"))
+    rtol = float(G["rtol"])
+    x, nits, res, hist = s.solve_pcg(rtol=rtol, btol=0.0, atol=0.0, history=True)
+    assert abs(nits - int(G["nits"])) <= 2
+    ref = G["x"]
+    assert np.linalg.norm(x - ref) <= solution_tol(rtol) * np.linalg.norm(ref)
+    assert res <= rtol * hist[0]
+    assert len(hist) == nits + 1
+    s.close()
+
+
+@pytest.mark.parametrize("p,m", [(1, 32), (2, 12), (3, 6)])
+def test_larger_meshes_vs_oracle(gpu, oracle, p, m):
+    v, e = gpu.kuhn_cube(m)
+    e2l, bdry, nodes = gpu.lagrange_dofs(v, e, p)
+    f = gpu.sine_source(nodes)
+    kappa = np.exp(0.5 * np.random.default_rng(p * 100 + m).standard_normal(len(e)))
+    o = oracle.assemble(p, v, e, e2l, bdry, f, None, kappa)
+    s = build(gpu, p, v, e, e2l, bdry, f, None, kappa)
+    ptr, cols, vals = s.get_matrix()
+    assert np.array_equal(ptr, o["ptr"])
+    assert np.array_equal(cols, o["cols"])
+    assert np.array_equal(vals, o["vals"])
+    assert np.array_equal(s.get_rhs(), o["rhs"])
+    assert np.array_equal(s.get_diagonal(), o["diag"])
+    rtol = 1e-10
+    xo, no, ro, _ = oracle.pcg(o["ptr"], o["cols"], o["vals"], o["diag"], o["rhs"], rtol=rtol,
+                               btol=0.0, atol=0.0)
+    x, nits, res = s.solve_pcg(rtol=rtol, btol=0.0, atol=0.0)
+    assert abs(nits - no) <= 2
+    assert np.linalg.norm(x - xo) <= solution_tol(rtol) * np.linalg.norm(xo)
+    # the GPU's own residual, recomputed independently in FP64 by the oracle
+    r = o["rhs"] - oracle.spmv(o["ptr"], o["cols"], o["vals"], x)
+    assert np.linalg.norm(r) <= 2 * rtol * np.linalg.norm(o["rhs"])
+    s.close()
+
+
+def test_matvec_vs_oracle(gpu, oracle):
+    G = load_golden("p2_m6_sine")
+    s = build(gpu, 2, G["verts"], G["elems"], G["e2l"], G["bdry"], G["f"], G["g"])
+    x = np.random.default_rng(5).standard_normal(len(G["bdry"]))
+    y = s.mat_vec(x)
+    yo = oracle.spmv(G["rows_ptr"], G["rows_cols"], G["rows_vals"], x)
+    assert np.allclose(y, yo, rtol=1e-13, atol=1e-13 * np.abs(yo).max())
+    s.close()
+
+
+def test_set_matrix_path(gpu):
+    """The OEM-solver entry: a CSR assembled elsewhere (the reference's rows)."""
+    G = load_golden("p3_m3_kappa")
+    s = gpu.Solver(0)
+    s.set_matrix(G["rows_ptr"], G["rows_cols"], G["rows_vals"], G["rhs"])
+    assert np.array_equal(s.get_diagonal(), G["diag"])
+    x, nits, res = s.solve_pcg(rtol=float(G["rtol"]), btol=0.0, atol=0.0)
+    assert abs(nits - int(G["nits"])) <= 2
+    assert np.linalg.norm(x - G["x"]) <= solution_tol(float(G["rtol"])) * np.linalg.norm(G["x"])
+    s.close()
+
+
+def test_device_tensors_in_place(gpu):
+    import torch
+    G = load_golden("p2_m5_kappa")
+    dev = {k: torch.from_numpy(np.ascontiguousarray(G[k])).cuda()
+           for k in ("verts", "elems", "e2l", "bdry", "f", "g", "kappa")}
+    s = build(gpu, 2, dev["verts"], dev["elems"], dev["e2l"], dev["bdry"], dev["f"], dev["g"], dev["kappa"])
+    ptr, cols, vals = s.get_matrix()
+    assert np.array_equal(vals, G["rows_vals"])
+    x = torch.zeros(len(G["bdry"]), dtype=torch.float64, device="cuda")
+    _, nits, res = s.solve_pcg(rtol=float(G["rtol"]), btol=0.0, atol=0.0, out=x)
+    assert abs(nits - int(G["nits"])) <= 2
+    xr = G["x"]
+    assert np.linalg.norm(x.cpu().numpy() - xr) <= solution_tol(float(G["rtol"])) * np.linalg.norm(xr)
+    s.close()
+
+
+def test_maxit_stops(gpu):
+    G = load_golden("p2_m6_sine")
+    s = build(gpu, 2, G["verts"], G["elems"], G["e2l"], G["bdry"], G["f"], G["g"])
+    x, nits, res = s.solve_pcg(rtol=1e-14, btol=0.0, atol=0.0, maxit=5)
+    assert nits == 5
+    s.close()
+
+
+def test_nonzero_initial_guess(gpu, oracle):
+    G = load_golden("p1_m5_kappa")
+    s = build(gpu, 1, G["verts"], G["elems"], G["e2l"], G["bdry"], G["f"], G["g"], G["kappa"])
+    x0 = np.linspace(0, 1, len(G["bdry"]))
+    xo, no, _, _ = oracle.pcg(G["rows_ptr"], G["rows_cols"], G["rows_vals"], G["diag"], G["rhs"],
+                              x0=x0, rtol=1e-10, btol=0.0, atol=0.0)
+    x, nits, _ = s.solve_pcg(x0=x0, rtol=1e-10, btol=0.0, atol=0.0)
+    assert abs(nits - no) <= 2
+    assert np.linalg.norm(x - xo) <= 1e-7 * np.linalg.norm(xo)
+    s.close()
+
+
+def test_breakdown_reported(gpu):
+    """p.Ap == 0 stops PCG as the reference does (solver-phg.c:561-571) and
+    comes back as PHG_GPU_ERR_BREAKDOWN."""
+    s = gpu.Solver(0)
+    s.set_matrix(np.array([0, 1, 2]), np.array([0, 1], np.int32), np.array([1.0, -1.0]),
+                 np.array([1.0, 1.0]))
+    with pytest.raises(gpu.PhgGpuError) as ei:
+        s.solve_pcg(rtol=1e-10)
+    assert ei.value.code == -5
+    s.close()
+
+
+def test_bad_index_reported(gpu):
+    G = load_golden("p1_m4_sine")
+    s = gpu.Solver(0)
+    s.set_mesh(G["verts"], G["elems"])
+    e2l = G["e2l"].copy()
+    e2l[3, 2] = len(G["bdry"]) + 7
+    with pytest.raises(gpu.PhgGpuError) as ei:
+        s.set_dof_map(1, e2l, G["bdry"])
+    assert ei.value.code == -1
+    # the system stays usable
+    s.set_dof_map(1, G["e2l"], G["bdry"])
+    s.build_linear_system(f=G["f"], g=G["g"])
+    assert np.array_equal(s.get_rhs(), G["rhs"])
+    s.close()
+
+
+def test_zero_rhs_gives_zero(gpu):
+    G = load_golden("p2_m3_sine")
+    s = build(gpu, 2, G["verts"], G["elems"], G["e2l"], G["bdry"], np.zeros_like(G["f"]))
+    x, nits, res = s.solve_pcg(x0=np.ones(len(G["bdry"])))
+    assert nits == 0 and not x.any()
+    s.close()

@@ -1,0 +1,67 @@
+"""Pins the CPU oracle (oracle/phg_oracle.c) against outputs of the
+unmodified reference built from its sources (tests/golden/, generated by
+tests/golden/make_golden.py).  Everything is compared bit for bit."""
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden, GOLDEN
+
+
+def test_quadrature_rules_bitexact(oracle):
+    z = np.load(GOLDEN + "/quad_rules.npz")
+    for order in range(7):
+        ref = z["order%d" % order]
+        pts, wts = oracle.quad_rule(order)
+        assert np.array_equal(pts, ref[:, :4]), order
+        assert np.array_equal(wts, ref[:, 4]), order
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_assembly_bitexact(oracle, name):
+    G = load_golden(name)
+    o = oracle.assemble(int(G["order"]), G["verts"], G["elems"], G["e2l"], G["bdry"], G["f"],
+                        G["g"], G.get("kappa"))
+    for pre, op in (("rows_raw", "raw_"), ("rows", ""), ("bdry_rows", "b")):
+        assert np.array_equal(G[pre + "_ptr"], o[op + "ptr"]), pre
+        assert np.array_equal(G[pre + "_cols"], o[op + "cols"]), pre
+        assert np.array_equal(G[pre + "_vals"], o[op + "vals"]), pre
+    for k in ("rhs_raw", "rhs", "diag"):
+        assert np.array_equal(G[k], o[k]), k
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_pcg_bitexact(oracle, name):
+    G = load_golden(name)
+    x, nits, res, hist = oracle.pcg(G["rows_ptr"], G["rows_cols"], G["rows_vals"], G["diag"],
+                                    G["rhs"], rtol=float(G["rtol"]), btol=0.0, atol=0.0)
+    assert nits == int(G["nits"])
+    assert res == float(G["residual"])
+    assert np.array_equal(x, G["x"])
+    assert hist[-1] == res and len(hist) == nits + 1
+
+
+def test_linear_solution_reproduced():
+    """u = x + y + z lies in every P_k space (examples/functions.h:34-42,
+    TEST_CASE 1): the reference's discrete solution equals it at the nodes up
+    to the solver tolerance."""
+    import phg_b200 as pb
+    G = load_golden("p3_m3_linear")
+    e2l, bdry, nodes = pb.lagrange_dofs(G["verts"], G["elems"], 3)
+    perm = np.empty(len(bdry), np.int64)
+    perm[G["e2l"].ravel()] = e2l.ravel()
+    u = nodes[perm].sum(axis=1)
+    assert np.max(np.abs(G["x"] - u)) < 1e-7
+    b = G["bdry"].astype(bool)
+    assert np.allclose(G["g"][b], u[b], rtol=0, atol=1e-15)
+
+
+def test_zero_drop_pattern_is_value_dependent():
+    """With non-dyadic coordinates (m = 5) rounding leaves tiny non-zero
+    element entries that the reference keeps: the P1 pattern is wider than
+    the exact-arithmetic 7-point stencil, so a pattern built from exact
+    arithmetic would not match."""
+    G = load_golden("p1_m5_kappa")
+    ptr = G["rows_ptr"]
+    interior = np.flatnonzero(G["bdry"] == 0)
+    lens = ptr[interior + 1] - ptr[interior]
+    assert lens.max() > 7
