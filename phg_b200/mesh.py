@@ -20,7 +20,12 @@ def kuhn_cube(m):
 
     Vertex (i, j, k) has index i + (m+1) (j + (m+1) k) and coordinates
     (i/m, j/m, k/m).  Subcubes are visited with i fastest; each contributes
-    6 tetrahedra in PERMS order, vertices ordered along the walk.
+    6 tetrahedra in PERMS order.  A tetrahedron walking w0 -> w1 -> w2 -> w3
+    from the subcube's low corner to its high corner is stored as
+    (w0, w3, w2, w1): the main diagonal first, which is the vertex order the
+    reference's refinement setup gives these elements after import (it keeps
+    this order unchanged), so the element Jacobians -- and the exact zeros of
+    the element matrices -- are the reference's.
     """
     m = int(m)
     n1 = m + 1
@@ -41,7 +46,7 @@ def kuhn_cube(m):
         for s in range(3):
             pos[:, perm[s]] += 1
             elems[:, p, s + 1] = pos @ stride
-    return verts, elems.reshape(-1, 4).astype(np.int32)
+    return verts, elems[:, :, [0, 3, 2, 1]].reshape(-1, 4).astype(np.int32)
 
 
 def write_medit(path, verts, elems):
