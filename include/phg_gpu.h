@@ -127,6 +127,28 @@ int phgGpuSolverPCG(phgGpuSystem *sys, double rtol, double btol,
  * profiling. */
 int phgGpuGetLaunchCount(phgGpuSystem *sys, int64_t *count);
 
+/* Jacobi-PCG on a CSR matrix in device memory, allocating no memory (no
+ * counterpart in the reference; the same iteration as phgGpuSolverPCG).
+ * For callers that cannot allocate device memory -- an application whose
+ * own pool has reserved the GPU, or a plugin in a process whose device
+ * memory another runtime owns.  The working vectors live in a fixed array
+ * that is part of the library (about 9 MB held on every GPU that loads the
+ * library, until the process exits), which limits n to
+ * PHG_GPU_NOALLOC_MAX_ROWS (larger n: PHG_GPU_ERR_LIMIT).  ptr (int64,
+ * n + 1), cols, vals, rhs and x (initial guess in, solution out) must be
+ * device memory of the current device; work runs on `stream`
+ * (cudaStream_t, NULL = default stream) and the call returns when it is
+ * done.  The first call on a device looks up the array's device address;
+ * make that first call before any stream capture.  All calls share the one
+ * array, so calls that overlap on the GPU (other host threads, other
+ * streams) race: serialise them.  Returns the iteration count or a negative
+ * error code. */
+#define PHG_GPU_NOALLOC_MAX_ROWS 262144
+int phgGpuSolverPCGNoAlloc(int64_t n, const int64_t *ptr, const int32_t *cols,
+			   const double *vals, const double *rhs, double *x,
+			   double rtol, double btol, double atol, int maxit,
+			   void *stream, double *residual);
+
 #ifdef __cplusplus
 }
 #endif

@@ -39,7 +39,11 @@ SIGNATURES = {
     "phgGpuSolverPCG": (C.c_int, [_P, C.c_double, C.c_double, C.c_double, C.c_int, _P,
                                   C.POINTER(C.c_double), _P]),
     "phgGpuGetLaunchCount": (C.c_int, [_P, C.POINTER(_I64)]),
+    "phgGpuSolverPCGNoAlloc": (C.c_int, [_I64, _P, _P, _P, _P, _P, C.c_double, C.c_double,
+                                         C.c_double, C.c_int, _P, C.POINTER(C.c_double)]),
 }
+
+NOALLOC_MAX_ROWS = 262144
 
 _LIB = None
 
@@ -195,3 +199,16 @@ class Solver:
         if history:
             return x, nits, res.value, hist[:nits + 1]
         return x, nits, res.value
+
+
+def solve_pcg_no_alloc(ptr, cols, vals, rhs, x, rtol=1e-10, btol=1e-10, atol=0.0, maxit=10000,
+                       stream=None):
+    """phgGpuSolverPCGNoAlloc: Jacobi-PCG on a CSR matrix held in device
+    memory (torch CUDA tensors: ptr int64, cols int32, vals/rhs/x float64),
+    without allocating any memory -- for callers that cannot allocate.  x is
+    the initial guess and receives the solution.  Returns (nits, residual)."""
+    res = C.c_double()
+    nits = _check(lib().phgGpuSolverPCGNoAlloc(len(ptr) - 1, _ptr(ptr), _ptr(cols), _ptr(vals),
+                                               _ptr(rhs), _ptr(x), rtol, btol, atol, int(maxit),
+                                               stream, C.byref(res)))
+    return nits, res.value

@@ -107,6 +107,11 @@ constexpr int kGraphChunk = 16;
 
 }  // namespace
 
+namespace phgb {
+// Lets other translation units of the library report through phgGpuLastError().
+void set_last_error(const char *msg) { g_last_error = msg; }
+}  // namespace phgb
+
 struct phgGpuSystem_ {
     int device = 0;
     cudaStream_t stream = nullptr;
