@@ -8,9 +8,11 @@ faces; element assembly into CSR (order-2 stiffness rule, order-4 RHS rule),
 boundary elimination, then Jacobi-PCG from x = 0 to relative residual 1e-8.
 Inputs are synthetic (generated here), not a dataset.
 
-Metric: time to tolerance of one step in ms (lower is better).
+Metric: time to tolerance of one step in ms (lower is better), with the
+mixed-precision solver (FP32 inner PCG, FP64 reliable updates; the FP64
+residual meets the tolerance); the plain FP64 step is timed beside it.
   value  inputs already resident in HBM (mesh, element->DOF map, Dirichlet
-         flags, f): SetMesh + SetDofMap + BuildLinearSystem + SolverPCG.
+         flags, f): SetMesh + SetDofMap + BuildLinearSystem + SolverPCGMixed.
   e2e    the same calls with HOST (pinned) input buffers: the host->device
          copies of the inputs and the device->host copy of the solution are
          inside the timed region.
@@ -215,20 +217,28 @@ def impl_ours(args):
     host = {"verts": v, "elems": e, "e2l": e2l, "bdry": bdry, "f": f}
     pinned = {k: torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for k, a in host.items()}
     d = {k: t.to(dev) for k, t in pinned.items()}
-    x_dev = torch.zeros(ndof, dtype=torch.float64, device=dev)
+    x_mixed = torch.zeros(ndof, dtype=torch.float64, device=dev)
+    x_fp64 = torch.zeros(ndof, dtype=torch.float64, device=dev)
     x_host = torch.zeros(ndof, dtype=torch.float64).pin_memory()
     rtol = 1e-8
 
     stream = torch.cuda.Stream(dev)
     s = pb.Solver(local, stream.cuda_stream)
 
-    def step(inp, x):
+    def assemble(inp):
         s.set_mesh(inp["verts"], inp["elems"])
         s.set_dof_map(p, inp["e2l"], inp["bdry"])
         s.build_linear_system(f=inp["f"])
+
+    def step(inp, x, mixed):
+        assemble(inp)
         x.zero_()
-        _, nits, res = s.solve_pcg(out=x, rtol=rtol, btol=0.0, atol=0.0)
-        return nits, res
+        if mixed:
+            _, nits, res, nupd = s.solve_pcg_mixed(out=x, rtol=rtol, btol=0.0, atol=0.0)
+        else:
+            _, nits, res = s.solve_pcg(out=x, rtol=rtol, btol=0.0, atol=0.0)
+            nupd = 0
+        return nits, res, nupd
 
     def barrier():
         if dist is not None:
@@ -241,7 +251,7 @@ def impl_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    def timed(inp, x, k):
+    def timed(inp, x, k, mixed):
         barrier()
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -249,34 +259,35 @@ def impl_ours(args):
         with torch.cuda.stream(stream):
             a.record(stream)
             for _ in range(k):
-                out = step(inp, x)
+                out = step(inp, x, mixed)
             b.record(stream)
         torch.cuda.synchronize()
         barrier()
-        return a.elapsed_time(b) / k, out, s.launch_count() - l0
+        return max_over_ranks(a.elapsed_time(b) / k), out, s.launch_count() - l0
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
-            step(d, x_dev)
+            step(d, x_mixed, True)
+            step(d, x_fp64, False)
     clocks = ClockSampler(local)
     clocks.start()
-    ms, (nits, res), launches = timed(d, x_dev, args.steps)
+    ms, (nits, res, nupd), launches = timed(d, x_mixed, args.steps, True)
+    ms64, (nits64, res64, _), _ = timed(d, x_fp64, args.steps, False)
     clock_info = clocks.stop()
-    ms = max_over_ranks(ms)
 
-    # end to end through the C ABI with host buffers
+    # end to end through the C ABI with host buffers (mixed path)
     with torch.cuda.stream(stream):
-        step(pinned, x_host)
-    e2e_ms, _, _ = timed(pinned, x_host, max(1, args.steps))
-    e2e_ms = max_over_ranks(e2e_ms)
+        step(pinned, x_host, True)
+    e2e_ms, _, _ = timed(pinned, x_host, max(1, args.steps), True)
     h2d = sum(t.numel() * t.element_size() for t in pinned.values())
     d2h = x_host.numel() * x_host.element_size()
 
-    # accuracy of the solution against the exact sine solution (discretisation)
+    # accuracy: mixed vs FP64 solution, both vs the exact sine solution
+    xm, x64 = x_mixed.cpu().numpy(), x_fp64.cpu().numpy()
     u = np.sin(np.pi * nodes[:, 0]) * np.sin(np.pi * nodes[:, 1]) * np.sin(np.pi * nodes[:, 2])
-    err = float(np.max(np.abs(x_dev.cpu().numpy() - u)))
+    rel_l2_vs_fp64 = float(np.linalg.norm(xm - x64) / np.linalg.norm(x64))
 
-    # phase breakdown of one step
+    # phase breakdown of one mixed step
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
     with torch.cuda.stream(stream):
         ev[0].record(stream)
@@ -286,54 +297,48 @@ def impl_ours(args):
         ev[2].record(stream)
         s.build_linear_system(f=d["f"])
         ev[3].record(stream)
-        x_dev.zero_()
-        s.solve_pcg(out=x_dev, rtol=rtol, btol=0.0, atol=0.0)
+        x_mixed.zero_()
+        s.solve_pcg_mixed(out=x_mixed, rtol=rtol, btol=0.0, atol=0.0)
         ev[4].record(stream)
     torch.cuda.synchronize()
     phases = [ev[i].elapsed_time(ev[i + 1]) for i in range(4)]
     n, nnz, _ = s.sizes()
+    layout, param, tune = s.spmv_plan()
 
-    # dominant kernel: the CSR SpMV, timed alone on the launching stream
-    xs = torch.randn(n, dtype=torch.float64, device=dev)
-    ys = torch.empty_like(xs)
-    reps = 50
-    with torch.cuda.stream(stream):
-        for _ in range(5):
-            s.mat_vec(xs, ys)
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        for _ in range(reps):
-            s.mat_vec(xs, ys)
-        b.record(stream)
-    torch.cuda.synchronize()
-    spmv_ms = a.elapsed_time(b) / reps
-    spmv_bytes = 12 * nnz + 4 * (n + 1) + 16 * n
+    # the dominant kernels, timed alone on the launching stream
+    spmv32_ms = s.time_spmv(fp32=True, reps=50)
+    spmv64_ms = s.time_spmv(fp32=False, reps=50)
+    b32 = 8 * nnz + 4 * (n + 1) + 8 * n
+    b64 = 12 * nnz + 4 * (n + 1) + 16 * n
     peak, peak_kind = measured_hbm_peak()
-    achieved = spmv_bytes / (spmv_ms * 1e-3) / 1e9
-    # per PCG iteration: SpMV + 88 bytes/row of vector traffic
-    it_bytes = spmv_bytes + 88 * n
-    solve_ms = phases[3]
+    ach32 = b32 / (spmv32_ms * 1e-3) / 1e9
+    ach64 = b64 / (spmv64_ms * 1e-3) / 1e9
 
     line = {
         "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
-        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64",
         "data": "synthetic", "config": dict(workload(m), parallelism="replicas x%d" % world,
-                                            path="fp64"),
+                                            path="mixed: FP32 inner PCG, FP64 reliable updates"),
         "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
-        "roofline": {"bound": "hbm", "kernel": "spmv_kernel (CSR, fp64)", "achieved": round(achieved, 1),
-                     "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": committed_traffic("spmv_p2_m64_fp64"),
-                     "algorithmic_bytes": int(spmv_bytes), "launch_ms": round(spmv_ms, 5)},
+        "roofline": {"bound": "hbm", "kernel": "sell_spmv_kernel<float> (unroll %d)" % tune.get("fp32_unroll", 0),
+                     "achieved": round(ach32, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": round(ach32 / peak, 4), "traffic": committed_traffic("spmv32_p2_m64"),
+                     "algorithmic_bytes": int(b32), "launch_ms": round(spmv32_ms, 5)},
+        "fp64": {"ms": round(ms64, 3), "mixed_over_fp64": round(ms / ms64, 4), "nits": int(nits64),
+                 "spmv_ms": round(spmv64_ms, 5), "spmv_gbs": round(ach64, 1),
+                 "spmv_frac": round(ach64 / peak, 4), "traffic": committed_traffic("spmv64_p2_m64")},
         "gpu_launches": int(launches),
         "clocks": clock_info,
-        "pcg": {"nits": int(nits), "residual": res, "max_err_vs_exact": err,
-                "ms_per_iteration": round(solve_ms / max(nits, 1), 4),
-                "iteration_gbs": round(it_bytes * nits / (solve_ms * 1e-3) / 1e9, 1)},
+        "pcg": {"nits": int(nits), "reliable_updates": int(nupd), "residual_fp64": res,
+                "rel_l2_vs_fp64_solution": rel_l2_vs_fp64,
+                "max_err_vs_exact": float(np.max(np.abs(xm - u))),
+                "fp64_max_err_vs_exact": float(np.max(np.abs(x64 - u)))},
         "phases_ms": {"set_mesh": round(phases[0], 3), "set_dof_map": round(phases[1], 3),
-                      "assemble": round(phases[2], 3), "pcg": round(phases[3], 3)},
+                      "assemble": round(phases[2], 3), "pcg_mixed": round(phases[3], 3)},
         "assembly_melem_s": round(6 * m ** 3 / (phases[2] * 1e-3) / 1e6, 1),
+        "spmv_autotune_ms": {k: round(v, 5) for k, v in tune.items()},
         "n": int(n), "nnz": int(nnz),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -344,7 +349,7 @@ def impl_ours(args):
                 "value": round(reference_step_ms(r0, r0["nits"]), 1), "unit": "ms",
                 "cores": r0["threads"], "kind": "reference",
                 "sample": "the full workload once: reference OpenMP build (oracle/_ref/phg_dump_omp), "
-                          "element loop + phgSolverAssemble + PCG (%d its)" % r0["nits"]}
+                          "element loop + phgSolverAssemble + FP64 PCG (%d its)" % r0["nits"]}
         except Exception as ex:  # report, never fail the GPU measurement
             line["cpu_baseline"] = {"value": None, "unit": "ms", "cores": os.cpu_count(),
                                     "kind": "reference", "sample": "failed: %s" % ex}

@@ -122,6 +122,74 @@ int phgGpuSolverPCG(phgGpuSystem *sys, double rtol, double btol,
 		    double atol, int maxit, double *x, double *residual,
 		    double *hist);
 
+/* Jacobi-PCG for many right-hand sides at once: column k of B (n x nrhs,
+ * row major: B[i * nrhs + k]) is solved by its own PCG recurrence and
+ * stopping rule (rtol relative to ||b_k||, from x = 0), and the columns share
+ * one SpMM per iteration, so the matrix is read once per tile of columns.
+ * mixed = 0: FP64; mixed = 1: FP32 matrix values, vectors and SpMM with FP64
+ * reliable updates (as phgGpuSolverPCGMixed).  X (n x nrhs, row major) gets
+ * the solutions, nits[k] (optional) the iterations, res[k] (optional)
+ * ||b_k - A x_k||_2 in FP64.  At most 64 columns per call.  The SpMM tile
+ * width (8/16/32/64 columns, which fixes the rows per warp) is autotuned at
+ * the first call for a shape.  Extends the reference (its PCG takes one
+ * vector, solver-phg.c:495). */
+int phgGpuSolverBlockPCG(phgGpuSystem *sys, int nrhs, const double *B,
+			 double *X, double rtol, int maxit, int mixed,
+			 int *nits, double *res);
+/* The SpMM tile chosen for the last block solve and the measured time of
+ * each candidate (8, 16, 32, 64 columns; 0 when not tried). */
+int phgGpuGetBlockTile(phgGpuSystem *sys, int *tile, double *times_ms);
+
+/* Adjoint gradient of J = 1/2 ||u - u_obs||_2^2 (sum over all DOFs) with
+ * respect to log kappa_e for every element, for the system last built by
+ * phgGpuBuildLinearSystem (its kappa): solves A lambda = u - u_obs on the
+ * free DOFs (lambda = 0 on Dirichlet DOFs) with the FP64 PCG to relative
+ * residual rtol, then grad[e] = -kappa_e lambda_e^T K_e^0 u_e.  u is the
+ * solution of that system (n), u_obs the data (n); grad gets nelem values;
+ * *J (optional) the functional, *nits (optional) the adjoint iterations.
+ * No counterpart in the reference (it has no derivatives). */
+int phgGpuAdjointGradient(phgGpuSystem *sys, const double *u,
+			  const double *u_obs, double rtol, int maxit,
+			  double *grad, double *J, int *nits);
+
+/* Mixed-precision Jacobi-PCG on the assembled system: FP32 matrix values,
+ * Krylov vectors and SpMV with FP64-accumulated dot products, inside FP64
+ * refinement -- the FP64 solution x and FP64 residual b - A x are updated
+ * ("reliable updates") whenever the FP32 residual has fallen tenfold, and the
+ * search direction is kept across updates, so the iteration converges like
+ * the FP64 one.  The stopping rule is the reference's (get_tol,
+ * src/solver-phg.c:104, on the initial residual) applied to the FP64
+ * residual; on return *residual is ||b - A x||_2 computed in FP64.  Extends
+ * the reference (its FLOAT is fixed at build time, configure.in:627-671).
+ * Returns the number of FP32 iterations or a negative error code;
+ * *nupdates gets the number of reliable updates. */
+int phgGpuSolverPCGMixed(phgGpuSystem *sys, double rtol, double btol,
+			 double atol, int maxit, double *x, double *residual,
+			 int *nupdates);
+
+/* The SpMV layout the autotuner chose for the current matrix (no
+ * counterpart in the reference): at the first solve or product for a matrix
+ * shape it times CSR with 4/8/16/32 lanes per row and SELL-C-sigma (32-row
+ * slices, rows sorted by length in 256-row windows) with 2/4/8-fold
+ * unrolling, and keeps the fastest.  kind: 0 = CSR (param = lanes per row),
+ * 1 = SELL (param = unroll); times_ms (optional, 11 doubles) gets the
+ * measured time of each candidate in that order, then the times of the FP32
+ * SELL product (mixed solver) unrolled 4/8/16 times and the unroll chosen
+ * for it (0 before a mixed solve).  Returns the number of FP64 candidates. */
+int phgGpuGetSpMVPlan(phgGpuSystem *sys, int *kind, int *param,
+		      double *times_ms);
+
+/* Average device time of one SpMV with the chosen layout, FP64 values
+ * (fp32 = 0) or the FP32 values of the mixed solver (fp32 = 1), over `reps`
+ * back-to-back launches on the system's stream (no counterpart in the
+ * reference; used to report the SpMV roofline). */
+int phgGpuTimeSpMV(phgGpuSystem *sys, int fp32, int reps, double *ms_per_launch);
+
+/* Overrides the autotuner for the current matrix shape: kind 0 = CSR with
+ * param = 4/8/16/32 lanes per row, kind 1 = SELL with param = 2/4/8
+ * (no counterpart in the reference). */
+int phgGpuSetSpMVPlan(phgGpuSystem *sys, int kind, int param);
+
 /* Number of kernels this system has launched so far (the nodes of captured
  * PCG graphs included): no counterpart in the reference, an aid for
  * profiling. */

@@ -39,6 +39,15 @@ SIGNATURES = {
     "phgGpuSolverPCG": (C.c_int, [_P, C.c_double, C.c_double, C.c_double, C.c_int, _P,
                                   C.POINTER(C.c_double), _P]),
     "phgGpuGetLaunchCount": (C.c_int, [_P, C.POINTER(_I64)]),
+    "phgGpuGetSpMVPlan": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), _P]),
+    "phgGpuSetSpMVPlan": (C.c_int, [_P, C.c_int, C.c_int]),
+    "phgGpuSolverBlockPCG": (C.c_int, [_P, C.c_int, _P, _P, C.c_double, C.c_int, C.c_int, _P, _P]),
+    "phgGpuGetBlockTile": (C.c_int, [_P, C.POINTER(C.c_int), _P]),
+    "phgGpuAdjointGradient": (C.c_int, [_P, _P, _P, C.c_double, C.c_int, _P, C.POINTER(C.c_double),
+                                        C.POINTER(C.c_int)]),
+    "phgGpuTimeSpMV": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_double)]),
+    "phgGpuSolverPCGMixed": (C.c_int, [_P, C.c_double, C.c_double, C.c_double, C.c_int, _P,
+                                       C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     "phgGpuSolverPCGNoAlloc": (C.c_int, [_I64, _P, _P, _P, _P, _P, C.c_double, C.c_double,
                                          C.c_double, C.c_int, _P, C.POINTER(C.c_double)]),
 }
@@ -130,6 +139,7 @@ class Solver:
 
     def set_mesh(self, verts, elems):
         verts, elems = _np(verts, np.float64), _np(elems, np.int32)
+        self.nelem = len(elems)
         _check(lib().phgGpuSetMesh(self._h, len(verts), _ptr(verts), len(elems), _ptr(elems)))
 
     def set_dof_map(self, order, e2l, bdry):
@@ -178,6 +188,71 @@ class Solver:
             y = np.empty(self.sizes()[0])
         _check(lib().phgGpuMatVec(self._h, _ptr(x), _ptr(y)))
         return y
+
+    def solve_pcg_mixed(self, x0=None, rtol=1e-8, btol=0.0, atol=0.0, maxit=10000, out=None):
+        """FP32-inner / FP64-refinement Jacobi-PCG.  Returns
+        (x, nits, residual, reliable_updates); residual = ||b - A x|| in FP64."""
+        n = self.sizes()[0]
+        if out is not None:
+            x = out
+        else:
+            x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+        res, nupd = C.c_double(), C.c_int()
+        nits = _check(lib().phgGpuSolverPCGMixed(self._h, rtol, btol, atol, int(maxit), _ptr(x),
+                                                 C.byref(res), C.byref(nupd)))
+        return x, nits, res.value, nupd.value
+
+    SPMV_LAYOUTS = (("csr", 4), ("csr", 8), ("csr", 16), ("csr", 32),
+                    ("sell", 2), ("sell", 4), ("sell", 8))
+
+    def time_spmv(self, fp32=False, reps=50):
+        """Average ms of one SpMV launch (chosen layout; FP32 values if fp32)."""
+        ms = C.c_double()
+        _check(lib().phgGpuTimeSpMV(self._h, 1 if fp32 else 0, int(reps), C.byref(ms)))
+        return ms.value
+
+    def set_spmv_plan(self, layout, param):
+        _check(lib().phgGpuSetSpMVPlan(self._h, 0 if layout == "csr" else 1, int(param)))
+
+    def solve_block_pcg(self, B, rtol=1e-8, maxit=10000, mixed=False, out=None):
+        """Block PCG on the columns of B (n x nrhs).  Returns (X, nits[nrhs],
+        residuals[nrhs])."""
+        B = _np(B, np.float64)
+        n, nrhs = B.shape
+        X = np.empty((n, nrhs)) if out is None else out
+        nits = np.zeros(nrhs, np.int32)
+        res = np.zeros(nrhs)
+        _check(lib().phgGpuSolverBlockPCG(self._h, nrhs, _ptr(B), _ptr(X), rtol, int(maxit),
+                                          1 if mixed else 0, _ptr(nits), _ptr(res)))
+        return X, nits, res
+
+    def block_tile(self):
+        t = C.c_int()
+        times = np.zeros(4)
+        _check(lib().phgGpuGetBlockTile(self._h, C.byref(t), _ptr(times)))
+        return t.value, dict(zip((8, 16, 32, 64), times.tolist()))
+
+    def adjoint_gradient(self, u, u_obs, rtol=1e-10, maxit=100000, out=None):
+        """dJ/dlog kappa_e for J = 1/2 ||u - u_obs||^2, u the solution of the
+        last built system.  Returns (grad, J, adjoint iterations)."""
+        u, u_obs = _np(u, np.float64), _np(u_obs, np.float64)
+        if out is None:
+            out = np.empty(self.nelem)
+        J, nits = C.c_double(), C.c_int()
+        _check(lib().phgGpuAdjointGradient(self._h, _ptr(u), _ptr(u_obs), rtol, int(maxit), _ptr(out),
+                                           C.byref(J), C.byref(nits)))
+        return out, J.value, nits.value
+
+    def spmv_plan(self):
+        """(layout, parameter, {candidate: ms}) chosen by the SpMV autotuner."""
+        kind, param = C.c_int(), C.c_int()
+        times = np.zeros(16)
+        nc = _check(lib().phgGpuGetSpMVPlan(self._h, C.byref(kind), C.byref(param), _ptr(times)))
+        names = ["csr4", "csr8", "csr16", "csr32", "sell_u2", "sell_u4", "sell_u8"][:nc]
+        info = dict(zip(names, times[:nc].tolist()))
+        info.update({"fp32_sell_u4": times[nc], "fp32_sell_u8": times[nc + 1], "fp32_sell_u16": times[nc + 2],
+                     "fp32_unroll": int(times[nc + 3])})
+        return ("csr" if kind.value == 0 else "sell"), param.value, info
 
     def launch_count(self):
         c = _I64()

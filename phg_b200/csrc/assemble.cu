@@ -9,6 +9,7 @@
 //   inc_ptr i32 [ndof+1], inc i32    per DOF, the incident (element, basis)
 //                                    pairs as keys e*N+a, ascending
 //   Ke      f64 [nelem][N][N]        element matrices (row a = basis a)
+//   Km      u32 [nelem][ceil(N*N/32)] nonzero bits of Ke
 //   Re      f64 [nelem][N]           element right-hand sides
 //   ptr/cols/vals                    CSR (rows in first-touch order)
 //   bptr/bcols/bvals                 saved boundary columns
@@ -50,13 +51,12 @@ __device__ __forceinline__ void jacobian_vol(const double *x, double *J, double 
         // row swap, written as selects so the array stays in registers
 #pragma unroll
         for (int r = j + 1; r < 4; r++) {
-            if (r == k) {
+            const bool sw = (r == k);
 #pragma unroll
-                for (int i = j; i < 8; i++) {
-                    const double t = a[j][i];
-                    a[j][i] = a[r][i];
-                    a[r][i] = t;
-                }
+            for (int i = j; i < 8; i++) {
+                const double t = a[j][i], u = a[r][i];
+                a[j][i] = sw ? u : t;
+                a[r][i] = sw ? t : u;
             }
         }
         const double t = a[j][j];
@@ -95,64 +95,95 @@ __device__ __forceinline__ void jacobian_vol(const double *x, double *J, double 
 }
 
 // ---------------------------------------------------------------------------
-// Element kernel: one warp per element.
-//   Ke[e] = N x N stiffness: integral of grad phi_b . kappa grad phi_a with the
+// Element kernel.  A warp takes 32 elements at a time:
+//   phase A  one thread per element: vertex gather, Jacobian and volume
+//            (the long serial part), written to shared memory;
+//   phase B  the warp walks its 32 elements one by one, lanes spread over
+//            (basis, point) for the gradients and over basis pairs for the
+//            matrix, then a coalesced store of the N x N element matrix.
+// Outputs per element e:
+//   Ke[e]   N x N stiffness, integral of grad phi_b . kappa grad phi_a with the
 //           order-2(p-1) rule (phgQuadGradBasAGradBas, quad.c:5260-5344, basis
 //           gradients as phgQuadGetBasisGradient, quad.c:3314-3421)
-//   Re[e] = N right-hand side entries, integral of f_h phi_a with the order-2p
+//   Re[e]   N right-hand side entries, integral of f_h phi_a with the order-2p
 //           rule (phgQuadDofTimesBas, quad.c:5481-5530; f_h at the points as
 //           phgDofEval_, dof-utils.c:59-300)
+//   Km[e]   bit (a*N + b) set iff Ke[e][a][b] != 0 (the entries the reference's
+//           phgMatAddEntries_ keeps), read by the first row-walk pass
 template <int P>
 struct ElemDims {
     static constexpr int N = P == 1 ? 4 : P == 2 ? 10 : 20;
     static constexpr int QK = P == 1 ? 1 : P == 2 ? 4 : 14;
     static constexpr int QR = P == 1 ? 4 : P == 2 ? 14 : 24;
+    static constexpr int MW = (N * N + 31) / 32;          // mask words per element
+    static constexpr int WARPS = 4;                       // warps per block
 };
 
-constexpr int kElemWarps = 4;
+constexpr int kGeo = 18;   // doubles of geometry per element: J (16), volume, pad
 
+// Geometry: one thread per element, J (16) and the volume into geo[e][0..16].
+__global__ void __launch_bounds__(128)
+geometry_kernel(int64_t nelem, int64_t nvert, const double *__restrict__ verts, const int32_t *__restrict__ elems,
+                double *__restrict__ geo, int *status) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nelem; e += (int64_t)gridDim.x * blockDim.x) {
+        double x[12];
+        bool ok = true;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int32_t v = elems[4 * e + j];
+            if (v < 0 || v >= nvert) {
+                ok = false;
+                x[3 * j] = x[3 * j + 1] = x[3 * j + 2] = 0.0;
+            } else {
+                x[3 * j] = verts[3 * (int64_t)v];
+                x[3 * j + 1] = verts[3 * (int64_t)v + 1];
+                x[3 * j + 2] = verts[3 * (int64_t)v + 2];
+            }
+        }
+        if (!ok) atomicExch(status, PHGB_DEV_BAD_INDEX);
+        double J[16], vol;
+        jacobian_vol(x, J, vol);
+        double *o = geo + (size_t)e * kGeo;
+#pragma unroll
+        for (int t = 0; t < 16; t++) o[t] = J[t];
+        o[16] = vol;
+    }
+}
+
+// Element matrices and vectors: one warp per element.
 template <int P>
-__global__ void __launch_bounds__(kElemWarps * 32)
-element_kernel(int64_t nelem, int64_t nvert, int64_t ndof, const double *__restrict__ verts,
-               const int32_t *__restrict__ elems, const int32_t *__restrict__ e2l,
+__global__ void __launch_bounds__(ElemDims<P>::WARPS * 32)
+element_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, const int32_t *__restrict__ e2l,
                const double *__restrict__ kappa, const double *__restrict__ f,
                const double *__restrict__ wk, const double *__restrict__ gk,
                const double *__restrict__ wr, const double *__restrict__ br,
-               double *__restrict__ Ke, double *__restrict__ Re, int *status) {
+               double *__restrict__ Ke, double *__restrict__ Re, uint32_t *__restrict__ Km, int *status) {
     using D = ElemDims<P>;
-    constexpr int N = D::N, QK = D::QK, QR = D::QR;
-    __shared__ double s_grad[kElemWarps][N * QK * 3];
-    __shared__ double s_K[kElemWarps][N * N];
-    __shared__ double s_f[kElemWarps][N];
-    __shared__ double s_fq[kElemWarps][QR];
+    constexpr int N = D::N, QK = D::QK, QR = D::QR, MW = D::MW, W = D::WARPS;
+    __shared__ double s_geo[W][kGeo + 1];       // J (16), volume, kappa
+    __shared__ double s_grad[W][N * QK * 3];
+    __shared__ double s_K[W][N * N];
+    __shared__ double s_f[W][N];
+    __shared__ double s_fq[W][QR];
 
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    double *grad = s_grad[w], *K = s_K[w], *fl = s_f[w], *fq = s_fq[w];
+    double *J = s_geo[w], *grad = s_grad[w], *K = s_K[w], *fl = s_f[w], *fq = s_fq[w];
 
-    for (int64_t e = (int64_t)blockIdx.x * kElemWarps + w; e < nelem;
-         e += (int64_t)gridDim.x * kElemWarps) {
-        // vertex coordinates, broadcast to the whole warp
-        double cx = 0, cy = 0, cz = 0;
-        if (lane < 4) {
-            const int32_t v = elems[4 * e + lane];
-            if (v < 0 || v >= nvert) {
-                atomicExch(status, PHGB_DEV_BAD_INDEX);
-            } else {
-                cx = verts[3 * (int64_t)v];
-                cy = verts[3 * (int64_t)v + 1];
-                cz = verts[3 * (int64_t)v + 2];
+    for (int64_t e = (int64_t)blockIdx.x * W + w; e < nelem; e += (int64_t)gridDim.x * W) {
+        if (lane < 17) J[lane] = geo[(size_t)e * kGeo + lane];
+        if (lane == 17) J[17] = kappa != nullptr ? kappa[e] : 0.0;
+        // f_h at the element's nodes
+        if (lane < N) {
+            double fv = 0.0;
+            if (f != nullptr) {
+                const int32_t d = e2l[(size_t)e * N + lane];
+                if (d < 0 || d >= ndof) atomicExch(status, PHGB_DEV_BAD_INDEX);
+                else fv = f[d];
             }
+            fl[lane] = fv;
         }
-        double x[12];
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            x[3 * j] = __shfl_sync(0xffffffffu, cx, j);
-            x[3 * j + 1] = __shfl_sync(0xffffffffu, cy, j);
-            x[3 * j + 2] = __shfl_sync(0xffffffffu, cz, j);
-        }
-        double J[16], vol;
-        jacobian_vol(x, J, vol);
-        const double kap = kappa != nullptr ? kappa[e] : 0.0;
+        __syncwarp();
+        const double vol = J[16], kap = J[17];
 
         // basis gradients at the stiffness points: grad[(k*QK + q)*3 + c]
         for (int idx = lane; idx < N * QK; idx += 32) {
@@ -170,10 +201,14 @@ element_kernel(int64_t nelem, int64_t nvert, int64_t ndof, const double *__restr
                 const double g0 = G[0], g1 = G[1], g2 = G[2], g3 = G[3];
 #pragma unroll
                 for (int c = 0; c < 3; c++)
-                    o[c] = rn_add(rn_add(rn_add(rn_mul(g0, J[c]), rn_mul(g1, J[4 + c])),
-                                     rn_mul(g2, J[8 + c])),
-                                rn_mul(g3, J[12 + c]));
+                    o[c] = rn_add(rn_add(rn_add(rn_mul(g0, J[c]), rn_mul(g1, J[4 + c])), rn_mul(g2, J[8 + c])),
+                                  rn_mul(g3, J[12 + c]));
             }
+        }
+        for (int q = lane; q < QR; q += 32) {
+            double v = 0.0;
+            for (int k = 0; k < N; k++) v = rn_add(v, rn_mul(br[q * N + k], fl[k]));
+            fq[q] = v;
         }
         __syncwarp();
 
@@ -189,7 +224,7 @@ element_kernel(int64_t nelem, int64_t nvert, int64_t ndof, const double *__restr
                 const double *g1 = grad + 3 * (b * QK + q);
                 const double *g2 = grad + 3 * (a * QK + q);
                 const double d0 = rn_add(0., rn_add(rn_add(rn_mul(g1[0], g2[0]), rn_mul(g1[1], g2[1])),
-                                                rn_mul(g1[2], g2[2])));
+                                                    rn_mul(g1[2], g2[2])));
                 const double t = rn_mul(d0, wk[q]);
                 d = rn_add(d, kappa != nullptr ? rn_mul(t, kap) : t);
             }
@@ -197,31 +232,21 @@ element_kernel(int64_t nelem, int64_t nvert, int64_t ndof, const double *__restr
             K[a * N + b] = v;
             K[b * N + a] = v;
         }
-        __syncwarp();
-        double *ke = Ke + (size_t)e * N * N;
-        for (int t = lane; t < N * N; t += 32) ke[t] = K[t];
-
-        // right-hand side
-        if (lane < N) {
-            double fv = 0.0;
-            if (f != nullptr) {
-                const int32_t d = e2l[(size_t)e * N + lane];
-                if (d < 0 || d >= ndof) atomicExch(status, PHGB_DEV_BAD_INDEX);
-                else fv = f[d];
-            }
-            fl[lane] = fv;
-        }
-        __syncwarp();
-        for (int q = lane; q < QR; q += 32) {
-            double v = 0.0;
-            for (int k = 0; k < N; k++) v = rn_add(v, rn_mul(br[q * N + k], fl[k]));
-            fq[q] = v;
-        }
-        __syncwarp();
         if (lane < N) {
             double d = 0.0;
             for (int q = 0; q < QR; q++) d = rn_add(d, rn_mul(rn_mul(br[q * N + lane], wr[q]), fq[q]));
             Re[(size_t)e * N + lane] = rn_mul(d, vol);
+        }
+        __syncwarp();
+        double *ke = Ke + (size_t)e * N * N;
+        for (int t = lane; t < N * N; t += 32) ke[t] = K[t];
+        if (lane < MW) {
+            uint32_t m = 0;
+            for (int bit = 0; bit < 32; bit++) {
+                const int t = lane * 32 + bit;
+                if (t < N * N && K[t] != 0.0) m |= 1u << bit;
+            }
+            Km[(size_t)e * MW + lane] = m;
         }
         __syncwarp();
     }
@@ -316,18 +341,24 @@ __global__ void scan_add_kernel(int64_t n, int32_t *__restrict__ out, const int6
 }
 
 // ---------------------------------------------------------------------------
-// Row walk: one warp per row.  For an interior row the warp visits the row's
-// incidences in element order; lane j handles element column j, skips exact
-// zeros (phgMatAddEntries_, matvec.c:5459-5461), finds or appends the column
-// (add_columns_to_row, matvec.c:3286-3321: first-touch order) through a
-// per-warp open-addressing table in shared memory, and (pass 2) accumulates
-// the value.  Boundary columns are then separated from the row as
-// save_bdry_columns does (matvec.c:4430-4488) and lifted into the RHS as
-// update_rhs does (solver.c:707-725).  A Dirichlet row is the sum of the unit
-// rows of its elements (phgDofDirichletBC, dof-utils.c:1369-1392).
-template <int N, int HS>
+// Row walk: G lanes per row (G >= N; 32/G rows per warp side by side).  For an
+// interior row the lane group visits the row's incidences in element order;
+// lane j handles element column j, skips exact zeros (phgMatAddEntries_,
+// matvec.c:5459-5461), finds or appends the column (add_columns_to_row,
+// matvec.c:3286-3321: first-touch order) through the group's open-addressing
+// table in shared memory, and (pass 2) accumulates the value.  Boundary
+// columns are then separated from the row as save_bdry_columns does
+// (matvec.c:4430-4488) and lifted into the RHS as update_rhs does
+// (solver.c:707-725).  A Dirichlet row is the sum of the unit rows of its
+// elements (phgDofDirichletBC, dof-utils.c:1369-1392).  The next incidence's
+// loads are issued before the current one is processed.
+template <int N>
 struct WalkCfg {
+    static constexpr int G = N <= 8 ? 8 : N <= 16 ? 16 : 32;   // lanes per row
+    static constexpr int R = 32 / G;                            // rows per warp
+    static constexpr int HS = N == 4 ? 128 : N == 10 ? 256 : 512;
     static constexpr int MAXROW = HS / 2;
+    static constexpr int MW = (N * N + 31) / 32;
     static constexpr int WARPS = 4;
 };
 
@@ -343,70 +374,100 @@ __device__ __forceinline__ double bdry_rhs(const double *g, int32_t k, int mult)
     return s;
 }
 
-template <int N, int HS, bool PASS2>
-__global__ void __launch_bounds__(WalkCfg<N, HS>::WARPS * 32)
+template <int N, bool PASS2>
+__global__ void __launch_bounds__(WalkCfg<N>::WARPS * 32)
 row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t *__restrict__ inc,
                 const int32_t *__restrict__ e2l, const uint8_t *__restrict__ bdry,
-                const double *__restrict__ Ke, const double *__restrict__ Re,
+                const double *__restrict__ Ke, const uint32_t *__restrict__ Km, const double *__restrict__ Re,
                 const double *__restrict__ g,
-                // pass 1 outputs
                 int32_t *__restrict__ cnt_keep, int32_t *__restrict__ cnt_bdry,
-                // pass 2 inputs / outputs
                 const int32_t *__restrict__ ptr, int32_t *__restrict__ cols, double *__restrict__ vals,
                 const int32_t *__restrict__ bptr, int32_t *__restrict__ bcols, double *__restrict__ bvals,
                 double *__restrict__ rhs, double *__restrict__ diag, int *status) {
-    using C = WalkCfg<N, HS>;
-    constexpr int MAXROW = C::MAXROW;
-    __shared__ int32_t s_key[C::WARPS][HS];
-    __shared__ int16_t s_pos[C::WARPS][HS];
-    __shared__ int32_t s_col[C::WARPS][PASS2 ? MAXROW : 1];
-    __shared__ double s_val[C::WARPS][PASS2 ? MAXROW : 1];
+    using C = WalkCfg<N>;
+    constexpr int G = C::G, R = C::R, HS = C::HS, MAXROW = C::MAXROW, MW = C::MW, W = C::WARPS;
+    __shared__ int32_t s_key[W][R][HS];
+    __shared__ int16_t s_pos[W][R][HS];
+    __shared__ int32_t s_col[W][R][PASS2 ? MAXROW : 1];
+    __shared__ double s_val[W][R][PASS2 ? MAXROW : 1];
+    __shared__ double s_lift[W][R][PASS2 ? MAXROW : 1];
 
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int grp = lane / G, gl = lane % G;
+    const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (grp * G);
     const unsigned lt_mask = (1u << lane) - 1u;
-    int32_t *key = s_key[w];
-    int16_t *hpos = s_pos[w];
+    int32_t *key = s_key[w][grp];
+    int16_t *hpos = s_pos[w][grp];
+    int32_t *scol = s_col[w][grp];
+    double *sval = s_val[w][grp];
+    double *slift = s_lift[w][grp];
 
-    for (int64_t d = (int64_t)blockIdx.x * C::WARPS + w; d < ndof; d += (int64_t)gridDim.x * C::WARPS) {
-        const int32_t i0 = inc_ptr[d], i1 = inc_ptr[d + 1];
-        if (bdry[d]) {
-            if (lane == 0) {
-                const int mult = i1 - i0;
-                if (!PASS2) {
-                    cnt_keep[d] = mult > 0 ? 1 : 0;
-                    cnt_bdry[d] = mult > 0 ? 1 : 0;
-                } else {
-                    double m = 0.0;
-                    for (int i = 0; i < mult; i++) m = rn_add(m, 1.0);
-                    if (mult > 0) {
-                        cols[ptr[d]] = (int32_t)d;
-                        vals[ptr[d]] = m;
-                        bcols[bptr[d]] = (int32_t)d;
-                        bvals[bptr[d]] = m;
-                    }
-                    diag[d] = m;
-                    rhs[d] = bdry_rhs(g, (int32_t)d, mult);
-                }
-            }
-            continue;
+    const int64_t nwarps = (int64_t)gridDim.x * W;
+    for (int64_t wb = ((int64_t)blockIdx.x * W + w) * R; wb < ndof; wb += nwarps * R) {
+        const int64_t d = wb + grp;
+        const bool active = d < ndof;
+        int32_t i0 = 0, i1 = 0;
+        bool isb = false;
+        if (active) {
+            i0 = inc_ptr[d];
+            i1 = inc_ptr[d + 1];
+            isb = bdry[d] != 0;
         }
+        if (active && isb && gl == 0) {
+            const int mult = i1 - i0;
+            if (!PASS2) {
+                cnt_keep[d] = mult > 0 ? 1 : 0;
+                cnt_bdry[d] = mult > 0 ? 1 : 0;
+            } else {
+                double m = 0.0;
+                for (int i = 0; i < mult; i++) m = rn_add(m, 1.0);
+                if (mult > 0) {
+                    cols[ptr[d]] = (int32_t)d;
+                    vals[ptr[d]] = m;
+                    bcols[bptr[d]] = (int32_t)d;
+                    bvals[bptr[d]] = m;
+                }
+                diag[d] = m;
+                rhs[d] = bdry_rhs(g, (int32_t)d, mult);
+            }
+        }
+        const bool walk = active && !isb;
+        const int nwalk = walk ? i1 - i0 : 0;
+        int maxwalk = nwalk;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) maxwalk = max(maxwalk, __shfl_xor_sync(0xffffffffu, maxwalk, o));
+        if (maxwalk == 0) continue;   // warp-uniform
 
-        for (int t = lane; t < HS; t += 32) key[t] = -1;
+        for (int t = gl; t < HS; t += G) key[t] = -1;
         __syncwarp();
         int L = 0;
         bool overflow = false;
-        for (int32_t ii = i0; ii < i1; ii++) {
-            const int32_t kk = inc[ii];
-            const int32_t e = kk / N, a = kk - e * N;
-            int32_t col = -1;
-            double v = 0.0;
-            bool nz = false;
-            if (lane < N) {
-                col = e2l[(size_t)e * N + lane];
-                v = Ke[((size_t)e * N + a) * N + lane];
-                nz = (v != 0.0);
+
+        // prefetched data of incidence ii
+        int32_t col = -1;
+        double v = 0.0;
+        bool nz = false;
+        auto load = [&](int ii, int32_t &c_, double &v_, bool &nz_) {
+            c_ = -1; v_ = 0.0; nz_ = false;
+            if (ii < nwalk && gl < N) {
+                const int32_t kk = inc[i0 + ii];
+                const int32_t e = kk / N, a = kk - e * N;
+                c_ = e2l[(size_t)e * N + gl];
+                if (PASS2) {
+                    v_ = Ke[((size_t)e * N + a) * N + gl];
+                    nz_ = v_ != 0.0;
+                } else {
+                    const int bit = a * N + gl;
+                    nz_ = (Km[(size_t)e * MW + (bit >> 5)] >> (bit & 31)) & 1u;
+                }
             }
-            // look up
+        };
+        load(0, col, v, nz);
+        for (int ii = 0; ii < maxwalk; ii++) {
+            int32_t ncol;
+            double nv;
+            bool nnz;
+            load(ii + 1, ncol, nv, nnz);
             int pos = -1;
             if (nz) {
                 unsigned h = hash32(col) & (HS - 1);
@@ -417,7 +478,7 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
                     h = (h + 1) & (HS - 1);
                 }
             }
-            const unsigned newm = __ballot_sync(0xffffffffu, nz && pos < 0);
+            const unsigned newm = __ballot_sync(0xffffffffu, nz && pos < 0) & gmask;
             if (nz && pos < 0) {
                 pos = L + __popc(newm & lt_mask);
                 if (pos < MAXROW) {
@@ -426,86 +487,108 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
                         if (atomicCAS(&key[h], -1, col) == -1) { hpos[h] = (int16_t)pos; break; }
                         h = (h + 1) & (HS - 1);
                     }
-                    if (PASS2) { s_col[w][pos] = col; s_val[w][pos] = v; }
+                    if (PASS2) { scol[pos] = col; sval[pos] = v; }
                 } else {
                     overflow = true;
                 }
             } else if (nz && PASS2) {
-                s_val[w][pos] = rn_add(s_val[w][pos], v);
+                sval[pos] = rn_add(sval[pos], v);
             }
             L += __popc(newm);
+            col = ncol; v = nv; nz = nnz;
             __syncwarp();
         }
-        if (__any_sync(0xffffffffu, overflow) || L > MAXROW) {
-            if (lane == 0) atomicExch(status, PHGB_DEV_ROW_OVERFLOW);
-            continue;
-        }
+        const bool bad = overflow || L > MAXROW;
+        const unsigned badm = __ballot_sync(0xffffffffu, bad) & gmask;
+        if (badm != 0 && gl == 0) atomicExch(status, PHGB_DEV_ROW_OVERFLOW);
 
         if (!PASS2) {
             int nk = 0, nb = 0;
-            for (int t = lane; t < HS; t += 32) {
-                const int32_t c = key[t];
-                if (c < 0) continue;
-                if (c != d && bdry[c]) nb++; else nk++;
+            if (walk && badm == 0)
+                for (int t = gl; t < HS; t += G) {
+                    const int32_t c = key[t];
+                    if (c < 0) continue;
+                    if (c != d && bdry[c]) nb++; else nk++;
+                }
+#pragma unroll
+            for (int o = G / 2; o > 0; o >>= 1) {
+                nk += __shfl_xor_sync(0xffffffffu, nk, o, G);
+                nb += __shfl_xor_sync(0xffffffffu, nb, o, G);
             }
-            nk = warp_sumi(nk);
-            nb = warp_sumi(nb);
-            if (lane == 0) { cnt_keep[d] = nk; cnt_bdry[d] = nb; }
+            if (walk && badm == 0 && gl == 0) { cnt_keep[d] = nk; cnt_bdry[d] = nb; }
             __syncwarp();
             continue;
         }
 
-        // pass 2: emit kept columns and saved boundary columns, in order
-        const int32_t p0 = ptr[d], b0 = bptr[d];
+        // pass 2: emit kept columns and saved boundary columns, in order.
+        // Lanes also evaluate, in parallel, the lift term of each boundary
+        // column (rhs_k * a_dk / D_kk, solver.c:716-724) into s_lift.
+        const bool emit = walk && badm == 0;
+        int32_t p0 = 0, b0 = 0;
+        if (emit) { p0 = ptr[d]; b0 = bptr[d]; }
         int nk = 0, nb = 0;
         double dg = 0.0;
-        for (int base = 0; base < L; base += 32) {
-            const int t = base + lane;
-            bool isb = false, valid = t < L;
+        int maxL = emit ? L : 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) maxL = max(maxL, __shfl_xor_sync(0xffffffffu, maxL, o));
+        for (int base = 0; base < maxL; base += G) {
+            const int t = base + gl;
+            bool isbc = false;
+            const bool valid = emit && t < L;
             int32_t c = 0;
-            double v = 0.0;
+            double val = 0.0;
             if (valid) {
-                c = s_col[w][t];
-                v = s_val[w][t];
-                isb = (c != d) && bdry[c];
-                if (c == d) dg = v;
+                c = scol[t];
+                val = sval[t];
+                isbc = (c != d) && bdry[c];
+                if (c == d) dg = val;
+                double term = 0.0;
+                if (isbc) {
+                    const int mult = inc_ptr[c + 1] - inc_ptr[c];
+                    double Dk = 0.0;
+                    for (int m = 0; m < mult; m++) Dk = rn_add(Dk, 1.0);
+                    const double rk = bdry_rhs(g, c, mult);
+                    term = __ddiv_rn(rn_mul(rn_mul(1.0, rk), val), Dk);
+                }
+                slift[t] = term;
+                if (!isbc) scol[t] = -1;   // only boundary columns remain for the lift below
             }
-            const unsigned km = __ballot_sync(0xffffffffu, valid && !isb);
-            const unsigned bm = __ballot_sync(0xffffffffu, valid && isb);
-            if (valid && !isb) {
+            const unsigned km = __ballot_sync(0xffffffffu, valid && !isbc) & gmask;
+            const unsigned bm = __ballot_sync(0xffffffffu, valid && isbc) & gmask;
+            if (valid && !isbc) {
                 const int r = nk + __popc(km & lt_mask);
                 cols[p0 + r] = c;
-                vals[p0 + r] = v;
+                vals[p0 + r] = val;
             }
-            if (valid && isb) {
+            if (valid && isbc) {
                 const int r = nb + __popc(bm & lt_mask);
                 bcols[b0 + r] = c;
-                bvals[b0 + r] = v;
+                bvals[b0 + r] = val;
             }
             nk += __popc(km);
             nb += __popc(bm);
         }
-        dg = warp_sum(dg);   // exactly one lane holds the diagonal
-        if (lane == 0) {
-            if (p0 + nk != ptr[d + 1] || b0 + nb != bptr[d + 1])
-                atomicExch(status, PHGB_DEV_COUNT_MISMATCH);
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) dg += __shfl_xor_sync(0xffffffffu, dg, o, G);   // one lane holds it
+        // element right-hand sides of this row, loaded by the lanes in parallel
+        // and added by the group's first lane in element order (zeros skipped)
+        double r = 0.0;
+        const int maxinc = __reduce_max_sync(0xffffffffu, (unsigned)(emit ? i1 - i0 : 0));
+        for (int base = 0; base < maxinc; base += G) {
+            const int ii = base + gl;
+            const double bb = (emit && ii < i1 - i0) ? Re[inc[i0 + ii]] : 0.0;
+            for (int t = 0; t < G; t++) {
+                const double bt = __shfl_sync(0xffffffffu, bb, t, G);
+                if (gl == 0 && base + t < i1 - i0 && bt != 0.0) r = rn_add(r, bt);
+            }
+        }
+        __syncwarp();
+        if (emit && gl == 0) {
+            if (p0 + nk != ptr[d + 1] || b0 + nb != bptr[d + 1]) atomicExch(status, PHGB_DEV_COUNT_MISMATCH);
             diag[d] = dg;
-            // rhs: element contributions in element order, zeros skipped
-            double r = 0.0;
-            for (int32_t ii = i0; ii < i1; ii++) {
-                const double b = Re[inc[ii]];
-                if (b != 0.0) r = rn_add(r, b);
-            }
-            // lift the boundary columns: r -= 1.0 * rhs_k * a_dk / D_kk
-            for (int t = 0; t < L; t++) {
-                const int32_t c = s_col[w][t];
-                if (c == d || !bdry[c]) continue;
-                const int mult = inc_ptr[c + 1] - inc_ptr[c];
-                double Dk = 0.0;
-                for (int m = 0; m < mult; m++) Dk = rn_add(Dk, 1.0);
-                const double rk = bdry_rhs(g, c, mult);
-                r = rn_sub(r, __ddiv_rn(rn_mul(rn_mul(1.0, rk), s_val[w][t]), Dk));
-            }
+            // lift the boundary columns in first-touch order: r -= term
+            for (int t = 0; t < L; t++)
+                if (scol[t] >= 0) r = rn_sub(r, slift[t]);
             rhs[d] = r;
         }
         __syncwarp();
@@ -522,17 +605,26 @@ static int grid_for(int64_t work, int per_block, int max_blocks) {
     return (int)b;
 }
 
+template <int P>
+static void elem_launch(const ElemArgs &A, cudaStream_t s) {
+    constexpr int W = ElemDims<P>::WARPS;
+    geometry_kernel<<<grid_for(A.nelem, 128, 148 * 64), 128, 0, s>>>(A.nelem, A.nvert, A.verts, A.elems, A.geo,
+                                                                    A.status);
+    const int blocks = grid_for(A.nelem, W, 148 * 64);
+    element_kernel<P><<<blocks, W * 32, 0, s>>>(A.nelem, A.ndof, A.geo, A.e2l, A.kappa, A.f, A.wk, A.gk, A.wr,
+                                                A.br, A.Ke, A.Re, A.Km, A.status);
+}
+
 cudaError_t launch_element_kernel(int p, const ElemArgs &A, cudaStream_t s) {
-    const int blocks = grid_for(A.nelem, kElemWarps, 148 * 64);
-#define PHGB_ELEM(P)                                                                       \
-    element_kernel<P><<<blocks, kElemWarps * 32, 0, s>>>(A.nelem, A.nvert, A.ndof, A.verts, \
-        A.elems, A.e2l, A.kappa, A.f, A.wk, A.gk, A.wr, A.br, A.Ke, A.Re, A.status)
-    if (p == 1) PHGB_ELEM(1);
-    else if (p == 2) PHGB_ELEM(2);
-    else PHGB_ELEM(3);
-#undef PHGB_ELEM
+    if (p == 1) elem_launch<1>(A, s);
+    else if (p == 2) elem_launch<2>(A, s);
+    else elem_launch<3>(A, s);
     return cudaGetLastError();
 }
+
+int64_t geometry_doubles(int64_t nelem) { return nelem * kGeo; }
+
+int element_mask_words(int p) { return p == 1 ? ElemDims<1>::MW : p == 2 ? ElemDims<2>::MW : ElemDims<3>::MW; }
 
 cudaError_t launch_incidence(int N, int64_t nelem, int64_t ndof, const int32_t *e2l, int32_t *cnt,
                              int32_t *inc_ptr, int32_t *cursor, int32_t *inc, int64_t *scan_ws,
@@ -561,27 +653,27 @@ cudaError_t launch_scan(int64_t n, const int32_t *in, int32_t *out, int64_t *ws,
     return cudaGetLastError();
 }
 
-template <int N, int HS>
+template <int N>
 static cudaError_t walk(bool pass2, const WalkArgs &A, cudaStream_t s) {
-    constexpr int W = WalkCfg<N, HS>::WARPS;
-    const int blocks = grid_for(A.ndof, W, 148 * 32);
+    constexpr int W = WalkCfg<N>::WARPS, R = WalkCfg<N>::R;
+    const int blocks = grid_for(ceil_div(A.ndof, R), W, 148 * 32);
     if (!pass2)
-        row_walk_kernel<N, HS, false><<<blocks, W * 32, 0, s>>>(
-            A.ndof, A.inc_ptr, A.inc, A.e2l, A.bdry, A.Ke, A.Re, A.g, A.cnt_keep, A.cnt_bdry,
+        row_walk_kernel<N, false><<<blocks, W * 32, 0, s>>>(
+            A.ndof, A.inc_ptr, A.inc, A.e2l, A.bdry, A.Ke, A.Km, A.Re, A.g, A.cnt_keep, A.cnt_bdry,
             nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, A.status);
     else
-        row_walk_kernel<N, HS, true><<<blocks, W * 32, 0, s>>>(
-            A.ndof, A.inc_ptr, A.inc, A.e2l, A.bdry, A.Ke, A.Re, A.g, nullptr, nullptr, A.ptr,
+        row_walk_kernel<N, true><<<blocks, W * 32, 0, s>>>(
+            A.ndof, A.inc_ptr, A.inc, A.e2l, A.bdry, A.Ke, A.Km, A.Re, A.g, nullptr, nullptr, A.ptr,
             A.cols, A.vals, A.bptr, A.bcols, A.bvals, A.rhs, A.diag, A.status);
     return cudaGetLastError();
 }
 
 cudaError_t launch_row_walk(int p, bool pass2, const WalkArgs &A, cudaStream_t s) {
-    if (p == 1) return walk<4, 128>(pass2, A, s);
-    if (p == 2) return walk<10, 256>(pass2, A, s);
-    return walk<20, 512>(pass2, A, s);
+    if (p == 1) return walk<4>(pass2, A, s);
+    if (p == 2) return walk<10>(pass2, A, s);
+    return walk<20>(pass2, A, s);
 }
 
-int row_walk_max_row(int p) { return p == 1 ? 64 : p == 2 ? 128 : 256; }
+int row_walk_max_row(int p) { return p == 1 ? WalkCfg<4>::MAXROW : p == 2 ? WalkCfg<10>::MAXROW : WalkCfg<20>::MAXROW; }
 
 }  // namespace phgb

@@ -11,7 +11,9 @@ struct ElemArgs {
     const int32_t *elems, *e2l;
     const double *kappa, *f;                 // may be null
     const double *wk, *gk, *wr, *br;         // element tables
+    double *geo;                             // scratch: nelem * geometry_doubles
     double *Ke, *Re;
+    uint32_t *Km;
     int *status;
 };
 
@@ -20,6 +22,7 @@ struct WalkArgs {
     const int32_t *inc_ptr, *inc, *e2l;
     const uint8_t *bdry;
     const double *Ke, *Re, *g;
+    const uint32_t *Km;
     int32_t *cnt_keep, *cnt_bdry;            // pass 1
     const int32_t *ptr, *bptr;               // pass 2
     int32_t *cols, *bcols;
@@ -36,5 +39,7 @@ int64_t scan_workspace_elems(int64_t n);
 cudaError_t launch_scan(int64_t n, const int32_t *in, int32_t *out, int64_t *ws, cudaStream_t s);
 cudaError_t launch_row_walk(int p, bool pass2, const WalkArgs &a, cudaStream_t s);
 int row_walk_max_row(int p);
+int element_mask_words(int p);
+int64_t geometry_doubles(int64_t nelem);
 
 }  // namespace phgb

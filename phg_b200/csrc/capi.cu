@@ -6,6 +6,8 @@
 #include "common.cuh"
 #include "fe_tables.h"
 #include "solve.h"
+#include "adjoint.h"
+#include "block.h"
 
 #include <math.h>
 #include <float.h>
@@ -83,6 +85,13 @@ bool is_device_ptr(const void *ptr) {
     return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+// x += y unless the correction y was already folded in (y_reset set).
+__global__ void fold_kernel(int64_t n, double *x, const float *y, const MixedState *ms) {
+    if (ms->y_reset) return;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] += (double)y[i];
+}
+
 __global__ void widen_kernel(int64_t n, const int32_t *in, int64_t *out) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         out[i] = in[i];
@@ -104,6 +113,12 @@ __global__ void diag_kernel(int64_t n, const int32_t *rp, const int32_t *ci, con
 }
 
 constexpr int kGraphChunk = 16;
+
+// SpMV autotuner candidates: CSR with 4/8/16/32 lanes per row, SELL-C-sigma
+// with the inner loop unrolled 2/4/8 times.
+constexpr int kTuneCandidates = 7;
+const int kTuneKind[kTuneCandidates] = {SPMV_CSR, SPMV_CSR, SPMV_CSR, SPMV_CSR, SPMV_SELL, SPMV_SELL, SPMV_SELL};
+const int kTuneParam[kTuneCandidates] = {4, 8, 16, 32, 2, 4, 8};
 
 }  // namespace
 
@@ -136,7 +151,8 @@ struct phgGpuSystem_ {
     DevBuf<double> wk, gk, wr, br;
 
     // assembly buffers
-    DevBuf<double> Ke, Re, kappa, f, g;
+    DevBuf<double> Ke, Re, kappa, f, g, geo;
+    DevBuf<uint32_t> Km;
     DevBuf<int32_t> cnt_keep, cnt_bdry;
 
     // assembled system
@@ -165,6 +181,41 @@ struct phgGpuSystem_ {
     } gkey{};
     int lpr = 8;
     int64_t launches = 0;   // kernels launched by this system (graph nodes included)
+
+    // SpMV layout chosen by the autotuner, and the SELL-C-sigma copy
+    SpmvPlan plan;
+    bool sell_valid = false;
+    int64_t sell_total = 0;
+    DevBuf<int32_t> sell_perm, sell_ssz, sell_sptr, sell_cols;
+    DevBuf<uint16_t> sell_len;
+    DevBuf<double> sell_vals;
+    DevBuf<float> sell_vals32;
+    bool tuned = false;
+    int64_t tuned_n = -1, tuned_nnz = -1;
+    int unroll32 = 0;                 // FP32 SELL unroll (0: not tuned yet)
+    double tune32_ms[3] = {};
+    double tune_ms[kTuneCandidates] = {};
+
+    // mixed-precision solver
+    DevBuf<float> r32, p32, Ap32, y32, D32;
+    // adjoint gradient
+    DevBuf<double> adj_u, adj_uobs, adj_rhs, adj_lambda, adj_grad;
+
+    // block PCG
+    DevBuf<double> bX, bR, bP, bAP, bB, bscal, bpart;
+    DevBuf<float> bY32, bR32, bP32, bAP32, bva32;
+    DevBuf<int> bint;
+    DevBuf<unsigned> btick;
+    int btile = 0;                      // autotuned SpMM tile (columns)
+    int64_t btile_n = -1, btile_nnz = -1;
+    int btile_K = -1;
+    double btile_ms[4] = {};
+    cudaGraphExec_t graph_block = nullptr;
+    GraphKey gkey_block{};
+    DevBuf<MixedState> mst;
+    MixedState *h_mst = nullptr;
+    cudaGraphExec_t graph_mixed = nullptr;
+    GraphKey gkey_mixed{};
 };
 
 namespace {
@@ -244,6 +295,114 @@ int solver_buffers(phgGpuSystem *s) {
     return PHG_GPU_OK;
 }
 
+// Builds the SELL-C-sigma copy of the current CSR (values in FP64 and FP32).
+int ensure_sell(phgGpuSystem *s) {
+    if (s->sell_valid) return PHG_GPU_OK;
+    const int64_t n = s->n, npos = sell_positions(n), nsl = npos / 32;
+    CHECK_RC(s->sell_perm.ensure((size_t)npos));
+    CHECK_RC(s->sell_len.ensure((size_t)npos));
+    CHECK_RC(s->sell_ssz.ensure((size_t)nsl));
+    CHECK_RC(s->sell_sptr.ensure((size_t)nsl + 1));
+    CHECK_RC(s->scan_ws.ensure((size_t)scan_workspace_elems(nsl)));
+    CK(launch_sell_sort(n, s->rp.p, s->sell_perm.p, s->sell_len.p, s->sell_ssz.p, s->stream));
+    CK(launch_scan(nsl, s->sell_ssz.p, s->sell_sptr.p, s->scan_ws.p, s->stream));
+    int32_t total = 0;
+    CK(cudaMemcpyAsync(&total, s->sell_sptr.p + nsl, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    if (total < 0) return fail(PHG_GPU_ERR_LIMIT, "SELL layout larger than 2^31 entries");
+    CHECK_RC(s->sell_cols.ensure((size_t)total));
+    CHECK_RC(s->sell_vals.ensure((size_t)total));
+    CHECK_RC(s->sell_vals32.ensure((size_t)total));
+    CK(launch_sell_fill(n, s->rp.p, s->ci.p, s->va.p, s->sell_perm.p, s->sell_len.p, s->sell_sptr.p,
+                        s->sell_cols.p, s->sell_vals.p, s->sell_vals32.p, s->stream));
+    s->launches += 5;
+    s->sell_total = total;
+    s->sell_valid = true;
+    return PHG_GPU_OK;
+}
+
+// Unroll depth of the FP32 SELL SpMV (mixed solver): 4, 8 or 16, timed once
+// per matrix shape.
+int tune_spmv32(phgGpuSystem *s) {
+    if (s->unroll32 != 0 && s->tuned_n == s->n && s->tuned_nnz == s->nnz) return PHG_GPU_OK;
+    CHECK_RC(s->r32.ensure((size_t)s->n));
+    CHECK_RC(s->Ap32.ensure((size_t)s->n));
+    CK(cudaMemsetAsync(s->r32.p, 0, sizeof(float) * s->n, s->stream));
+    const SellView S{s->n, sell_positions(s->n) / 32, s->sell_perm.p, s->sell_len.p, s->sell_sptr.p,
+                     s->sell_cols.p, s->sell_vals.p, s->sell_vals32.p};
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    const int cand[3] = {4, 8, 16};
+    int best = 0;
+    const int reps = 5;
+    for (int c = 0; c < 3; c++) {
+        for (int i = 0; i < 2; i++) CK(launch_spmv32(S, cand[c], s->r32.p, s->Ap32.p, s->stream));
+        CK(cudaEventRecord(a, s->stream));
+        for (int i = 0; i < reps; i++) CK(launch_spmv32(S, cand[c], s->r32.p, s->Ap32.p, s->stream));
+        CK(cudaEventRecord(b, s->stream));
+        CK(cudaEventSynchronize(b));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, a, b));
+        s->tune32_ms[c] = ms / reps;
+        s->launches += 2 + reps;
+        if (s->tune32_ms[c] < s->tune32_ms[best]) best = c;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    s->unroll32 = cand[best];
+    return PHG_GPU_OK;
+}
+
+SpmvPlan make_plan(phgGpuSystem *s, int kind, int param) {
+    SpmvPlan P;
+    P.kind = kind;
+    P.lpr = kind == SPMV_CSR ? param : 8;
+    P.unroll = kind == SPMV_SELL ? param : 4;
+    P.csr = CsrView{s->n, s->rp.p, s->ci.p, s->va.p};
+    P.sell = SellView{s->n, sell_positions(s->n) / 32, s->sell_perm.p, s->sell_len.p, s->sell_sptr.p,
+                      s->sell_cols.p, s->sell_vals.p, s->sell_vals32.p};
+    return P;
+}
+
+// Chooses the fastest SpMV layout for the current matrix shape by timing
+// every candidate on the system's stream (once per (n, nnz)).
+int tune_spmv(phgGpuSystem *s) {
+    if (s->tuned && s->tuned_n == s->n && s->tuned_nnz == s->nnz) {
+        if (s->plan.kind == SPMV_SELL) CHECK_RC(ensure_sell(s));
+        s->plan = make_plan(s, s->plan.kind, s->plan.kind == SPMV_CSR ? s->plan.lpr : s->plan.unroll);
+        return PHG_GPU_OK;
+    }
+    CHECK_RC(ensure_sell(s));
+    CHECK_RC(solver_buffers(s));
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    int best = 0;
+    const int reps = 5;
+    for (int c = 0; c < kTuneCandidates; c++) {
+        const SpmvPlan P = make_plan(s, kTuneKind[c], kTuneParam[c]);
+        for (int i = 0; i < 2; i++) CK(launch_spmv_plan(P, s->rhs.p, s->Ap.p, s->stream));
+        CK(cudaEventRecord(a, s->stream));
+        for (int i = 0; i < reps; i++) CK(launch_spmv_plan(P, s->rhs.p, s->Ap.p, s->stream));
+        CK(cudaEventRecord(b, s->stream));
+        CK(cudaEventSynchronize(b));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, a, b));
+        s->tune_ms[c] = ms / reps;
+        s->launches += 2 + reps;
+        if (s->tune_ms[c] < s->tune_ms[best]) best = c;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    s->plan = make_plan(s, kTuneKind[best], kTuneParam[best]);
+    s->unroll32 = 0;
+    s->tuned = true;
+    s->tuned_n = s->n;
+    s->tuned_nnz = s->nnz;
+    return PHG_GPU_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -296,14 +455,29 @@ int phgGpuDestroy(phgGpuSystem *s) {
     cudaSetDevice(s->device);
     if (s->stream != nullptr) cudaStreamSynchronize(s->stream);
     if (s->graph != nullptr) cudaGraphExecDestroy(s->graph);
+    if (s->graph_mixed != nullptr) cudaGraphExecDestroy(s->graph_mixed);
+    if (s->h_mst) cudaFreeHost(s->h_mst);
+    DevBuf<float> *fbufs[] = {&s->r32, &s->p32, &s->Ap32, &s->y32, &s->D32, &s->sell_vals32};
+    for (auto *b : fbufs) b->release();
+    s->sell_perm.release(); s->sell_ssz.release(); s->sell_sptr.release(); s->sell_cols.release();
+    s->sell_len.release(); s->sell_vals.release(); s->mst.release();
+    s->adj_u.release(); s->adj_uobs.release(); s->adj_rhs.release(); s->adj_lambda.release(); s->adj_grad.release();
+    if (s->graph_block != nullptr) cudaGraphExecDestroy(s->graph_block);
+    DevBuf<double> *bb[] = {&s->bX, &s->bR, &s->bP, &s->bAP, &s->bB, &s->bscal, &s->bpart};
+    for (auto *b : bb) b->release();
+    DevBuf<float> *bf[] = {&s->bY32, &s->bR32, &s->bP32, &s->bAP32, &s->bva32};
+    for (auto *b : bf) b->release();
+    s->bint.release();
+    s->btick.release();
     DevBuf<double> *dbufs[] = {&s->verts, &s->wk, &s->gk, &s->wr, &s->br, &s->Ke, &s->Re, &s->kappa, &s->f,
-                               &s->g, &s->va, &s->bva, &s->rhs, &s->diag, &s->x, &s->r, &s->p, &s->Ap,
+                               &s->g, &s->geo, &s->va, &s->bva, &s->rhs, &s->diag, &s->x, &s->r, &s->p, &s->Ap,
                                &s->partials, &s->hist, &s->sums};
     for (auto *b : dbufs) b->release();
     DevBuf<int32_t> *ibufs[] = {&s->elems, &s->e2l, &s->inc_ptr, &s->inc, &s->cnt, &s->cursor, &s->cnt_keep,
                                 &s->cnt_bdry, &s->rp, &s->ci, &s->brp, &s->bci};
     for (auto *b : ibufs) b->release();
     s->bdry.release();
+    s->Km.release();
     s->scan_ws.release();
     s->tmp64.release();
     s->st.release();
@@ -397,15 +571,17 @@ int phgGpuBuildLinearSystem(phgGpuSystem *s, const double *kappa, const double *
     CHECK_RC(stage(s, g, (size_t)ndof, s->g, &dg));
     CHECK_RC(s->Ke.ensure((size_t)s->nelem * N * N));
     CHECK_RC(s->Re.ensure((size_t)s->nelem * N));
+    CHECK_RC(s->Km.ensure((size_t)s->nelem * element_mask_words(s->order)));
+    CHECK_RC(s->geo.ensure((size_t)geometry_doubles(s->nelem)));
 
     ElemArgs ea{};
     ea.nelem = s->nelem; ea.nvert = s->nvert; ea.ndof = ndof;
     ea.verts = s->verts.p; ea.elems = s->elems.p; ea.e2l = s->e2l.p;
     ea.kappa = dk; ea.f = df;
     ea.wk = s->wk.p; ea.gk = s->gk.p; ea.wr = s->wr.p; ea.br = s->br.p;
-    ea.Ke = s->Ke.p; ea.Re = s->Re.p; ea.status = s->status.p;
+    ea.Ke = s->Ke.p; ea.Re = s->Re.p; ea.Km = s->Km.p; ea.geo = s->geo.p; ea.status = s->status.p;
     CK(launch_element_kernel(s->order, ea, s->stream));
-    s->launches += 1;
+    s->launches += 2;
 
     CHECK_RC(s->cnt_keep.ensure((size_t)ndof));
     CHECK_RC(s->cnt_bdry.ensure((size_t)ndof));
@@ -413,7 +589,7 @@ int phgGpuBuildLinearSystem(phgGpuSystem *s, const double *kappa, const double *
     CHECK_RC(s->brp.ensure((size_t)ndof + 1));
     WalkArgs wa{};
     wa.ndof = ndof; wa.inc_ptr = s->inc_ptr.p; wa.inc = s->inc.p; wa.e2l = s->e2l.p; wa.bdry = s->bdry.p;
-    wa.Ke = s->Ke.p; wa.Re = s->Re.p; wa.g = dg;
+    wa.Ke = s->Ke.p; wa.Re = s->Re.p; wa.g = dg; wa.Km = s->Km.p;
     wa.cnt_keep = s->cnt_keep.p; wa.cnt_bdry = s->cnt_bdry.p; wa.status = s->status.p;
     CK(launch_row_walk(s->order, false, wa, s->stream));
     s->launches += 7;   // pass 1 + two scans
@@ -441,6 +617,7 @@ int phgGpuBuildLinearSystem(phgGpuSystem *s, const double *kappa, const double *
     s->n = ndof;
     s->assembled = true;
     s->have_bdry_cols = true;
+    s->sell_valid = false;
     s->lpr = spmv_lanes_for((double)s->nnz / (double)ndof);
     return PHG_GPU_OK;
 }
@@ -476,6 +653,7 @@ int phgGpuSetMatrix(phgGpuSystem *s, int64_t n, const int64_t *ptr, const int32_
     s->bnnz = 0;
     s->assembled = true;
     s->have_bdry_cols = false;
+    s->sell_valid = false;
     s->lpr = spmv_lanes_for((double)nnz / (double)n);
     return PHG_GPU_OK;
 }
@@ -544,13 +722,199 @@ int phgGpuMatVec(phgGpuSystem *s, const double *x, double *y) {
     const double *dx;
     CHECK_RC(stage(s, x, (size_t)s->n, s->p, &dx));
     double *dy = ydev ? y : s->Ap.p;
-    CsrView A{s->n, s->rp.p, s->ci.p, s->va.p};
-    CK(launch_spmv(A, s->lpr, dx, dy, s->stream));
+    CHECK_RC(tune_spmv(s));
+    CK(launch_spmv_plan(s->plan, dx, dy, s->stream));
     s->launches += 1;
     if (!ydev) CHECK_RC(copy_out(s, y, dy, (size_t)s->n));
     // device-to-device calls stay asynchronous on the system's stream
     if (!(xdev && ydev)) CK(cudaStreamSynchronize(s->stream));
     return PHG_GPU_OK;
+}
+
+int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol, int maxit, double *x,
+                         double *residual, int *nupdates) {
+    if (s == nullptr || x == nullptr) return fail(PHG_GPU_ERR_ARG, "invalid arguments");
+    if (!s->assembled) return fail(PHG_GPU_ERR_STATE, "no assembled system");
+    if (maxit < 0) return fail(PHG_GPU_ERR_ARG, "maxit < 0");
+    CHECK_RC(set_device(s));
+    CHECK_RC(solver_buffers(s));
+    CHECK_RC(tune_spmv(s));
+    CHECK_RC(ensure_sell(s));
+    const int64_t n = s->n;
+    const size_t un = (size_t)n;
+    CHECK_RC(s->r32.ensure(un));
+    CHECK_RC(s->p32.ensure(un));
+    CHECK_RC(s->Ap32.ensure(un));
+    CHECK_RC(s->y32.ensure(un));
+    CHECK_RC(s->D32.ensure(un));
+    CHECK_RC(s->mst.ensure(1));
+    if (s->h_mst == nullptr) CK(cudaMallocHost((void **)&s->h_mst, sizeof(MixedState)));
+    CHECK_RC(copy_in(s, s->x.p, x, un));
+    CK(cudaMemsetAsync(s->ticket.p, 0, sizeof(unsigned), s->stream));
+    const SpmvPlan P = make_plan(s, s->plan.kind, s->plan.kind == SPMV_CSR ? s->plan.lpr : s->plan.unroll);
+    CHECK_RC(tune_spmv32(s));
+    const int unroll = s->unroll32;
+
+    CK(launch_init_sums(n, 0, s->x.p, s->rhs.p, s->diag.p, s->partials.p, s->ticket.p, s->sums.p, s->stream));
+    CK(cudaMemcpyAsync(s->h_sums, s->sums.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    s->launches += 1;
+    const double x1 = s->h_sums[0], rb = sqrt(s->h_sums[1]);
+    auto is_zero = [](double a) { return fabs(a) < 10.0 * DBL_MIN; };
+    if (is_zero(rb)) {
+        CK(cudaMemsetAsync(s->x.p, 0, sizeof(double) * n, s->stream));
+        CHECK_RC(copy_out(s, x, s->x.p, un));
+        CK(cudaStreamSynchronize(s->stream));
+        if (residual) *residual = 0.0;
+        if (nupdates) *nupdates = 0;
+        return 0;
+    }
+    bool x_nonzero = !is_zero(x1 / (double)n);
+    double tol = -1.0;
+    int nits_total = 0, nupd = 0;
+    double res_true = 0.0;
+    MixedBuffers B{n, s->x.p, s->r.p, s->r32.p, s->p32.p, s->Ap32.p, s->y32.p, s->D32.p, s->partials.p, s->mst.p,
+                   nullptr};
+    // the explicit FP64 residual b - A x is checked at the end; a recurrence
+    // that drifted above the tolerance restarts from it (at most twice)
+    for (int restart = 0; restart < 3; restart++) {
+        if (x_nonzero) {
+            CK(launch_spmv_plan(P, s->x.p, s->Ap.p, s->stream));
+            CK(launch_residual(n, s->rhs.p, s->Ap.p, s->r.p, s->stream));
+            s->launches += 2;
+        } else {
+            CK(cudaMemcpyAsync(s->r.p, s->rhs.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s->stream));
+        }
+        CK(launch_mixed_init(n, s->r.p, s->r32.p, s->y32.p, s->diag.p, s->D32.p, s->partials.p, s->ticket.p,
+                             s->sums.p, s->stream));
+        s->launches += 1;
+        CK(cudaMemcpyAsync(s->h_sums, s->sums.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        const double r0 = sqrt(s->h_sums[0]), rz0 = s->h_sums[1];
+        if (!isfinite(rz0)) return fail(PHG_GPU_ERR_NAN, "phgGpuSolverPCGMixed: zero or non-finite diagonal");
+        if (tol < 0.0) {   // get_tol (solver-phg.c:104-115) on the initial residual
+            tol = r0 * rtol;
+            if (tol < rb * btol) tol = rb * btol;
+            if (tol < atol) tol = atol;
+        }
+        MixedState m{};
+        m.pcg.rz_cur = rz0;
+        m.pcg.residual = r0;
+        m.pcg.tol = tol;
+        m.pcg.maxit = maxit - nits_total;
+        m.pcg.done = !(r0 > tol && nits_total < maxit);
+        m.maxr = r0;
+        m.delta = 0.1;
+        m.y_reset = 1;
+        *s->h_mst = m;
+        CK(cudaMemcpyAsync(s->mst.p, s->h_mst, sizeof(MixedState), cudaMemcpyHostToDevice, s->stream));
+
+        phgGpuSystem_::GraphKey key{};
+        key.x = s->x.p; key.r = s->r32.p; key.p = s->p32.p; key.Ap = s->Ap32.p; key.D = s->D32.p;
+        key.va = s->sell_vals32.p; key.hist = s->sell_cols.p; key.n = n; key.lpr = unroll; key.s = s->stream;
+        if (s->graph_mixed == nullptr || !(s->gkey_mixed == key)) {
+            if (s->graph_mixed != nullptr) { cudaGraphExecDestroy(s->graph_mixed); s->graph_mixed = nullptr; }
+            cudaGraph_t gr;
+            CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+            for (int i = 0; i < kGraphChunk; i++) launch_mixed_iteration(B, P.sell, unroll, s->stream);
+            CK(cudaStreamEndCapture(s->stream, &gr));
+            cudaError_t e = cudaGraphInstantiate(&s->graph_mixed, gr, 0);
+            cudaGraphDestroy(gr);
+            CK(e);
+            s->gkey_mixed = key;
+        }
+        while (!s->h_mst->pcg.done) {
+            CK(cudaGraphLaunch(s->graph_mixed, s->stream));
+            s->launches += 4 * kGraphChunk;
+            CK(cudaMemcpyAsync(s->h_mst, s->mst.p, sizeof(MixedState), cudaMemcpyDeviceToHost, s->stream));
+            CK(cudaStreamSynchronize(s->stream));
+        }
+        const MixedState &hm = *s->h_mst;
+        nits_total += hm.pcg.nits;
+        nupd += hm.nupdates;
+        fold_kernel<<<vec_blocks(n), 256, 0, s->stream>>>(n, s->x.p, s->y32.p, s->mst.p);
+        s->launches += 1;
+        if (hm.pcg.status == PCG_BREAKDOWN)
+            return fail(PHG_GPU_ERR_BREAKDOWN, "mixed PCG breakdown: the matrix may not be SPD");
+        if (hm.pcg.status == PCG_NONFINITE) return fail(PHG_GPU_ERR_NAN, "mixed PCG: non-finite residual");
+        // explicit FP64 residual of the accumulated solution
+        CK(launch_spmv_plan(P, s->x.p, s->Ap.p, s->stream));
+        CK(launch_residual(n, s->rhs.p, s->Ap.p, s->r.p, s->stream));
+        CK(launch_init_sums(n, 1, s->x.p, s->r.p, s->diag.p, s->partials.p, s->ticket.p, s->sums.p, s->stream));
+        s->launches += 3;
+        CK(cudaMemcpyAsync(s->h_sums, s->sums.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        res_true = sqrt(s->h_sums[0]);
+        if (!(res_true > tol) || nits_total >= maxit) break;
+        x_nonzero = true;
+    }
+    CHECK_RC(copy_out(s, x, s->x.p, un));
+    CK(cudaStreamSynchronize(s->stream));
+    if (residual) *residual = res_true;
+    if (nupdates) *nupdates = nupd;
+    return nits_total;
+}
+
+int phgGpuTimeSpMV(phgGpuSystem *s, int fp32, int reps, double *ms_per_launch) {
+    if (s == nullptr || ms_per_launch == nullptr || reps <= 0) return fail(PHG_GPU_ERR_ARG, "invalid arguments");
+    if (!s->assembled) return fail(PHG_GPU_ERR_STATE, "no assembled system");
+    CHECK_RC(set_device(s));
+    CHECK_RC(solver_buffers(s));
+    CHECK_RC(tune_spmv(s));
+    SpmvPlan P = make_plan(s, s->plan.kind, s->plan.kind == SPMV_CSR ? s->plan.lpr : s->plan.unroll);
+    if (fp32) {
+        CHECK_RC(ensure_sell(s));
+        CHECK_RC(s->r32.ensure((size_t)s->n));
+        CHECK_RC(s->Ap32.ensure((size_t)s->n));
+        CK(cudaMemsetAsync(s->r32.p, 0, sizeof(float) * s->n, s->stream));
+        CHECK_RC(tune_spmv32(s));
+        P = make_plan(s, SPMV_SELL, s->unroll32);
+    }
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    for (int i = 0; i < reps + 3; i++) {
+        if (i == 3) CK(cudaEventRecord(a, s->stream));
+        if (fp32) CK(launch_spmv32(P.sell, P.unroll, s->r32.p, s->Ap32.p, s->stream));
+        else CK(launch_spmv_plan(P, s->rhs.p, s->Ap.p, s->stream));
+    }
+    CK(cudaEventRecord(b, s->stream));
+    CK(cudaEventSynchronize(b));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    s->launches += reps + 3;
+    *ms_per_launch = ms / reps;
+    return PHG_GPU_OK;
+}
+
+int phgGpuSetSpMVPlan(phgGpuSystem *s, int kind, int param) {
+    if (s == nullptr) return fail(PHG_GPU_ERR_ARG, "null system");
+    if (!s->assembled) return fail(PHG_GPU_ERR_STATE, "no assembled system");
+    int c = 0;
+    while (c < kTuneCandidates && !(kTuneKind[c] == kind && kTuneParam[c] == param)) c++;
+    if (c == kTuneCandidates) return fail(PHG_GPU_ERR_ARG, "no SpMV layout (%d, %d)", kind, param);
+    CHECK_RC(set_device(s));
+    if (kind == SPMV_SELL) CHECK_RC(ensure_sell(s));
+    s->plan = make_plan(s, kind, param);
+    s->tuned = true;
+    s->tuned_n = s->n;
+    s->tuned_nnz = s->nnz;
+    return PHG_GPU_OK;
+}
+
+int phgGpuGetSpMVPlan(phgGpuSystem *s, int *kind, int *param, double *times_ms) {
+    if (s == nullptr) return fail(PHG_GPU_ERR_ARG, "null system");
+    if (!s->tuned) return fail(PHG_GPU_ERR_STATE, "the SpMV layout is chosen at the first solve or product");
+    if (kind) *kind = s->plan.kind;
+    if (param) *param = s->plan.kind == SPMV_CSR ? s->plan.lpr : s->plan.unroll;
+    if (times_ms) {
+        for (int c = 0; c < kTuneCandidates; c++) times_ms[c] = s->tune_ms[c];
+        for (int c = 0; c < 3; c++) times_ms[kTuneCandidates + c] = s->tune32_ms[c];
+        times_ms[kTuneCandidates + 3] = s->unroll32;
+    }
+    return kTuneCandidates;
 }
 
 int phgGpuGetLaunchCount(phgGpuSystem *s, int64_t *count) {
@@ -559,24 +923,19 @@ int phgGpuGetLaunchCount(phgGpuSystem *s, int64_t *count) {
     return PHG_GPU_OK;
 }
 
-int phgGpuSolverPCG(phgGpuSystem *s, double rtol, double btol, double atol, int maxit, double *x,
-                    double *residual, double *hist) {
-    if (s == nullptr || x == nullptr) return fail(PHG_GPU_ERR_ARG, "invalid arguments");
-    if (!s->assembled) return fail(PHG_GPU_ERR_STATE, "no assembled system");
-    if (maxit < 0) return fail(PHG_GPU_ERR_ARG, "maxit < 0");
-    CHECK_RC(set_device(s));
-    CHECK_RC(solver_buffers(s));
-    const int64_t n = s->n;
-    CHECK_RC(copy_in(s, s->x.p, x, (size_t)n));
-    double *dhist = nullptr;
-    if (hist != nullptr) {
-        CHECK_RC(s->hist.ensure((size_t)maxit + 1));
-        dhist = s->hist.p;
-    }
-    CK(cudaMemsetAsync(s->ticket.p, 0, sizeof(unsigned), s->stream));
+}  // extern "C"
 
+namespace {
+
+// FP64 Jacobi-PCG on the assembled matrix with right-hand side `drhs`
+// (device), iterating on s->x (initial guess in, solution out).  Returns the
+// iteration count or a negative error code.
+int pcg_core(phgGpuSystem *s, const double *drhs, double rtol, double btol, double atol, int maxit,
+             double *dhist, double *residual) {
+    const int64_t n = s->n;
+    CK(cudaMemsetAsync(s->ticket.p, 0, sizeof(unsigned), s->stream));
     // ||b|| and |x|_1 (solver-phg.c:498-518)
-    CK(launch_init_sums(n, 0, s->x.p, s->rhs.p, s->diag.p, s->partials.p, s->ticket.p, s->sums.p, s->stream));
+    CK(launch_init_sums(n, 0, s->x.p, drhs, s->diag.p, s->partials.p, s->ticket.p, s->sums.p, s->stream));
     s->launches += 1;
     CK(cudaMemcpyAsync(s->h_sums, s->sums.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
@@ -584,26 +943,25 @@ int phgGpuSolverPCG(phgGpuSystem *s, double rtol, double btol, double atol, int 
     auto is_zero = [](double a) { return fabs(a) < 10.0 * DBL_MIN; };   // utils.h:451
     if (is_zero(rb)) {
         CK(cudaMemsetAsync(s->x.p, 0, sizeof(double) * n, s->stream));
-        CHECK_RC(copy_out(s, x, s->x.p, (size_t)n));
-        CK(cudaStreamSynchronize(s->stream));
         if (residual) *residual = 0.0;
-        if (hist) hist[0] = 0.0;
+        if (dhist) CK(cudaMemsetAsync(dhist, 0, sizeof(double), s->stream));
         return 0;
     }
     CsrView A{n, s->rp.p, s->ci.p, s->va.p};
+    CHECK_RC(tune_spmv(s));
     if (!is_zero(x1 / (double)n)) {
-        CK(launch_spmv(A, s->lpr, s->x.p, s->Ap.p, s->stream));
-        CK(launch_residual(n, s->rhs.p, s->Ap.p, s->r.p, s->stream));
+        CK(launch_spmv_plan(s->plan, s->x.p, s->Ap.p, s->stream));
+        CK(launch_residual(n, drhs, s->Ap.p, s->r.p, s->stream));
         s->launches += 2;
     } else {
-        CK(cudaMemcpyAsync(s->r.p, s->rhs.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s->stream));
+        CK(cudaMemcpyAsync(s->r.p, drhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s->stream));
     }
     CK(launch_init_sums(n, 1, s->x.p, s->r.p, s->diag.p, s->partials.p, s->ticket.p, s->sums.p, s->stream));
     s->launches += 1;
     CK(cudaMemcpyAsync(s->h_sums, s->sums.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
     const double r0 = sqrt(s->h_sums[0]), rz0 = s->h_sums[1];
-    if (!isfinite(rz0)) return fail(PHG_GPU_ERR_NAN, "phgGpuSolverPCG: zero or non-finite diagonal");
+    if (!isfinite(rz0)) return fail(PHG_GPU_ERR_NAN, "PCG: zero or non-finite diagonal");
     // get_tol (solver-phg.c:104-115)
     double tol = r0 * rtol;
     if (tol < rb * btol) tol = rb * btol;
@@ -621,13 +979,14 @@ int phgGpuSolverPCG(phgGpuSystem *s, double rtol, double btol, double atol, int 
 
     PcgBuffers B{A, s->x.p, s->r.p, s->p.p, s->Ap.p, s->diag.p, s->partials.p, s->st.p, dhist};
     phgGpuSystem_::GraphKey key{};
-    key.x = B.x; key.r = B.r; key.p = B.p; key.Ap = B.Ap; key.D = B.D; key.va = A.va; key.hist = dhist;
-    key.n = n; key.lpr = s->lpr; key.s = s->stream;
+    key.x = B.x; key.r = B.r; key.p = B.p; key.Ap = B.Ap; key.D = B.D; key.hist = dhist;
+    key.n = n; key.lpr = s->plan.kind * 100 + s->plan.lpr * 10 + s->plan.unroll; key.s = s->stream;
+    key.va = s->plan.kind == SPMV_CSR ? (const void *)s->va.p : (const void *)s->sell_vals.p;
     if (s->graph == nullptr || !(s->gkey == key)) {
         if (s->graph != nullptr) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; }
         cudaGraph_t gr;
         CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-        for (int i = 0; i < kGraphChunk; i++) launch_pcg_iteration(B, s->lpr, s->stream);
+        for (int i = 0; i < kGraphChunk; i++) launch_pcg_iteration_plan(B, s->plan, s->stream);
         CK(cudaStreamEndCapture(s->stream, &gr));
         cudaError_t e = cudaGraphInstantiate(&s->graph, gr, 0);
         cudaGraphDestroy(gr);
@@ -640,10 +999,7 @@ int phgGpuSolverPCG(phgGpuSystem *s, double rtol, double btol, double atol, int 
         CK(cudaMemcpyAsync(s->h_st, s->st.p, sizeof(PcgState), cudaMemcpyDeviceToHost, s->stream));
         CK(cudaStreamSynchronize(s->stream));
     }
-    CHECK_RC(copy_out(s, x, s->x.p, (size_t)n));
     const int nits = s->h_st->nits;
-    if (hist) CHECK_RC(copy_out(s, hist, dhist, (size_t)nits + 1));
-    CK(cudaStreamSynchronize(s->stream));
     if (residual) *residual = s->h_st->residual;
     if (s->h_st->status == PCG_BREAKDOWN)
         return fail(PHG_GPU_ERR_BREAKDOWN, "PCG breakdown after %d iterations: the matrix may not be SPD", nits);
@@ -652,4 +1008,228 @@ int phgGpuSolverPCG(phgGpuSystem *s, double rtol, double btol, double atol, int 
     return nits;
 }
 
+}  // namespace
+
+extern "C" {
+
+int phgGpuSolverPCG(phgGpuSystem *s, double rtol, double btol, double atol, int maxit, double *x,
+                    double *residual, double *hist) {
+    if (s == nullptr || x == nullptr) return fail(PHG_GPU_ERR_ARG, "invalid arguments");
+    if (!s->assembled) return fail(PHG_GPU_ERR_STATE, "no assembled system");
+    if (maxit < 0) return fail(PHG_GPU_ERR_ARG, "maxit < 0");
+    CHECK_RC(set_device(s));
+    CHECK_RC(solver_buffers(s));
+    const int64_t n = s->n;
+    CHECK_RC(copy_in(s, s->x.p, x, (size_t)n));
+    double *dhist = nullptr;
+    if (hist != nullptr) {
+        CHECK_RC(s->hist.ensure((size_t)maxit + 1));
+        dhist = s->hist.p;
+    }
+    const int nits = pcg_core(s, s->rhs.p, rtol, btol, atol, maxit, dhist, residual);
+    if (nits < 0) return nits;
+    CHECK_RC(copy_out(s, x, s->x.p, (size_t)n));
+    if (hist) CHECK_RC(copy_out(s, hist, dhist, (size_t)nits + 1));
+    CK(cudaStreamSynchronize(s->stream));
+    return nits;
+}
+
+int phgGpuAdjointGradient(phgGpuSystem *s, const double *u, const double *u_obs, double rtol, int maxit,
+                          double *grad, double *J, int *nits_out) {
+    if (s == nullptr || u == nullptr || u_obs == nullptr || grad == nullptr)
+        return fail(PHG_GPU_ERR_ARG, "invalid arguments");
+    if (!s->assembled || !s->have_bdry_cols)
+        return fail(PHG_GPU_ERR_STATE, "phgGpuAdjointGradient: needs a system built by phgGpuBuildLinearSystem");
+    if (maxit < 0) return fail(PHG_GPU_ERR_ARG, "maxit < 0");
+    CHECK_RC(set_device(s));
+    CHECK_RC(solver_buffers(s));
+    const int64_t n = s->n;
+    const double *du, *duo;
+    CHECK_RC(stage(s, u, (size_t)n, s->adj_u, &du));
+    CHECK_RC(stage(s, u_obs, (size_t)n, s->adj_uobs, &duo));
+    CHECK_RC(s->adj_rhs.ensure((size_t)n));
+    CHECK_RC(s->adj_lambda.ensure((size_t)n));
+    CHECK_RC(s->adj_grad.ensure((size_t)s->nelem));
+    // adjoint right-hand side dJ/du on the free DOFs, and J
+    CK(launch_adjoint_rhs(n, du, duo, s->bdry.p, s->adj_rhs.p, s->partials.p, s->sums.p, s->stream));
+    s->launches += 2;
+    double Jv = 0.0;
+    CK(cudaMemcpyAsync(&Jv, s->sums.p, sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    // the assembled matrix is symmetric (interior block + diagonal
+    // Dirichlet block), so the adjoint system uses it as is
+    CK(cudaMemsetAsync(s->x.p, 0, sizeof(double) * n, s->stream));
+    double res = 0.0;
+    const int nits = pcg_core(s, s->adj_rhs.p, rtol, 0.0, 0.0, maxit, nullptr, &res);
+    if (nits < 0) return nits;
+    CK(cudaMemcpyAsync(s->adj_lambda.p, s->x.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s->stream));
+    const bool gdev = is_device_ptr(grad);
+    double *dg = gdev ? grad : s->adj_grad.p;
+    CK(launch_adjoint_grad(s->order, s->nelem, s->e2l.p, s->Ke.p, s->adj_lambda.p, du, dg, s->stream));
+    s->launches += 1;
+    if (!gdev) CHECK_RC(copy_out(s, grad, dg, (size_t)s->nelem));
+    CK(cudaStreamSynchronize(s->stream));
+    if (J) *J = Jv;
+    if (nits_out) *nits_out = nits;
+    return PHG_GPU_OK;
+}
+
+
+int phgGpuSolverBlockPCG(phgGpuSystem *s, int nrhs, const double *B, double *X, double rtol, int maxit,
+                         int mixed, int *nits_out, double *res_out) {
+    if (s == nullptr || B == nullptr || X == nullptr || nrhs <= 0) return fail(PHG_GPU_ERR_ARG, "invalid arguments");
+    if (nrhs > 64) return fail(PHG_GPU_ERR_LIMIT, "phgGpuSolverBlockPCG: at most 64 right-hand sides per call");
+    if (!s->assembled) return fail(PHG_GPU_ERR_STATE, "no assembled system");
+    if (maxit < 0) return fail(PHG_GPU_ERR_ARG, "maxit < 0");
+    CHECK_RC(set_device(s));
+    CHECK_RC(solver_buffers(s));
+    const int64_t n = s->n;
+    int K = 8;   // padded column count: a power of two, at least one 8-column tile
+    while (K < nrhs) K <<= 1;
+    const size_t nk = (size_t)n * K;
+    CHECK_RC(s->bX.ensure(nk));
+    CHECK_RC(s->bR.ensure(nk));
+    CHECK_RC(s->bP.ensure(nk));
+    CHECK_RC(s->bAP.ensure(nk));
+    CHECK_RC(s->bB.ensure((size_t)n * nrhs));
+    CHECK_RC(s->bscal.ensure(7 * 64));
+    CHECK_RC(s->bint.ensure(3 * 64 + 8));
+    CHECK_RC(s->bpart.ensure(block_partials_doubles()));
+    if (s->btick.p == nullptr) {
+        CHECK_RC(s->btick.ensure(block_ticket_count()));
+        CK(cudaMemsetAsync(s->btick.p, 0, sizeof(unsigned) * block_ticket_count(), s->stream));
+    }
+    if (mixed) {
+        CHECK_RC(s->bY32.ensure(nk));
+        CHECK_RC(s->bR32.ensure(nk));
+        CHECK_RC(s->bP32.ensure(nk));
+        CHECK_RC(s->bAP32.ensure(nk));
+        CHECK_RC(s->bva32.ensure((size_t)s->nnz));
+        CHECK_RC(s->D32.ensure((size_t)n));
+        CK(launch_to_float(s->nnz, s->va.p, s->bva32.p, s->stream));
+        s->launches += 1;
+    }
+    BlockPtrs P{};
+    P.n = n;
+    P.K = K;
+    P.rp = s->rp.p;
+    P.ci = s->ci.p;
+    double *sc = s->bscal.p;
+    P.rz_cur = sc; P.rz_prev = sc + 64; P.alpha = sc + 128; P.res = sc + 192; P.tol = sc + 256;
+    P.maxr = sc + 320; P.pAp = sc + 384;
+    P.nits = s->bint.p; P.done = s->bint.p + 64; P.status = s->bint.p + 128; P.flags = s->bint.p + 192;
+    P.delta = 0.1;
+    P.partials = s->bpart.p;
+    P.tickets = s->btick.p;
+    BlockVecs V{};
+    V.va = s->va.p; V.D = s->diag.p; V.X = s->bX.p; V.R = s->bR.p; V.P = s->bP.p; V.AP = s->bAP.p;
+    V.va32 = s->bva32.p; V.D32 = s->D32.p; V.Y32 = s->bY32.p; V.R32 = s->bR32.p; V.P32 = s->bP32.p;
+    V.AP32 = s->bAP32.p;
+
+    // autotune the SpMM tile once per matrix shape and column count
+    if (!(s->btile != 0 && s->btile_n == n && s->btile_nnz == s->nnz && s->btile_K == K)) {
+        CK(cudaMemsetAsync(s->bP.p, 0, sizeof(double) * nk, s->stream));
+        CK(cudaMemsetAsync(s->bint.p, 0, sizeof(int) * (3 * 64 + 8), s->stream));   // flags: not done
+        cudaEvent_t a, b;
+        CK(cudaEventCreate(&a));
+        CK(cudaEventCreate(&b));
+        const int cand[4] = {8, 16, 32, 64};
+        int best = -1;
+        for (int c = 0; c < 4; c++) {
+            s->btile_ms[c] = 0.0;
+            if (cand[c] > K) continue;
+            for (int i = 0; i < 2; i++) {
+                if (mixed) CK(launch_block_spmm32(P, cand[c], s->bva32.p, s->bP32.p, s->bAP32.p, s->stream));
+                else CK(launch_block_spmm64(P, cand[c], s->va.p, s->bP.p, s->bAP.p, s->stream));
+            }
+            CK(cudaEventRecord(a, s->stream));
+            for (int i = 0; i < 3; i++) {
+                if (mixed) CK(launch_block_spmm32(P, cand[c], s->bva32.p, s->bP32.p, s->bAP32.p, s->stream));
+                else CK(launch_block_spmm64(P, cand[c], s->va.p, s->bP.p, s->bAP.p, s->stream));
+            }
+            CK(cudaEventRecord(b, s->stream));
+            CK(cudaEventSynchronize(b));
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, a, b));
+            s->btile_ms[c] = ms / 3;
+            s->launches += 5;
+            if (best < 0 || s->btile_ms[c] < s->btile_ms[best]) best = c;
+        }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        s->btile = cand[best < 0 ? 0 : best];
+        s->btile_n = n; s->btile_nnz = s->nnz; s->btile_K = K;
+    }
+    const int T = s->btile;
+
+    // R = B (zero initial guess), X = 0
+    const double *dB;
+    CHECK_RC(stage(s, B, (size_t)n * nrhs, s->bB, &dB));
+    CK(launch_block_pack(n, nrhs, K, dB, s->bR.p, s->stream));
+    CK(cudaMemsetAsync(s->bX.p, 0, sizeof(double) * nk, s->stream));
+    int hflags[8] = {0, 0, 0, 1, maxit, 0, 0, 0};
+    CK(cudaMemcpyAsync(P.flags, hflags, sizeof(hflags), cudaMemcpyHostToDevice, s->stream));
+    CK(launch_block_init(P, mixed != 0, s->bR.p, s->diag.p, s->bR32.p, s->D32.p, s->bY32.p, rtol, s->stream));
+    s->launches += 2;
+
+    phgGpuSystem_::GraphKey key{};
+    key.x = s->bX.p; key.r = s->bR.p; key.p = mixed ? (const void *)s->bP32.p : (const void *)s->bP.p;
+    key.Ap = s->bva32.p; key.D = s->diag.p; key.va = s->va.p; key.hist = s->bpart.p;
+    key.n = n; key.lpr = T * 1000 + K * 2 + (mixed ? 1 : 0); key.s = s->stream;
+    if (s->graph_block == nullptr || !(s->gkey_block == key)) {
+        if (s->graph_block != nullptr) { cudaGraphExecDestroy(s->graph_block); s->graph_block = nullptr; }
+        cudaGraph_t gr;
+        CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+        for (int i = 0; i < kGraphChunk; i++) launch_block_iteration(P, T, mixed != 0, V, s->stream);
+        CK(cudaStreamEndCapture(s->stream, &gr));
+        cudaError_t e = cudaGraphInstantiate(&s->graph_block, gr, 0);
+        cudaGraphDestroy(gr);
+        CK(e);
+        s->gkey_block = key;
+    }
+    int all_done = 0;
+    CK(cudaMemcpyAsync(&all_done, P.flags, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    while (!all_done) {
+        CK(cudaGraphLaunch(s->graph_block, s->stream));
+        s->launches += (mixed ? 4 : 3) * kGraphChunk;
+        CK(cudaMemcpyAsync(&all_done, P.flags, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+    }
+    // iteration counts and status, then the explicit FP64 residual B - A X per column
+    std::vector<int> hint(3 * 64);
+    CK(cudaMemcpyAsync(hint.data(), P.nits, sizeof(int) * 3 * 64, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    CK(cudaMemsetAsync(P.flags, 0, sizeof(int), s->stream));   // the kernels skip work once all are done
+    CK(launch_block_spmm64(P, T, s->va.p, s->bX.p, s->bAP.p, s->stream));
+    CK(launch_block_pack(n, nrhs, K, dB, s->bR.p, s->stream));
+    CK(launch_block_sub((int64_t)nk, s->bR.p, s->bAP.p, s->stream));   // AP = R - AP
+    CK(launch_block_init(P, false, s->bAP.p, s->diag.p, nullptr, nullptr, nullptr, 0.0, s->stream));
+    s->launches += 4;
+    std::vector<double> hres(64);
+    CK(cudaMemcpyAsync(hres.data(), P.res, sizeof(double) * 64, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    const bool xdev = is_device_ptr(X);
+    double *dX = xdev ? X : s->bB.p;
+    CK(launch_block_unpack(n, nrhs, K, s->bX.p, dX, s->stream));
+    if (!xdev) CHECK_RC(copy_out(s, X, dX, (size_t)n * nrhs));
+    CK(cudaStreamSynchronize(s->stream));
+    if (res_out)
+        for (int k = 0; k < nrhs; k++) res_out[k] = hres[k];
+    if (nits_out)
+        for (int k = 0; k < nrhs; k++) nits_out[k] = hint[k];
+    for (int k = 0; k < nrhs; k++) {
+        if (hint[128 + k] == 1) return fail(PHG_GPU_ERR_BREAKDOWN, "block PCG: breakdown in column %d", k);
+        if (hint[128 + k] == 2) return fail(PHG_GPU_ERR_NAN, "block PCG: non-finite residual in column %d", k);
+    }
+    return PHG_GPU_OK;
+}
+
+int phgGpuGetBlockTile(phgGpuSystem *s, int *tile, double *times_ms) {
+    if (s == nullptr) return fail(PHG_GPU_ERR_ARG, "null system");
+    if (s->btile == 0) return fail(PHG_GPU_ERR_STATE, "no block solve yet");
+    if (tile) *tile = s->btile;
+    if (times_ms)
+        for (int c = 0; c < 4; c++) times_ms[c] = s->btile_ms[c];
+    return PHG_GPU_OK;
+}
 }  // extern "C"

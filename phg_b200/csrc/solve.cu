@@ -244,4 +244,320 @@ cudaError_t launch_residual(int64_t n, const double *b, const double *y, double 
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// SELL-C-sigma layout (C = 32 rows per slice, rows sorted by length inside
+// windows of sigma = 256 rows).  Slice s stores entry j of its lane l at
+// sptr[s] + 32 j + l: a warp reads 32 consecutive values (one 256-byte
+// stream for FP64) per step, one thread per row, no shuffles.  Each thread
+// stops at its own row length, so the padding is never read.
+constexpr int kSellWin = 256;
+
+__global__ void __launch_bounds__(kSellWin)
+sell_sort_kernel(int64_t n, const int32_t *__restrict__ rp, int32_t *__restrict__ perm,
+                 uint16_t *__restrict__ len, int32_t *__restrict__ slice_size) {
+    __shared__ int32_t key[kSellWin];
+    const int i = threadIdx.x;
+    const int64_t base = (int64_t)blockIdx.x * kSellWin, row = base + i;
+    const int32_t l = row < n ? rp[row + 1] - rp[row] : 0;
+    key[i] = l * kSellWin + (kSellWin - 1 - i);   // unique; descending = long rows first, then row order
+    __syncthreads();
+    // bitonic sort, descending
+    for (int k = 2; k <= kSellWin; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const int p = i ^ j;
+            if (p > i) {
+                const bool desc = (i & k) == 0;
+                const int32_t a = key[i], b = key[p];
+                if (desc ? (a < b) : (a > b)) { key[i] = b; key[p] = a; }
+            }
+            __syncthreads();
+        }
+    }
+    const int32_t kk = key[i];
+    const int src = kSellWin - 1 - (kk % kSellWin);
+    const int32_t li = kk / kSellWin;
+    perm[base + i] = base + src < n ? (int32_t)(base + src) : -1;
+    len[base + i] = (uint16_t)li;
+    if ((i & 31) == 0) slice_size[(base + i) >> 5] = 32 * li;   // the slice's first row is its longest
+}
+
+template <typename VT>
+__global__ void sell_fill_kernel(int64_t npos, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
+                                 const double *__restrict__ va, const int32_t *__restrict__ perm,
+                                 const uint16_t *__restrict__ len, const int32_t *__restrict__ sptr,
+                                 int32_t *__restrict__ cols, VT *__restrict__ vals, float *__restrict__ vals32) {
+    for (int64_t pos = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pos < npos;
+         pos += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t row = perm[pos];
+        if (row < 0) continue;
+        const int l = len[pos];
+        const int64_t b = (int64_t)sptr[pos >> 5] + (pos & 31);
+        const int32_t r0 = rp[row];
+        for (int j = 0; j < l; j++) {
+            cols[b + 32 * j] = ci[r0 + j];
+            const double v = va[r0 + j];
+            vals[b + 32 * j] = (VT)v;
+            if (vals32 != nullptr) vals32[b + 32 * j] = (float)v;
+        }
+    }
+}
+
+template <typename VT, bool DOT, int U>
+__global__ void __launch_bounds__(kVecThreads)
+sell_spmv_kernel(int64_t nslices, const int32_t *__restrict__ perm, const uint16_t *__restrict__ len,
+                 const int32_t *__restrict__ sptr, const int32_t *__restrict__ cols, const VT *__restrict__ vals,
+                 const VT *__restrict__ x, VT *__restrict__ y, double *partials, PcgState *st) {
+    if (DOT && st->done) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * kVecThreads + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * kVecThreads) >> 5;
+    double dot = 0.0, dummy = 0.0;
+    for (int64_t s = warp; s < nslices; s += nwarps) {
+        const int64_t pos = s * 32 + lane;
+        const int32_t row = perm[pos];
+        const int l = len[pos];
+        const int w = __shfl_sync(0xffffffffu, l, 0);
+        const int64_t b = (int64_t)sptr[s] + lane;
+        VT acc = (VT)0;   // FP32 SpMV accumulates in FP32, FP64 in FP64
+        for (int j = 0; j < w; j += U) {
+            int32_t c[U];
+            VT v[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const bool ok = j + u < l;
+                c[u] = ok ? __ldcs(&cols[b + 32 * (j + u)]) : 0;
+                v[u] = ok ? __ldcs(&vals[b + 32 * (j + u)]) : (VT)0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++)
+                if (j + u < l) acc += v[u] * __ldg(&x[c[u]]);
+        }
+        if (row >= 0) {
+            y[row] = (VT)acc;
+            if (DOT) dot += (double)x[row] * (double)(VT)acc;
+        }
+    }
+    if (!DOT) return;
+    if (grid_sum2(dot, dummy, partials, &st->ticket) && threadIdx.x == 0) {
+        const int k = st->nits + 1;
+        st->pAp = dot;
+        if (dot == 0.0) {
+            st->done = 1;
+            st->status = PCG_BREAKDOWN;
+            st->nits = k;
+        } else {
+            st->alpha = st->rz_cur / dot;
+        }
+    }
+}
+
+int64_t sell_positions(int64_t n) { return ceil_div(n, kSellWin) * kSellWin; }
+
+cudaError_t launch_sell_sort(int64_t n, const int32_t *rp, int32_t *perm, uint16_t *len, int32_t *slice_size,
+                             cudaStream_t s) {
+    sell_sort_kernel<<<(unsigned)ceil_div(n, kSellWin), kSellWin, 0, s>>>(n, rp, perm, len, slice_size);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sell_fill(int64_t n, const int32_t *rp, const int32_t *ci, const double *va, const int32_t *perm,
+                             const uint16_t *len, const int32_t *sptr, int32_t *cols, double *vals, float *vals32,
+                             cudaStream_t s) {
+    const int64_t npos = sell_positions(n);
+    sell_fill_kernel<double><<<vec_blocks(npos), kVecThreads, 0, s>>>(npos, rp, ci, va, perm, len, sptr, cols,
+                                                                      vals, vals32);
+    return cudaGetLastError();
+}
+
+template <bool DOT, typename VT>
+static void plan_spmv(const SpmvPlan &P, const VT *vals, const VT *x, VT *y, double *partials, PcgState *st,
+                      cudaStream_t s) {
+    if (P.kind == SPMV_CSR) {
+        spmv_dispatch<DOT, VT>(P.lpr, P.csr.n, P.csr.rp, P.csr.ci, vals, x, y, partials, st, s);
+        return;
+    }
+    const SellView &S = P.sell;
+    const int blocks = vec_blocks(S.nslices * 32);
+    switch (P.unroll) {
+    case 2: sell_spmv_kernel<VT, DOT, 2><<<blocks, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, vals, x, y, partials, st); break;
+    case 8: sell_spmv_kernel<VT, DOT, 8><<<blocks, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, vals, x, y, partials, st); break;
+    default: sell_spmv_kernel<VT, DOT, 4><<<blocks, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, vals, x, y, partials, st); break;
+    }
+}
+
+cudaError_t launch_spmv_plan(const SpmvPlan &P, const double *x, double *y, cudaStream_t s) {
+    plan_spmv<false, double>(P, P.kind == SPMV_CSR ? P.csr.va : P.sell.vals, x, y, nullptr, nullptr, s);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pcg_iteration_plan(const PcgBuffers &B, const SpmvPlan &P, cudaStream_t s) {
+    const int vb = vec_blocks(B.A.n);
+    pcg_dir_kernel<double><<<vb, kVecThreads, 0, s>>>(B.A.n, B.r, B.D, B.p, B.st);
+    plan_spmv<true, double>(P, P.kind == SPMV_CSR ? P.csr.va : P.sell.vals, B.p, B.Ap, B.partials, B.st, s);
+    pcg_update_kernel<double, double><<<vb, kVecThreads, 0, s>>>(B.A.n, B.x, B.r, B.p, B.Ap, B.D, B.partials,
+                                                                B.st, B.hist);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Mixed precision: FP32 PCG with reliable updates inside FP64 refinement.
+//
+// The Krylov vectors (r, p, Ap and the correction y) and the SpMV are FP32;
+// every dot product accumulates in FP64.  The FP64 solution x and the FP64
+// residual r_true = b - A x are brought up to date by a "reliable update"
+// whenever the iterated FP32 residual has dropped by `delta` since the last
+// update (and before the iteration may stop): x += y, r_true -= A y in FP64,
+// and the FP32 residual is replaced by the rounded r_true.  The search
+// direction is kept, so the iteration does not restart and converges like the
+// FP64 recurrence.  The stopping rule is the reference's, applied to the FP64
+// residual.  Kernels per iteration: dir32, SpMV32 (+ p.Ap), update32, and the
+// reliable update (returns at once unless flagged).
+
+__global__ void __launch_bounds__(kVecThreads)
+mixed_update_kernel(int64_t n, float *__restrict__ y, float *__restrict__ r, const float *__restrict__ p,
+                    const float *__restrict__ Ap, const float *__restrict__ D, double *partials, MixedState *ms) {
+    PcgState *st = &ms->pcg;
+    if (st->done) return;
+    const float a = (float)st->alpha;
+    const bool reset = ms->y_reset != 0;
+    double rr = 0.0, rz = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        y[i] = (reset ? 0.0f : y[i]) + a * p[i];
+        const float ri = r[i] - a * Ap[i];
+        r[i] = ri;
+        rr += (double)ri * (double)ri;
+        rz += (double)ri * (double)(ri / D[i]);
+    }
+    if (grid_sum2(rr, rz, partials, &st->ticket) && threadIdx.x == 0) {
+        const int k = st->nits + 1;
+        const double res = sqrt(rr);
+        st->nits = k;
+        st->residual = res;
+        st->rz_prev = st->rz_cur;
+        st->rz_cur = rz;
+        ms->y_reset = 0;
+        if (!isfinite(res)) {
+            st->done = 1;
+            st->status = PCG_NONFINITE;
+        } else if (!(res > st->tol) || k >= st->maxit) {
+            ms->ru_flag = 1;
+            ms->final_check = 1;
+        } else if (res < ms->delta * ms->maxr) {
+            ms->ru_flag = 1;
+        }
+    }
+}
+
+// Reliable update on the SELL layout (FP64 values): x += y, r_true -= A y,
+// r32 = (float) r_true, ||r_true||^2 and r32.(r32/D).
+template <int U>
+__global__ void __launch_bounds__(kVecThreads)
+mixed_reliable_kernel(int64_t nslices, const int32_t *__restrict__ perm, const uint16_t *__restrict__ len,
+                      const int32_t *__restrict__ sptr, const int32_t *__restrict__ cols,
+                      const double *__restrict__ vals, double *__restrict__ x, const float *__restrict__ y,
+                      double *__restrict__ rtrue, float *__restrict__ r32, const float *__restrict__ D,
+                      double *partials, MixedState *ms, double *hist) {
+    PcgState *st = &ms->pcg;
+    if (st->done || !ms->ru_flag) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * kVecThreads + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * kVecThreads) >> 5;
+    double rr = 0.0, rz = 0.0;
+    for (int64_t s = warp; s < nslices; s += nwarps) {
+        const int64_t pos = s * 32 + lane;
+        const int32_t row = perm[pos];
+        const int l = len[pos];
+        const int w = __shfl_sync(0xffffffffu, l, 0);
+        const int64_t b = (int64_t)sptr[s] + lane;
+        double acc = 0.0;
+        for (int j = 0; j < w; j += U) {
+            int32_t c[U];
+            double v[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const bool ok = j + u < l;
+                c[u] = ok ? __ldcs(&cols[b + 32 * (j + u)]) : 0;
+                v[u] = ok ? __ldcs(&vals[b + 32 * (j + u)]) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++)
+                if (j + u < l) acc += v[u] * (double)__ldg(&y[c[u]]);
+        }
+        if (row >= 0) {
+            x[row] += (double)y[row];
+            const double rt = rtrue[row] - acc;
+            rtrue[row] = rt;
+            const float rf = (float)rt;
+            r32[row] = rf;
+            rr += rt * rt;
+            rz += (double)rf * (double)(rf / D[row]);
+        }
+    }
+    if (grid_sum2(rr, rz, partials, &st->ticket) && threadIdx.x == 0) {
+        const double res = sqrt(rr);
+        st->residual = res;
+        st->rz_cur = rz;
+        ms->maxr = res;
+        ms->y_reset = 1;
+        ms->ru_flag = 0;
+        ms->nupdates += 1;
+        if (hist != nullptr) hist[st->nits] = res;
+        if (ms->final_check) {
+            ms->final_check = 0;
+            if (!(res > st->tol) || st->nits >= st->maxit) st->done = 1;
+        }
+    }
+}
+
+// r32 = (float) rtrue, y = 0, and (||rtrue||^2, r32.(r32/D)).
+__global__ void __launch_bounds__(kVecThreads)
+mixed_init_kernel(int64_t n, const double *__restrict__ rtrue, float *__restrict__ r32, float *__restrict__ y,
+                  const double *__restrict__ D64, float *__restrict__ D32, double *partials, unsigned *ticket,
+                  double *out) {
+    double rr = 0.0, rz = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double rt = rtrue[i];
+        const float rf = (float)rt, df = (float)D64[i];
+        r32[i] = rf;
+        y[i] = 0.0f;
+        D32[i] = df;
+        rr += rt * rt;
+        rz += (double)rf * (double)(rf / df);
+    }
+    if (grid_sum2(rr, rz, partials, ticket) && threadIdx.x == 0) { out[0] = rr; out[1] = rz; }
+}
+
+cudaError_t launch_mixed_init(int64_t n, const double *rtrue, float *r32, float *y, const double *D64, float *D32,
+                              double *partials, unsigned *ticket, double *out, cudaStream_t s) {
+    mixed_init_kernel<<<vec_blocks(n), kVecThreads, 0, s>>>(n, rtrue, r32, y, D64, D32, partials, ticket, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_spmv32(const SellView &S, int unroll, const float *x, float *y, cudaStream_t s) {
+    const int sb = vec_blocks(S.nslices * 32);
+    switch (unroll) {
+    case 2: sell_spmv_kernel<float, false, 2><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals32, x, y, nullptr, nullptr); break;
+    case 8: sell_spmv_kernel<float, false, 8><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals32, x, y, nullptr, nullptr); break;
+    case 16: sell_spmv_kernel<float, false, 16><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals32, x, y, nullptr, nullptr); break;
+    default: sell_spmv_kernel<float, false, 4><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals32, x, y, nullptr, nullptr); break;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mixed_iteration(const MixedBuffers &B, const SellView &S, int unroll, cudaStream_t s) {
+    const int vb = vec_blocks(B.n);
+    PcgState *st = &B.ms->pcg;
+    pcg_dir_kernel<float><<<vb, kVecThreads, 0, s>>>(B.n, B.r32, B.D32, B.p32, st);
+    const int sb = vec_blocks(S.nslices * 32);
+    switch (unroll) {
+    case 2: sell_spmv_kernel<float, true, 2><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals32, B.p32, B.Ap32, B.partials, st); break;
+    case 8: sell_spmv_kernel<float, true, 8><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals32, B.p32, B.Ap32, B.partials, st); break;
+    case 16: sell_spmv_kernel<float, true, 16><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals32, B.p32, B.Ap32, B.partials, st); break;
+    default: sell_spmv_kernel<float, true, 4><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals32, B.p32, B.Ap32, B.partials, st); break;
+    }
+    mixed_update_kernel<<<vb, kVecThreads, 0, s>>>(B.n, B.y32, B.r32, B.p32, B.Ap32, B.D32, B.partials, B.ms);
+    mixed_reliable_kernel<4><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals, B.x, B.y32,
+                                                         B.rtrue, B.r32, B.D32, B.partials, B.ms, B.hist);
+    return cudaGetLastError();
+}
+
 }  // namespace phgb

@@ -30,7 +30,56 @@ struct PcgBuffers {
     double *hist;         // may be null
 };
 
+// SpMV layouts: CSR with `lpr` lanes per row, or SELL-C-sigma (C = 32,
+// sigma = 256) with the inner loop unrolled `unroll` times.
+enum { SPMV_CSR = 0, SPMV_SELL = 1 };
+
+struct SellView {
+    int64_t n, nslices;
+    const int32_t *perm;      // sorted position -> row, -1 for padding positions
+    const uint16_t *len;      // row length at each sorted position
+    const int32_t *sptr;      // slice offsets (nslices + 1)
+    const int32_t *cols;
+    const double *vals;
+    const float *vals32;      // FP32 copy of the values (mixed precision), may be null
+};
+
+struct SpmvPlan {
+    int kind = SPMV_CSR, lpr = 8, unroll = 4;
+    CsrView csr{};
+    SellView sell{};
+};
+
+// State of the mixed-precision PCG (FP32 Krylov vectors, FP64 x and
+// residual); `pcg` comes first so the FP32 SpMV kernel can update it.
+struct MixedState {
+    PcgState pcg;
+    double maxr, delta;
+    int ru_flag, final_check, y_reset, nupdates;
+};
+
+struct MixedBuffers {
+    int64_t n;
+    double *x, *rtrue;
+    float *r32, *p32, *Ap32, *y32, *D32;
+    double *partials;
+    MixedState *ms;
+    double *hist;
+};
+
 int vec_blocks(int64_t n);
+cudaError_t launch_mixed_init(int64_t n, const double *rtrue, float *r32, float *y, const double *D64, float *D32,
+                              double *partials, unsigned *ticket, double *out, cudaStream_t s);
+cudaError_t launch_spmv32(const SellView &S, int unroll, const float *x, float *y, cudaStream_t s);
+cudaError_t launch_mixed_iteration(const MixedBuffers &B, const SellView &S, int unroll, cudaStream_t s);
+int64_t sell_positions(int64_t n);   // perm/len entries = slices * 32
+cudaError_t launch_sell_sort(int64_t n, const int32_t *rp, int32_t *perm, uint16_t *len, int32_t *slice_size,
+                             cudaStream_t s);
+cudaError_t launch_sell_fill(int64_t n, const int32_t *rp, const int32_t *ci, const double *va, const int32_t *perm,
+                             const uint16_t *len, const int32_t *sptr, int32_t *cols, double *vals, float *vals32,
+                             cudaStream_t s);
+cudaError_t launch_spmv_plan(const SpmvPlan &P, const double *x, double *y, cudaStream_t s);
+cudaError_t launch_pcg_iteration_plan(const PcgBuffers &B, const SpmvPlan &P, cudaStream_t s);
 int spmv_lanes_for(double avg_nnz_per_row);
 cudaError_t launch_spmv(const CsrView &A, int lpr, const double *x, double *y, cudaStream_t s);
 cudaError_t launch_pcg_iteration(const PcgBuffers &B, int lpr, cudaStream_t s);

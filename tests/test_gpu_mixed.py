@@ -1,0 +1,89 @@
+"""SpMV layouts and the mixed-precision (FP32 inner / FP64 refinement) PCG."""
+import numpy as np
+import pytest
+
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def system(pb, p, m, kappa_seed=None):
+    v, e = pb.kuhn_cube(m)
+    e2l, bdry, nodes = pb.lagrange_dofs(v, e, p)
+    f = pb.sine_source(nodes)
+    kappa = None
+    if kappa_seed is not None:
+        kappa = np.exp(0.5 * np.random.default_rng(kappa_seed).standard_normal(len(e)))
+    s = pb.Solver(0)
+    s.set_mesh(v, e)
+    s.set_dof_map(p, e2l, bdry)
+    s.build_linear_system(kappa=kappa, f=f)
+    return s
+
+
+@pytest.mark.parametrize("layout,param", [("csr", 4), ("csr", 8), ("csr", 16), ("csr", 32),
+                                          ("sell", 2), ("sell", 4), ("sell", 8)])
+def test_every_spmv_layout_matches_oracle(gpu, oracle, layout, param):
+    for name in ("p2_m6_sine", "p3_m3_kappa", "p1_m5_kappa"):
+        G = load_golden(name)
+        s = gpu.Solver(0)
+        s.set_matrix(G["rows_ptr"], G["rows_cols"], G["rows_vals"], G["rhs"])
+        s.set_spmv_plan(layout, param)
+        x = np.random.default_rng(3).standard_normal(len(G["rhs"]))
+        y = s.mat_vec(x)
+        yo = oracle.spmv(G["rows_ptr"], G["rows_cols"], G["rows_vals"], x)
+        assert np.allclose(y, yo, rtol=1e-13, atol=1e-13 * np.abs(yo).max()), (name, layout, param)
+        # PCG through the same layout
+        xs, nits, _ = s.solve_pcg(rtol=float(G["rtol"]), btol=0.0, atol=0.0)
+        assert abs(nits - int(G["nits"])) <= 2
+        assert np.linalg.norm(xs - G["x"]) <= 1e3 * float(G["rtol"]) * np.linalg.norm(G["x"])
+        s.close()
+
+
+def test_autotuner_reports_a_choice(gpu):
+    s = system(gpu, 2, 8)
+    s.solve_pcg(rtol=1e-8, btol=0.0, atol=0.0)
+    layout, param, times = s.spmv_plan()
+    assert (layout, param) in gpu.Solver.SPMV_LAYOUTS
+    assert all(times[k] > 0 for k in ("csr4", "csr8", "csr16", "csr32", "sell_u2", "sell_u4", "sell_u8"))
+    s.close()
+
+
+@pytest.mark.parametrize("p,m,seed", [(1, 32, None), (2, 12, None), (2, 10, 7), (3, 6, 9)])
+def test_mixed_precision_reaches_fp64_tolerance(gpu, oracle, p, m, seed):
+    """Tolerances: the FP64 residual ||b - A x|| (recomputed here by the oracle
+    in FP64) meets the reference's stopping rule; the solution is as close to
+    the tightly converged FP64 solution as the FP64 PCG result at the same
+    rtol is, within a factor of 10 (+ 1e-12 relative)."""
+    rtol = 1e-8
+    s = system(gpu, p, m, seed)
+    ptr, cols, vals = s.get_matrix()
+    rhs, diag = s.get_rhs(), s.get_diagonal()
+    x64, n64, _ = s.solve_pcg(rtol=rtol, btol=0.0, atol=0.0)
+    xm, nm, res, nupd = s.solve_pcg_mixed(rtol=rtol, btol=0.0, atol=0.0)
+    r = rhs - oracle.spmv(ptr, cols, vals, xm)
+    assert np.linalg.norm(r) <= rtol * np.linalg.norm(rhs) * (1 + 1e-9)
+    assert abs(res - np.linalg.norm(r)) <= 1e-6 * res + 1e-300
+    xt, _, _, _ = oracle.pcg(ptr, cols, vals, diag, rhs, rtol=1e-13, btol=0.0, atol=0.0)
+    e64 = np.linalg.norm(x64 - xt) / np.linalg.norm(xt)
+    em = np.linalg.norm(xm - xt) / np.linalg.norm(xt)
+    print("p=%d m=%d: fp64 %d its err %.2e, mixed %d its (%d updates) err %.2e"
+          % (p, m, n64, e64, nm, nupd, em))
+    assert em <= 10 * e64 + 1e-12
+    assert nm <= 1.5 * n64 + 5
+    s.close()
+
+
+def test_mixed_zero_rhs_and_breakdown(gpu):
+    G = load_golden("p2_m3_sine")
+    s = gpu.Solver(0)
+    s.set_matrix(G["rows_ptr"], G["rows_cols"], G["rows_vals"], np.zeros_like(G["rhs"]))
+    x, nits, res, _ = s.solve_pcg_mixed(x0=np.ones(len(G["rhs"])))
+    assert nits == 0 and not x.any()
+    s.close()
+    s = gpu.Solver(0)
+    s.set_matrix(np.array([0, 1, 2]), np.array([0, 1], np.int32), np.array([1.0, -1.0]), np.array([1.0, 1.0]))
+    with pytest.raises(gpu.PhgGpuError) as ei:
+        s.solve_pcg_mixed(rtol=1e-10)
+    assert ei.value.code == -5
+    s.close()
