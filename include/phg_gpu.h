@@ -172,10 +172,12 @@ int phgGpuSolverPCGMixed(phgGpuSystem *sys, double rtol, double btol,
  * shape it times CSR with 4/8/16/32 lanes per row and SELL-C-sigma (32-row
  * slices, rows sorted by length in 256-row windows) with 2/4/8-fold
  * unrolling, and keeps the fastest.  kind: 0 = CSR (param = lanes per row),
- * 1 = SELL (param = unroll); times_ms (optional, 11 doubles) gets the
+ * 1 = SELL (param = unroll); times_ms (optional, 15 doubles) gets the
  * measured time of each candidate in that order, then the times of the FP32
- * SELL product (mixed solver) unrolled 4/8/16 times and the unroll chosen
- * for it (0 before a mixed solve).  Returns the number of FP64 candidates. */
+ * products of the mixed solver (SELL unrolled 4/8/16, pair-SELL -- two
+ * consecutive entries per lane -- unrolled 2/4/8), the unroll chosen for it
+ * and its layout (0 SELL, 1 pair SELL); 0 before a mixed solve.  Returns the
+ * number of FP64 candidates. */
 int phgGpuGetSpMVPlan(phgGpuSystem *sys, int *kind, int *param,
 		      double *times_ms);
 

@@ -246,12 +246,15 @@ class Solver:
     def spmv_plan(self):
         """(layout, parameter, {candidate: ms}) chosen by the SpMV autotuner."""
         kind, param = C.c_int(), C.c_int()
-        times = np.zeros(16)
+        times = np.zeros(24)
         nc = _check(lib().phgGpuGetSpMVPlan(self._h, C.byref(kind), C.byref(param), _ptr(times)))
         names = ["csr4", "csr8", "csr16", "csr32", "sell_u2", "sell_u4", "sell_u8"][:nc]
         info = dict(zip(names, times[:nc].tolist()))
-        info.update({"fp32_sell_u4": times[nc], "fp32_sell_u8": times[nc + 1], "fp32_sell_u16": times[nc + 2],
-                     "fp32_unroll": int(times[nc + 3])})
+        for i, name in enumerate(("fp32_sell_u4", "fp32_sell_u8", "fp32_sell_u16", "fp32_pair_u2",
+                                  "fp32_pair_u4", "fp32_pair_u8")):
+            info[name] = float(times[nc + i])
+        info["fp32_unroll"] = int(times[nc + 6])
+        info["fp32_layout"] = "pair" if int(times[nc + 7]) == 1 else "sell"
         return ("csr" if kind.value == 0 else "sell"), param.value, info
 
     def launch_count(self):

@@ -192,8 +192,12 @@ struct phgGpuSystem_ {
     DevBuf<float> sell_vals32;
     bool tuned = false;
     int64_t tuned_n = -1, tuned_nnz = -1;
-    int unroll32 = 0;                 // FP32 SELL unroll (0: not tuned yet)
-    double tune32_ms[3] = {};
+    int unroll32 = 0;                 // FP32 product unroll (0: not tuned yet)
+    int kind32 = 0;                   // FP32 product layout: 0 SELL, 1 pair SELL
+    double tune32_ms[6] = {};
+    bool sell2_valid = false;
+    DevBuf<int32_t> sell2_ssz, sell2_sptr, sell2_cols;
+    DevBuf<float> sell2_vals;
     double tune_ms[kTuneCandidates] = {};
 
     // mixed-precision solver
@@ -321,25 +325,57 @@ int ensure_sell(phgGpuSystem *s) {
     return PHG_GPU_OK;
 }
 
-// Unroll depth of the FP32 SELL SpMV (mixed solver): 4, 8 or 16, timed once
-// per matrix shape.
+// The FP32 pair layout (mixed solver), built from the SELL slices.
+int ensure_sell2(phgGpuSystem *s) {
+    if (s->sell2_valid) return PHG_GPU_OK;
+    const int64_t nsl = sell_positions(s->n) / 32;
+    CHECK_RC(s->sell2_ssz.ensure((size_t)nsl));
+    CHECK_RC(s->sell2_sptr.ensure((size_t)nsl + 1));
+    CHECK_RC(s->scan_ws.ensure((size_t)scan_workspace_elems(nsl)));
+    const SellView S{s->n, nsl, s->sell_perm.p, s->sell_len.p, s->sell_sptr.p, s->sell_cols.p, s->sell_vals.p,
+                     s->sell_vals32.p};
+    CK(launch_sell2_sizes(S, s->sell2_ssz.p, s->stream));
+    CK(launch_scan(nsl, s->sell2_ssz.p, s->sell2_sptr.p, s->scan_ws.p, s->stream));
+    int32_t total = 0;
+    CK(cudaMemcpyAsync(&total, s->sell2_sptr.p + nsl, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    if (total < 0) return fail(PHG_GPU_ERR_LIMIT, "pair SELL layout larger than 2^31 entries");
+    CHECK_RC(s->sell2_cols.ensure((size_t)total));
+    CHECK_RC(s->sell2_vals.ensure((size_t)total));
+    CK(launch_sell2_fill(S, s->rp.p, s->ci.p, s->va.p, s->sell2_sptr.p, s->sell2_cols.p, s->sell2_vals.p, s->stream));
+    s->launches += 5;
+    s->sell2_valid = true;
+    return PHG_GPU_OK;
+}
+
+SellView sell_view(phgGpuSystem *s) {
+    return SellView{s->n, sell_positions(s->n) / 32, s->sell_perm.p, s->sell_len.p, s->sell_sptr.p,
+                    s->sell_cols.p, s->sell_vals.p, s->sell_vals32.p};
+}
+
+Sell2View sell2_view(phgGpuSystem *s) { return Sell2View{s->sell2_sptr.p, s->sell2_cols.p, s->sell2_vals.p}; }
+
+// Layout and unroll of the FP32 product (mixed solver), timed once per
+// matrix shape: SELL unrolled 4/8/16, pair SELL unrolled 2/4/8.
 int tune_spmv32(phgGpuSystem *s) {
+    CHECK_RC(ensure_sell(s));
+    CHECK_RC(ensure_sell2(s));
     if (s->unroll32 != 0 && s->tuned_n == s->n && s->tuned_nnz == s->nnz) return PHG_GPU_OK;
     CHECK_RC(s->r32.ensure((size_t)s->n));
     CHECK_RC(s->Ap32.ensure((size_t)s->n));
     CK(cudaMemsetAsync(s->r32.p, 0, sizeof(float) * s->n, s->stream));
-    const SellView S{s->n, sell_positions(s->n) / 32, s->sell_perm.p, s->sell_len.p, s->sell_sptr.p,
-                     s->sell_cols.p, s->sell_vals.p, s->sell_vals32.p};
+    const SellView S = sell_view(s);
+    const Sell2View S2 = sell2_view(s);
     cudaEvent_t a, b;
     CK(cudaEventCreate(&a));
     CK(cudaEventCreate(&b));
-    const int cand[3] = {4, 8, 16};
+    const int ckind[6] = {0, 0, 0, 1, 1, 1}, cu[6] = {4, 8, 16, 2, 4, 8};
     int best = 0;
     const int reps = 5;
-    for (int c = 0; c < 3; c++) {
-        for (int i = 0; i < 2; i++) CK(launch_spmv32(S, cand[c], s->r32.p, s->Ap32.p, s->stream));
+    for (int c = 0; c < 6; c++) {
+        for (int i = 0; i < 2; i++) CK(launch_spmv32k(S, S2, ckind[c], cu[c], s->r32.p, s->Ap32.p, s->stream));
         CK(cudaEventRecord(a, s->stream));
-        for (int i = 0; i < reps; i++) CK(launch_spmv32(S, cand[c], s->r32.p, s->Ap32.p, s->stream));
+        for (int i = 0; i < reps; i++) CK(launch_spmv32k(S, S2, ckind[c], cu[c], s->r32.p, s->Ap32.p, s->stream));
         CK(cudaEventRecord(b, s->stream));
         CK(cudaEventSynchronize(b));
         float ms = 0;
@@ -350,7 +386,8 @@ int tune_spmv32(phgGpuSystem *s) {
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    s->unroll32 = cand[best];
+    s->kind32 = ckind[best];
+    s->unroll32 = cu[best];
     return PHG_GPU_OK;
 }
 
@@ -457,7 +494,8 @@ int phgGpuDestroy(phgGpuSystem *s) {
     if (s->graph != nullptr) cudaGraphExecDestroy(s->graph);
     if (s->graph_mixed != nullptr) cudaGraphExecDestroy(s->graph_mixed);
     if (s->h_mst) cudaFreeHost(s->h_mst);
-    DevBuf<float> *fbufs[] = {&s->r32, &s->p32, &s->Ap32, &s->y32, &s->D32, &s->sell_vals32};
+    DevBuf<float> *fbufs[] = {&s->r32, &s->p32, &s->Ap32, &s->y32, &s->D32, &s->sell_vals32, &s->sell2_vals};
+    s->sell2_ssz.release(); s->sell2_sptr.release(); s->sell2_cols.release();
     for (auto *b : fbufs) b->release();
     s->sell_perm.release(); s->sell_ssz.release(); s->sell_sptr.release(); s->sell_cols.release();
     s->sell_len.release(); s->sell_vals.release(); s->mst.release();
@@ -618,6 +656,7 @@ int phgGpuBuildLinearSystem(phgGpuSystem *s, const double *kappa, const double *
     s->assembled = true;
     s->have_bdry_cols = true;
     s->sell_valid = false;
+    s->sell2_valid = false;
     s->lpr = spmv_lanes_for((double)s->nnz / (double)ndof);
     return PHG_GPU_OK;
 }
@@ -654,6 +693,7 @@ int phgGpuSetMatrix(phgGpuSystem *s, int64_t n, const int64_t *ptr, const int32_
     s->assembled = true;
     s->have_bdry_cols = false;
     s->sell_valid = false;
+    s->sell2_valid = false;
     s->lpr = spmv_lanes_for((double)nnz / (double)n);
     return PHG_GPU_OK;
 }
@@ -811,12 +851,14 @@ int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol,
 
         phgGpuSystem_::GraphKey key{};
         key.x = s->x.p; key.r = s->r32.p; key.p = s->p32.p; key.Ap = s->Ap32.p; key.D = s->D32.p;
-        key.va = s->sell_vals32.p; key.hist = s->sell_cols.p; key.n = n; key.lpr = unroll; key.s = s->stream;
+        key.va = s->sell2_vals.p; key.hist = s->sell_cols.p; key.n = n; key.lpr = unroll + 100 * s->kind32;
+        key.s = s->stream;
         if (s->graph_mixed == nullptr || !(s->gkey_mixed == key)) {
             if (s->graph_mixed != nullptr) { cudaGraphExecDestroy(s->graph_mixed); s->graph_mixed = nullptr; }
             cudaGraph_t gr;
             CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-            for (int i = 0; i < kGraphChunk; i++) launch_mixed_iteration(B, P.sell, unroll, s->stream);
+            for (int i = 0; i < kGraphChunk; i++)
+                launch_mixed_iteration2(B, sell_view(s), sell2_view(s), s->kind32, unroll, s->stream);
             CK(cudaStreamEndCapture(s->stream, &gr));
             cudaError_t e = cudaGraphInstantiate(&s->graph_mixed, gr, 0);
             cudaGraphDestroy(gr);
@@ -863,19 +905,15 @@ int phgGpuTimeSpMV(phgGpuSystem *s, int fp32, int reps, double *ms_per_launch) {
     CHECK_RC(tune_spmv(s));
     SpmvPlan P = make_plan(s, s->plan.kind, s->plan.kind == SPMV_CSR ? s->plan.lpr : s->plan.unroll);
     if (fp32) {
-        CHECK_RC(ensure_sell(s));
-        CHECK_RC(s->r32.ensure((size_t)s->n));
-        CHECK_RC(s->Ap32.ensure((size_t)s->n));
-        CK(cudaMemsetAsync(s->r32.p, 0, sizeof(float) * s->n, s->stream));
         CHECK_RC(tune_spmv32(s));
-        P = make_plan(s, SPMV_SELL, s->unroll32);
+        CK(cudaMemsetAsync(s->r32.p, 0, sizeof(float) * s->n, s->stream));
     }
     cudaEvent_t a, b;
     CK(cudaEventCreate(&a));
     CK(cudaEventCreate(&b));
     for (int i = 0; i < reps + 3; i++) {
         if (i == 3) CK(cudaEventRecord(a, s->stream));
-        if (fp32) CK(launch_spmv32(P.sell, P.unroll, s->r32.p, s->Ap32.p, s->stream));
+        if (fp32) CK(launch_spmv32k(sell_view(s), sell2_view(s), s->kind32, s->unroll32, s->r32.p, s->Ap32.p, s->stream));
         else CK(launch_spmv_plan(P, s->rhs.p, s->Ap.p, s->stream));
     }
     CK(cudaEventRecord(b, s->stream));
@@ -911,8 +949,9 @@ int phgGpuGetSpMVPlan(phgGpuSystem *s, int *kind, int *param, double *times_ms) 
     if (param) *param = s->plan.kind == SPMV_CSR ? s->plan.lpr : s->plan.unroll;
     if (times_ms) {
         for (int c = 0; c < kTuneCandidates; c++) times_ms[c] = s->tune_ms[c];
-        for (int c = 0; c < 3; c++) times_ms[kTuneCandidates + c] = s->tune32_ms[c];
-        times_ms[kTuneCandidates + 3] = s->unroll32;
+        for (int c = 0; c < 6; c++) times_ms[kTuneCandidates + c] = s->tune32_ms[c];
+        times_ms[kTuneCandidates + 6] = s->unroll32;
+        times_ms[kTuneCandidates + 7] = s->kind32;
     }
     return kTuneCandidates;
 }

@@ -19,47 +19,84 @@ namespace phgb {
 
 constexpr int kVecThreads = 256;
 
-// Block-wide sum of two values; thread 0 gets the result.  Fixed tree order.
-__device__ __forceinline__ void block_sum2(double &a, double &b) {
-    __shared__ double sa[32], sb[32];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    a = warp_sum(a);
-    b = warp_sum(b);
-    if (lane == 0) { sa[w] = a; sb[w] = b; }
-    __syncthreads();
-    if (w == 0) {
-        a = lane < nw ? sa[lane] : 0.0;
-        b = lane < nw ? sb[lane] : 0.0;
-        a = warp_sum(a);
-        b = warp_sum(b);
-    }
+// Grid-wide sum of two values without block barriers: each warp reduces its
+// values (fixed butterfly), the last warp of a block to arrive adds the
+// block's warp sums in warp order and publishes them, and the last block to
+// arrive adds the block sums in block order.  Nobody waits: a warp that is
+// not last simply leaves.  Returns true in exactly one thread (lane 0 of the
+// final warp), which then holds the totals.  Kernels call grid_sum_init()
+// once, before any early exit that is not uniform across the block.
+struct RedShared {
+    double a[32], b[32];
+    unsigned cnt;
+};
+
+__device__ __forceinline__ RedShared &red_smem() {
+    __shared__ RedShared r;
+    return r;
+}
+
+__device__ __forceinline__ void grid_sum_init() {
+    if (threadIdx.x == 0) red_smem().cnt = 0u;
     __syncthreads();
 }
 
-// Publishes this block's partial sums; returns true in the last block to
-// arrive, which then holds the grid totals in (a, b) on thread 0.
 __device__ __forceinline__ bool grid_sum2(double &a, double &b, double *partials, unsigned *ticket) {
-    __shared__ bool last;
-    block_sum2(a, b);
-    if (threadIdx.x == 0) {
-        partials[2 * blockIdx.x] = a;
-        partials[2 * blockIdx.x + 1] = b;
+    RedShared &R = red_smem();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    unsigned arrived = 0;
+    if (lane == 0) {
+        R.a[w] = a;
+        R.b[w] = b;
+        __threadfence_block();
+        arrived = atomicAdd(&R.cnt, 1u);
+    }
+    arrived = __shfl_sync(0xffffffffu, arrived, 0);
+    if (arrived != (unsigned)nw - 1) return false;
+    __threadfence_block();
+    double ta = lane < nw ? ((volatile double *)R.a)[lane] : 0.0;
+    double tb = lane < nw ? ((volatile double *)R.b)[lane] : 0.0;
+    ta = warp_sum(ta);
+    tb = warp_sum(tb);
+    if (lane == 0) {
+        partials[2 * blockIdx.x] = ta;
+        partials[2 * blockIdx.x + 1] = tb;
         __threadfence();
-        const unsigned t = atomicAdd(ticket, 1u);
-        last = (t == gridDim.x - 1);
+        arrived = atomicAdd(ticket, 1u);
     }
-    __syncthreads();
-    if (!last) return false;
+    arrived = __shfl_sync(0xffffffffu, arrived, 0);
+    if (arrived != gridDim.x - 1) return false;
     __threadfence();
-    double ta = 0.0, tb = 0.0;
-    for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
-        ta += __ldcg(&partials[2 * i]);
-        tb += __ldcg(&partials[2 * i + 1]);
+    // four independent accumulators per lane keep several loads in flight;
+    // they are combined in a fixed order
+    double sa[4] = {0.0, 0.0, 0.0, 0.0}, sb[4] = {0.0, 0.0, 0.0, 0.0};
+    for (unsigned i0 = 0; i0 < gridDim.x; i0 += 128) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const unsigned i = i0 + q * 32 + lane;
+            if (i < gridDim.x) {
+                sa[q] += __ldcg(&partials[2 * i]);
+                sb[q] += __ldcg(&partials[2 * i + 1]);
+            }
+        }
     }
-    block_sum2(ta, tb);
-    if (threadIdx.x == 0) { a = ta; b = tb; *ticket = 0u; }
-    return true;
+    double ta2 = warp_sum((sa[0] + sa[1]) + (sa[2] + sa[3]));
+    double tb2 = warp_sum((sb[0] + sb[1]) + (sb[2] + sb[3]));
+    if (lane == 0) {
+        a = ta2;
+        b = tb2;
+        *ticket = 0u;
+    }
+    return lane == 0;
 }
+
+// Loads/stores of V consecutive elements (16 bytes) at an index that is a
+// multiple of V.
+template <typename T> struct Vec16;
+template <> struct Vec16<double> { using type = double2; static constexpr int V = 2; };
+template <> struct Vec16<float> { using type = float4; static constexpr int V = 4; };
 
 // ---------------------------------------------------------------------------
 // SpMV: LPR lanes per row (CSR vector form).  With DOT, also p.y -> state.
@@ -69,6 +106,7 @@ spmv_kernel(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict
             const VT *__restrict__ va, const VT *__restrict__ x, VT *__restrict__ y,
             double *partials, PcgState *st) {
     if (DOT && st->done) return;
+    if (DOT) grid_sum_init();
     const int lane = threadIdx.x % LPR;
     constexpr int RPW = 32 / LPR;   // rows per warp per step
     const int64_t warp = ((int64_t)blockIdx.x * kVecThreads + threadIdx.x) >> 5;
@@ -92,7 +130,7 @@ spmv_kernel(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict
         }
     }
     if (!DOT) return;
-    if (grid_sum2(dot, dummy, partials, &st->ticket) && threadIdx.x == 0) {
+    if (grid_sum2(dot, dummy, partials, &st->ticket)) {
         const int k = st->nits + 1;
         st->pAp = dot;
         if (dot == 0.0) {
@@ -132,24 +170,34 @@ pcg_dir_kernel(int64_t n, const VT *__restrict__ r, const VT *__restrict__ dinv_
 }
 
 // x += alpha p, r -= alpha Ap; sums ||r||^2 and r.(r/D); closes the iteration.
+// Each thread handles 16-byte vectors of consecutive rows.
 template <typename VT, typename XT>
 __global__ void __launch_bounds__(kVecThreads)
 pcg_update_kernel(int64_t n, XT *__restrict__ x, VT *__restrict__ r, const VT *__restrict__ p,
                   const VT *__restrict__ Ap, const VT *__restrict__ D, double *partials, PcgState *st,
                   double *hist) {
     if (st->done) return;
+    grid_sum_init();
     const double alpha = st->alpha;
     const VT va = (VT)alpha;
     double rr = 0.0, rz = 0.0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        x[i] += (XT)(alpha * (double)p[i]);
-        const VT ri = r[i] - va * Ap[i];
-        r[i] = ri;
-        const double rd = (double)ri;
-        rr += rd * rd;
-        rz += rd * (double)(ri / D[i]);
+    constexpr int V = Vec16<VT>::V;
+    const int64_t nv = (n + V - 1) / V;
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nv; c += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i0 = c * V;
+#pragma unroll
+        for (int q = 0; q < V; q++) {
+            const int64_t i = i0 + q;
+            if (i >= n) break;
+            x[i] += (XT)(alpha * (double)p[i]);
+            const VT ri = r[i] - va * Ap[i];
+            r[i] = ri;
+            const double rd = (double)ri;
+            rr += rd * rd;
+            rz += rd * (double)(ri / D[i]);
+        }
     }
-    if (grid_sum2(rr, rz, partials, &st->ticket) && threadIdx.x == 0) {
+    if (grid_sum2(rr, rz, partials, &st->ticket)) {
         const int k = st->nits + 1;
         const double res = sqrt(rr);
         st->nits = k;
@@ -171,6 +219,7 @@ template <typename VT, typename XT>
 __global__ void __launch_bounds__(kVecThreads)
 init_sums_kernel(int64_t n, int mode, const XT *__restrict__ x, const VT *__restrict__ b,
                  const VT *__restrict__ D, double *partials, unsigned *ticket, double *out) {
+    grid_sum_init();
     double s0 = 0.0, s1 = 0.0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const double bi = (double)b[i];
@@ -182,7 +231,7 @@ init_sums_kernel(int64_t n, int mode, const XT *__restrict__ x, const VT *__rest
             s1 += bi * (double)(b[i] / D[i]);
         }
     }
-    if (grid_sum2(s0, s1, partials, ticket) && threadIdx.x == 0) { out[0] = s0; out[1] = s1; }
+    if (grid_sum2(s0, s1, partials, ticket)) { out[0] = s0; out[1] = s1; }
 }
 
 // r = b - y  (y = A x)
@@ -308,6 +357,7 @@ sell_spmv_kernel(int64_t nslices, const int32_t *__restrict__ perm, const uint16
                  const int32_t *__restrict__ sptr, const int32_t *__restrict__ cols, const VT *__restrict__ vals,
                  const VT *__restrict__ x, VT *__restrict__ y, double *partials, PcgState *st) {
     if (DOT && st->done) return;
+    if (DOT) grid_sum_init();
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * kVecThreads + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * kVecThreads) >> 5;
@@ -338,7 +388,7 @@ sell_spmv_kernel(int64_t nslices, const int32_t *__restrict__ perm, const uint16
         }
     }
     if (!DOT) return;
-    if (grid_sum2(dot, dummy, partials, &st->ticket) && threadIdx.x == 0) {
+    if (grid_sum2(dot, dummy, partials, &st->ticket)) {
         const int k = st->nits + 1;
         st->pAp = dot;
         if (dot == 0.0) {
@@ -417,6 +467,7 @@ mixed_update_kernel(int64_t n, float *__restrict__ y, float *__restrict__ r, con
                     const float *__restrict__ Ap, const float *__restrict__ D, double *partials, MixedState *ms) {
     PcgState *st = &ms->pcg;
     if (st->done) return;
+    grid_sum_init();
     const float a = (float)st->alpha;
     const bool reset = ms->y_reset != 0;
     double rr = 0.0, rz = 0.0;
@@ -427,7 +478,7 @@ mixed_update_kernel(int64_t n, float *__restrict__ y, float *__restrict__ r, con
         rr += (double)ri * (double)ri;
         rz += (double)ri * (double)(ri / D[i]);
     }
-    if (grid_sum2(rr, rz, partials, &st->ticket) && threadIdx.x == 0) {
+    if (grid_sum2(rr, rz, partials, &st->ticket)) {
         const int k = st->nits + 1;
         const double res = sqrt(rr);
         st->nits = k;
@@ -458,6 +509,7 @@ mixed_reliable_kernel(int64_t nslices, const int32_t *__restrict__ perm, const u
                       double *partials, MixedState *ms, double *hist) {
     PcgState *st = &ms->pcg;
     if (st->done || !ms->ru_flag) return;
+    grid_sum_init();
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * kVecThreads + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * kVecThreads) >> 5;
@@ -492,7 +544,7 @@ mixed_reliable_kernel(int64_t nslices, const int32_t *__restrict__ perm, const u
             rz += (double)rf * (double)(rf / D[row]);
         }
     }
-    if (grid_sum2(rr, rz, partials, &st->ticket) && threadIdx.x == 0) {
+    if (grid_sum2(rr, rz, partials, &st->ticket)) {
         const double res = sqrt(rr);
         st->residual = res;
         st->rz_cur = rz;
@@ -513,6 +565,7 @@ __global__ void __launch_bounds__(kVecThreads)
 mixed_init_kernel(int64_t n, const double *__restrict__ rtrue, float *__restrict__ r32, float *__restrict__ y,
                   const double *__restrict__ D64, float *__restrict__ D32, double *partials, unsigned *ticket,
                   double *out) {
+    grid_sum_init();
     double rr = 0.0, rz = 0.0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const double rt = rtrue[i];
@@ -523,7 +576,7 @@ mixed_init_kernel(int64_t n, const double *__restrict__ rtrue, float *__restrict
         rr += rt * rt;
         rz += (double)rf * (double)(rf / df);
     }
-    if (grid_sum2(rr, rz, partials, ticket) && threadIdx.x == 0) { out[0] = rr; out[1] = rz; }
+    if (grid_sum2(rr, rz, partials, ticket)) { out[0] = rr; out[1] = rz; }
 }
 
 cudaError_t launch_mixed_init(int64_t n, const double *rtrue, float *r32, float *y, const double *D64, float *D32,
@@ -555,6 +608,147 @@ cudaError_t launch_mixed_iteration(const MixedBuffers &B, const SellView &S, int
     default: sell_spmv_kernel<float, true, 4><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals32, B.p32, B.Ap32, B.partials, st); break;
     }
     mixed_update_kernel<<<vb, kVecThreads, 0, s>>>(B.n, B.y32, B.r32, B.p32, B.Ap32, B.D32, B.partials, B.ms);
+    mixed_reliable_kernel<4><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals, B.x, B.y32,
+                                                         B.rtrue, B.r32, B.D32, B.partials, B.ms, B.hist);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// FP32 values in "pair" SELL: the same slices as SELL-C-sigma, but each lane
+// keeps two consecutive entries of its row side by side, so a warp moves
+// 256 bytes of values and 256 bytes of column indices per load instruction
+// (float2 / int2).  Slice s holds ceil(w_s / 2) pairs of 64 entries.
+__global__ void sell2_sizes_kernel(int64_t nslices, const uint16_t *__restrict__ len, int32_t *__restrict__ size) {
+    for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nslices; s += (int64_t)gridDim.x * blockDim.x)
+        size[s] = 64 * ((len[s * 32] + 1) / 2);
+}
+
+__global__ void sell2_fill_kernel(int64_t npos, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
+                                  const double *__restrict__ va, const int32_t *__restrict__ perm,
+                                  const uint16_t *__restrict__ len, const int32_t *__restrict__ sptr2,
+                                  int32_t *__restrict__ cols2, float *__restrict__ vals2) {
+    for (int64_t pos = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pos < npos;
+         pos += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t row = perm[pos];
+        const int l = len[pos];
+        const int64_t b = (int64_t)sptr2[pos >> 5] + 2 * (pos & 31);
+        const int32_t r0 = row >= 0 ? rp[row] : 0;
+        const int lp = (l + 1) & ~1;
+        for (int j = 0; j < lp; j++) {
+            const int64_t idx = b + (int64_t)(j >> 1) * 64 + (j & 1);
+            if (j < l) {
+                cols2[idx] = ci[r0 + j];
+                vals2[idx] = (float)va[r0 + j];
+            } else {   // odd-length row: a harmless pad (never added)
+                cols2[idx] = 0;
+                vals2[idx] = 0.0f;
+            }
+        }
+    }
+}
+
+template <bool DOT, int U>
+__global__ void __launch_bounds__(kVecThreads)
+sell2_spmv_kernel(int64_t nslices, const int32_t *__restrict__ perm, const uint16_t *__restrict__ len,
+                  const int32_t *__restrict__ sptr2, const int32_t *__restrict__ cols2,
+                  const float *__restrict__ vals2, const float *__restrict__ x, float *__restrict__ y,
+                  double *partials, PcgState *st) {
+    if (DOT && st->done) return;
+    if (DOT) grid_sum_init();
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * kVecThreads + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * kVecThreads) >> 5;
+    double dot = 0.0, dummy = 0.0;
+    for (int64_t s = warp; s < nslices; s += nwarps) {
+        const int64_t pos = s * 32 + lane;
+        const int32_t row = perm[pos];
+        const int l = len[pos];
+        const int wp = (__shfl_sync(0xffffffffu, l, 0) + 1) >> 1;
+        const int2 *cp = reinterpret_cast<const int2 *>(cols2 + sptr2[s]) + lane;
+        const float2 *vp = reinterpret_cast<const float2 *>(vals2 + sptr2[s]) + lane;
+        float acc = 0.0f;
+        for (int jp = 0; jp < wp; jp += U) {
+            int2 c[U];
+            float2 v[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const bool ok = 2 * (jp + u) < l;
+                c[u] = ok ? __ldcs(cp + 32 * (jp + u)) : make_int2(0, 0);
+                v[u] = ok ? __ldcs(vp + 32 * (jp + u)) : make_float2(0.0f, 0.0f);
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int j = 2 * (jp + u);
+                if (j < l) acc += v[u].x * __ldg(&x[c[u].x]);
+                if (j + 1 < l) acc += v[u].y * __ldg(&x[c[u].y]);
+            }
+        }
+        if (row >= 0) {
+            y[row] = acc;
+            if (DOT) dot += (double)x[row] * (double)acc;
+        }
+    }
+    if (!DOT) return;
+    if (grid_sum2(dot, dummy, partials, &st->ticket)) {
+        const int k = st->nits + 1;
+        st->pAp = dot;
+        if (dot == 0.0) {
+            st->done = 1;
+            st->status = PCG_BREAKDOWN;
+            st->nits = k;
+        } else {
+            st->alpha = st->rz_cur / dot;
+        }
+    }
+}
+
+cudaError_t launch_sell2_sizes(const SellView &S, int32_t *sizes, cudaStream_t s) {
+    sell2_sizes_kernel<<<vec_blocks(S.nslices), kVecThreads, 0, s>>>(S.nslices, S.len, sizes);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sell2_fill(const SellView &S, const int32_t *rp, const int32_t *ci, const double *va,
+                              const int32_t *sptr2, int32_t *cols2, float *vals2, cudaStream_t s) {
+    const int64_t npos = S.nslices * 32;
+    sell2_fill_kernel<<<vec_blocks(npos), kVecThreads, 0, s>>>(npos, rp, ci, va, S.perm, S.len, sptr2, cols2, vals2);
+    return cudaGetLastError();
+}
+
+// FP32 product for the mixed solver: kind 0 = SELL (unroll u), 1 = pair SELL (unroll u pairs)
+template <bool DOT>
+static void spmv32_dispatch(const SellView &S, const Sell2View &S2, int kind, int u, const float *x, float *y,
+                            double *partials, PcgState *st, cudaStream_t s) {
+    const int sb = vec_blocks(S.nslices * 32);
+    if (kind == 0) {
+        switch (u) {
+        case 2: sell_spmv_kernel<float, DOT, 2><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals32, x, y, partials, st); break;
+        case 8: sell_spmv_kernel<float, DOT, 8><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals32, x, y, partials, st); break;
+        case 16: sell_spmv_kernel<float, DOT, 16><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals32, x, y, partials, st); break;
+        default: sell_spmv_kernel<float, DOT, 4><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals32, x, y, partials, st); break;
+        }
+    } else {
+        switch (u) {
+        case 2: sell2_spmv_kernel<DOT, 2><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S2.sptr2, S2.cols2, S2.vals2, x, y, partials, st); break;
+        case 8: sell2_spmv_kernel<DOT, 8><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S2.sptr2, S2.cols2, S2.vals2, x, y, partials, st); break;
+        default: sell2_spmv_kernel<DOT, 4><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S2.sptr2, S2.cols2, S2.vals2, x, y, partials, st); break;
+        }
+    }
+}
+
+cudaError_t launch_spmv32k(const SellView &S, const Sell2View &S2, int kind, int u, const float *x, float *y,
+                           cudaStream_t s) {
+    spmv32_dispatch<false>(S, S2, kind, u, x, y, nullptr, nullptr, s);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mixed_iteration2(const MixedBuffers &B, const SellView &S, const Sell2View &S2, int kind, int u,
+                                    cudaStream_t s) {
+    const int vb = vec_blocks(B.n);
+    PcgState *st = &B.ms->pcg;
+    pcg_dir_kernel<float><<<vb, kVecThreads, 0, s>>>(B.n, B.r32, B.D32, B.p32, st);
+    spmv32_dispatch<true>(S, S2, kind, u, B.p32, B.Ap32, B.partials, st, s);
+    mixed_update_kernel<<<vb, kVecThreads, 0, s>>>(B.n, B.y32, B.r32, B.p32, B.Ap32, B.D32, B.partials, B.ms);
+    const int sb = vec_blocks(S.nslices * 32);
     mixed_reliable_kernel<4><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals, B.x, B.y32,
                                                          B.rtrue, B.r32, B.D32, B.partials, B.ms, B.hist);
     return cudaGetLastError();

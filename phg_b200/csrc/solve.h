@@ -44,6 +44,13 @@ struct SellView {
     const float *vals32;      // FP32 copy of the values (mixed precision), may be null
 };
 
+// FP32 pair layout of the same slices (see solve.cu).
+struct Sell2View {
+    const int32_t *sptr2;     // slice offsets in entries (nslices + 1)
+    const int32_t *cols2;
+    const float *vals2;
+};
+
 struct SpmvPlan {
     int kind = SPMV_CSR, lpr = 8, unroll = 4;
     CsrView csr{};
@@ -70,6 +77,13 @@ struct MixedBuffers {
 int vec_blocks(int64_t n);
 cudaError_t launch_mixed_init(int64_t n, const double *rtrue, float *r32, float *y, const double *D64, float *D32,
                               double *partials, unsigned *ticket, double *out, cudaStream_t s);
+cudaError_t launch_sell2_sizes(const SellView &S, int32_t *sizes, cudaStream_t s);
+cudaError_t launch_sell2_fill(const SellView &S, const int32_t *rp, const int32_t *ci, const double *va,
+                              const int32_t *sptr2, int32_t *cols2, float *vals2, cudaStream_t s);
+cudaError_t launch_spmv32k(const SellView &S, const Sell2View &S2, int kind, int u, const float *x, float *y,
+                           cudaStream_t s);
+cudaError_t launch_mixed_iteration2(const MixedBuffers &B, const SellView &S, const Sell2View &S2, int kind, int u,
+                                    cudaStream_t s);
 cudaError_t launch_spmv32(const SellView &S, int unroll, const float *x, float *y, cudaStream_t s);
 cudaError_t launch_mixed_iteration(const MixedBuffers &B, const SellView &S, int unroll, cudaStream_t s);
 int64_t sell_positions(int64_t n);   // perm/len entries = slices * 32

