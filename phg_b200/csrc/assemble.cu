@@ -390,7 +390,6 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
     __shared__ int16_t s_pos[W][R][HS];
     __shared__ int32_t s_col[W][R][PASS2 ? MAXROW : 1];
     __shared__ double s_val[W][R][PASS2 ? MAXROW : 1];
-    __shared__ double s_lift[W][R][PASS2 ? MAXROW : 1];
 
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int grp = lane / G, gl = lane % G;
@@ -400,7 +399,6 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
     int16_t *hpos = s_pos[w][grp];
     int32_t *scol = s_col[w][grp];
     double *sval = s_val[w][grp];
-    double *slift = s_lift[w][grp];
 
     const int64_t nwarps = (int64_t)gridDim.x * W;
     for (int64_t wb = ((int64_t)blockIdx.x * W + w) * R; wb < ndof; wb += nwarps * R) {
@@ -522,7 +520,8 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
 
         // pass 2: emit kept columns and saved boundary columns, in order.
         // Lanes also evaluate, in parallel, the lift term of each boundary
-        // column (rhs_k * a_dk / D_kk, solver.c:716-724) into s_lift.
+        // column (rhs_k * a_dk / D_kk, solver.c:716-724); it replaces the
+        // column's value in s_val once the value has been emitted.
         const bool emit = walk && badm == 0;
         int32_t p0 = 0, b0 = 0;
         if (emit) { p0 = ptr[d]; b0 = bptr[d]; }
@@ -550,7 +549,7 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
                     const double rk = bdry_rhs(g, c, mult);
                     term = __ddiv_rn(rn_mul(rn_mul(1.0, rk), val), Dk);
                 }
-                slift[t] = term;
+                sval[t] = term;
                 if (!isbc) scol[t] = -1;   // only boundary columns remain for the lift below
             }
             const unsigned km = __ballot_sync(0xffffffffu, valid && !isbc) & gmask;
@@ -588,7 +587,7 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
             diag[d] = dg;
             // lift the boundary columns in first-touch order: r -= term
             for (int t = 0; t < L; t++)
-                if (scol[t] >= 0) r = rn_sub(r, slift[t]);
+                if (scol[t] >= 0) r = rn_sub(r, sval[t]);
             rhs[d] = r;
         }
         __syncwarp();

@@ -98,6 +98,22 @@ template <typename T> struct Vec16;
 template <> struct Vec16<double> { using type = double2; static constexpr int V = 2; };
 template <> struct Vec16<float> { using type = float4; static constexpr int V = 4; };
 
+template <typename T> struct VArr { T v[Vec16<T>::V]; };
+
+template <typename T> __device__ __forceinline__ VArr<T> vload(const T *p) {
+    VArr<T> a;
+    *reinterpret_cast<typename Vec16<T>::type *>(a.v) = *reinterpret_cast<const typename Vec16<T>::type *>(p);
+    return a;
+}
+template <typename T> __device__ __forceinline__ VArr<T> vload_ro(const T *p) {
+    VArr<T> a;
+    *reinterpret_cast<typename Vec16<T>::type *>(a.v) = __ldg(reinterpret_cast<const typename Vec16<T>::type *>(p));
+    return a;
+}
+template <typename T> __device__ __forceinline__ void vstore(T *p, const VArr<T> &a) {
+    *reinterpret_cast<typename Vec16<T>::type *>(p) = *reinterpret_cast<const typename Vec16<T>::type *>(a.v);
+}
+
 // ---------------------------------------------------------------------------
 // SpMV: LPR lanes per row (CSR vector form).  With DOT, also p.y -> state.
 template <int LPR, bool DOT, typename VT>
@@ -143,7 +159,7 @@ spmv_kernel(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict
     }
 }
 
-// p = r / D (first iteration) or p = z + beta p.
+// p = r / D (first iteration) or p = z + beta p; 16-byte vectors of rows.
 template <typename VT>
 __global__ void __launch_bounds__(kVecThreads)
 pcg_dir_kernel(int64_t n, const VT *__restrict__ r, const VT *__restrict__ dinv_or_d, VT *__restrict__ p,
@@ -163,7 +179,24 @@ pcg_dir_kernel(int64_t n, const VT *__restrict__ r, const VT *__restrict__ dinv_
         beta = st->rz_cur / st->rz_prev;
     }
     const VT vb = (VT)beta;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    constexpr int V = Vec16<VT>::V;
+    const int64_t nfull = n / V;
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nfull; c += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = c * V;
+        const VArr<VT> rr = vload_ro(r + i), dd = vload_ro(dinv_or_d + i);
+        VArr<VT> pp;
+        if (k == 1) {
+#pragma unroll
+            for (int q = 0; q < V; q++) pp.v[q] = rr.v[q] / dd.v[q];
+        } else {
+            pp = vload(p + i);
+#pragma unroll
+            for (int q = 0; q < V; q++) pp.v[q] = vb * pp.v[q] + rr.v[q] / dd.v[q];
+        }
+        vstore(p + i, pp);
+    }
+    for (int64_t i = nfull * V + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
         const VT z = r[i] / dinv_or_d[i];
         p[i] = k == 1 ? z : vb * p[i] + z;
     }
@@ -182,20 +215,32 @@ pcg_update_kernel(int64_t n, XT *__restrict__ x, VT *__restrict__ r, const VT *_
     const VT va = (VT)alpha;
     double rr = 0.0, rz = 0.0;
     constexpr int V = Vec16<VT>::V;
-    const int64_t nv = (n + V - 1) / V;
-    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nv; c += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i0 = c * V;
+    const int64_t nfull = n / V;
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nfull; c += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = c * V;
+        const VArr<VT> pp = vload_ro(p + i), aa = vload_ro(Ap + i), dd = vload_ro(D + i);
+        VArr<VT> rv = vload(r + i);
+        VArr<XT> xv = vload(x + i);
 #pragma unroll
         for (int q = 0; q < V; q++) {
-            const int64_t i = i0 + q;
-            if (i >= n) break;
-            x[i] += (XT)(alpha * (double)p[i]);
-            const VT ri = r[i] - va * Ap[i];
-            r[i] = ri;
+            xv.v[q] += (XT)(alpha * (double)pp.v[q]);
+            const VT ri = rv.v[q] - va * aa.v[q];
+            rv.v[q] = ri;
             const double rd = (double)ri;
             rr += rd * rd;
-            rz += rd * (double)(ri / D[i]);
+            rz += rd * (double)(ri / dd.v[q]);
         }
+        vstore(r + i, rv);
+        vstore(x + i, xv);
+    }
+    for (int64_t i = nfull * V + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] += (XT)(alpha * (double)p[i]);
+        const VT ri = r[i] - va * Ap[i];
+        r[i] = ri;
+        const double rd = (double)ri;
+        rr += rd * rd;
+        rz += rd * (double)(ri / D[i]);
     }
     if (grid_sum2(rr, rz, partials, &st->ticket)) {
         const int k = st->nits + 1;
@@ -249,6 +294,15 @@ int vec_blocks(int64_t n) {
     return (int)b;
 }
 
+// Grid of the vectorised element-wise kernels: one 16-byte vector per thread
+// and step, at most 4 blocks per SM (fewer partial sums to combine).
+static int vvec_blocks(int64_t n, int V) {
+    int64_t b = ceil_div(ceil_div(n, V), kVecThreads);
+    if (b > 148 * 4) b = 148 * 4;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
 int spmv_lanes_for(double avg_nnz_per_row) {
     if (avg_nnz_per_row <= 6) return 4;
     if (avg_nnz_per_row <= 16) return 8;
@@ -274,7 +328,7 @@ cudaError_t launch_spmv(const CsrView &A, int lpr, const double *x, double *y, c
 }
 
 cudaError_t launch_pcg_iteration(const PcgBuffers &B, int lpr, cudaStream_t s) {
-    const int vb = vec_blocks(B.A.n);
+    const int vb = vvec_blocks(B.A.n, 2);
     pcg_dir_kernel<double><<<vb, kVecThreads, 0, s>>>(B.A.n, B.r, B.D, B.p, B.st);
     spmv_dispatch<true, double>(lpr, B.A.n, B.A.rp, B.A.ci, B.A.va, B.p, B.Ap, B.partials, B.st, s);
     pcg_update_kernel<double, double><<<vb, kVecThreads, 0, s>>>(B.A.n, B.x, B.r, B.p, B.Ap, B.D, B.partials,
@@ -440,7 +494,7 @@ cudaError_t launch_spmv_plan(const SpmvPlan &P, const double *x, double *y, cuda
 }
 
 cudaError_t launch_pcg_iteration_plan(const PcgBuffers &B, const SpmvPlan &P, cudaStream_t s) {
-    const int vb = vec_blocks(B.A.n);
+    const int vb = vvec_blocks(B.A.n, 2);
     pcg_dir_kernel<double><<<vb, kVecThreads, 0, s>>>(B.A.n, B.r, B.D, B.p, B.st);
     plan_spmv<true, double>(P, P.kind == SPMV_CSR ? P.csr.va : P.sell.vals, B.p, B.Ap, B.partials, B.st, s);
     pcg_update_kernel<double, double><<<vb, kVecThreads, 0, s>>>(B.A.n, B.x, B.r, B.p, B.Ap, B.D, B.partials,
@@ -471,7 +525,25 @@ mixed_update_kernel(int64_t n, float *__restrict__ y, float *__restrict__ r, con
     const float a = (float)st->alpha;
     const bool reset = ms->y_reset != 0;
     double rr = 0.0, rz = 0.0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t nfull = n / 4;
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nfull; c += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = c * 4;
+        const VArr<float> pp = vload_ro(p + i), aa = vload_ro(Ap + i), dd = vload_ro(D + i);
+        VArr<float> yv = reset ? VArr<float>{{0.0f, 0.0f, 0.0f, 0.0f}} : vload(y + i);
+        VArr<float> rv = vload(r + i);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            yv.v[q] = yv.v[q] + a * pp.v[q];
+            const float ri = rv.v[q] - a * aa.v[q];
+            rv.v[q] = ri;
+            rr += (double)ri * (double)ri;
+            rz += (double)ri * (double)(ri / dd.v[q]);
+        }
+        vstore(y + i, yv);
+        vstore(r + i, rv);
+    }
+    for (int64_t i = nfull * 4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
         y[i] = (reset ? 0.0f : y[i]) + a * p[i];
         const float ri = r[i] - a * Ap[i];
         r[i] = ri;
@@ -597,7 +669,7 @@ cudaError_t launch_spmv32(const SellView &S, int unroll, const float *x, float *
 }
 
 cudaError_t launch_mixed_iteration(const MixedBuffers &B, const SellView &S, int unroll, cudaStream_t s) {
-    const int vb = vec_blocks(B.n);
+    const int vb = vvec_blocks(B.n, 4);
     PcgState *st = &B.ms->pcg;
     pcg_dir_kernel<float><<<vb, kVecThreads, 0, s>>>(B.n, B.r32, B.D32, B.p32, st);
     const int sb = vec_blocks(S.nslices * 32);
@@ -743,7 +815,7 @@ cudaError_t launch_spmv32k(const SellView &S, const Sell2View &S2, int kind, int
 
 cudaError_t launch_mixed_iteration2(const MixedBuffers &B, const SellView &S, const Sell2View &S2, int kind, int u,
                                     cudaStream_t s) {
-    const int vb = vec_blocks(B.n);
+    const int vb = vvec_blocks(B.n, 4);
     PcgState *st = &B.ms->pcg;
     pcg_dir_kernel<float><<<vb, kVecThreads, 0, s>>>(B.n, B.r32, B.D32, B.p32, st);
     spmv32_dispatch<true>(S, S2, kind, u, B.p32, B.Ap32, B.partials, st, s);

@@ -5,18 +5,21 @@ size-independent properties (each prints a one-line JSON summary).
            1e-10 (relative L2) of the oracle's PCG solution
   P1 96^3  (5,308,416 tets, kappa = exp(N(0,1))): FP64 forward + adjoint PCG
            to 1e-10, dJ/dlog kappa_e for all elements (timed); central
-           differences (h = 1e-6) on 32 seeded elements within 1e-5 relative of
-           the gradient computed from forward and adjoint solves converged to
-           1e-13 (the systems' condition numbers, ~1e7, leave errors of order
-           cond * rtol in a gradient from 1e-10 solves, which is reported)
+           differences on 32 seeded elements, Richardson-extrapolated from
+           h = 1e-3 and 2e-3, within 1e-5 relative of the gradient computed
+           from forward and adjoint solves converged to 1e-13 (the systems'
+           condition numbers, ~1e7, leave errors of order cond * rtol in a
+           gradient from 1e-10 solves, which is reported).  A step of 1e-6 is
+           not usable at this size: one element moves J (~40) by ~1e-12, the
+           size of J's own rounding, which the reported h = 1e-6 error shows
   P2 48^3  (663,552 tets): 64 right-hand sides (N(0,1) per free DOF), FP32
            block PCG with FP64 updates to 1e-8 each vs 64 single-vector FP64
            solves: every residual meets the tolerance, solutions agree, the
            block solve is faster
   P3 64^3  (1,572,864 tets, 7.19M DOFs, kappa = exp(0.5 N(0,1))): mixed PCG to
            1e-8 (FP64 residual recomputed independently), adjoint gradient,
-           central differences on 16 elements within 1e-5 relative (same
-           convention as for P1 96^3)
+           extrapolated central differences on 16 elements within 1e-5
+           relative (same convention as for P1 96^3)
 """
 import json
 import time
@@ -42,24 +45,29 @@ def misfit(u, u_obs):
     return float(0.5 * np.sum(d * d))
 
 
-def fd_check(s, f, logk, u_obs, els, rtol, h=1e-6):
-    """Central differences of J in log kappa_e.  Both solves of a pair stop
-    after the same number of iterations (the count the unperturbed solve
-    needs to reach a tight tolerance), so the iteration error is a smooth
-    function of kappa and cancels in the difference."""
+def fd_check(s, f, logk, u_obs, els, rtol, hs=(1e-3, 2e-3, 1e-6)):
+    """Central differences of J in log kappa_e for each step in hs.  Both
+    solves of a pair stop after the same number of iterations (the count the
+    unperturbed solve needs to reach a tight tolerance), so the iteration
+    error is a smooth function of kappa and cancels in the difference.
+    Returns {h: differences}, the extrapolation (4 D(h) - D(2h)) / 3 of the
+    first two steps (error O(h^4)), and the iteration count."""
     s.build_linear_system(kappa=np.exp(logk), f=f)
     _, nfix, _ = s.solve_pcg(rtol=rtol, btol=0.0, atol=0.0, maxit=1000000)
-    out = []
+    out = {h: [] for h in hs}
     for e in els:
-        vals = []
-        for sgn in (1.0, -1.0):
-            lk = logk.copy()
-            lk[e] += sgn * h
-            s.build_linear_system(kappa=np.exp(lk), f=f)
-            u, _, _ = s.solve_pcg(rtol=0.0, btol=0.0, atol=0.0, maxit=nfix)
-            vals.append(misfit(u, u_obs))
-        out.append((vals[0] - vals[1]) / (2 * h))
-    return np.array(out), nfix
+        for h in hs:
+            vals = []
+            for sgn in (1.0, -1.0):
+                lk = logk.copy()
+                lk[e] += sgn * h
+                s.build_linear_system(kappa=np.exp(lk), f=f)
+                u, _, _ = s.solve_pcg(rtol=0.0, btol=0.0, atol=0.0, maxit=nfix)
+                vals.append(misfit(u, u_obs))
+            out[h].append((vals[0] - vals[1]) / (2 * h))
+    out = {h: np.array(v) for h, v in out.items()}
+    rich = (4.0 * out[hs[0]] - out[hs[1]]) / 3.0
+    return out, rich, nfix
 
 
 def test_config_p1_32(gpu, oracle):
@@ -99,13 +107,14 @@ def test_config_p1_96_adjoint(gpu):
         u, _, _ = s.solve_pcg(rtol=1e-13, btol=0.0, atol=0.0, maxit=1000000)
         g, J, na13 = s.adjoint_gradient(u, u_obs, rtol=1e-13)
         els = np.random.default_rng(32).choice(len(e), 32, replace=False)
-        fd, nfix = fd_check(s, f, logk, u_obs, els, rtol=1e-13)
+        fds, fd, nfix = fd_check(s, f, logk, u_obs, els, rtol=1e-13)
     scale = np.max(np.abs(g[els]))
     err = np.max(np.abs(fd - g[els])) / scale
     err10 = np.max(np.abs(g10[els] - g[els])) / scale
     report("P1 96^3 adjoint", n=len(bdry), elements=len(e), forward_its=nf, adjoint_its=na, J=J,
            forward_adjoint_gradient_s=round(t_grad, 3), fd_iterations=nfix, max_rel_fd_err=err,
-           rtol_1e10_gradient_rel_err=err10)
+           fd_err_by_h={str(h): float(np.max(np.abs(v - g[els])) / scale) for h, v in fds.items()},
+           gradient_scale=float(scale), rtol_1e10_gradient_rel_err=err10)
     assert err <= 1e-5
 
 
@@ -174,7 +183,7 @@ def test_config_p3_64_mixed_adjoint(gpu, oracle):
         s.build_linear_system(kappa=np.exp(logk), f=f)
         u, _, _ = s.solve_pcg(rtol=1e-13, btol=0.0, atol=0.0, maxit=1000000)
         g13, J, na13 = s.adjoint_gradient(u, u_obs, rtol=1e-13)
-        fd, nfix = fd_check(s, f, logk, u_obs, els, rtol=1e-13)
+        fds, fd, nfix = fd_check(s, f, logk, u_obs, els, rtol=1e-13, hs=(1e-3, 2e-3))
         g10 = g
     g = g13
     scale = np.max(np.abs(g[els]))
@@ -182,5 +191,6 @@ def test_config_p3_64_mixed_adjoint(gpu, oracle):
     report("P3 64^3 mixed+adjoint", rtol_1e10_gradient_rel_err=float(np.max(np.abs(g10[els] - g[els])) / scale), n=len(bdry), nnz=int(len(vals)), mixed_its=nm, reliable_updates=nupd,
            fp64_its=n64, mixed_s=round(t_mixed, 4), fp64_s=round(t_fp64, 4),
            rel_l2_mixed_vs_fp64=float(np.linalg.norm(xm - x64) / np.linalg.norm(x64)),
-           adjoint_its=na, max_rel_fd_err=err)
+           adjoint_its=na, max_rel_fd_err=err, gradient_scale=float(scale),
+           fd_err_by_h={str(h): float(np.max(np.abs(v - g[els])) / scale) for h, v in fds.items()})
     assert err <= 1e-5
