@@ -84,6 +84,17 @@ int phgGpuSetDofMap(phgGpuSystem *sys, int order, int64_t ndof,
 int phgGpuBuildLinearSystem(phgGpuSystem *sys, const double *kappa,
 			    const double *f, const double *g);
 
+/* The same with a mass term, for -div(kappa grad u) + c u = f: each element
+ * matrix is phgQuadGradBasAGradBas + mass_coef * phgQuadBasDotBas
+ * (phgQuadBasABas with A = NULL, src/quad.c:5582-5625, order 2p rule), the
+ * element loop of examples/simplest.c:66-73 (reaction-diffusion, also the
+ * implicit time step of examples/heat.c:155-162 with the roles of the two
+ * coefficients exchanged).  mass_coef = 0 is phgGpuBuildLinearSystem.
+ * phgGpuAdjointGradient refuses a system with a mass term. */
+int phgGpuBuildLinearSystemMass(phgGpuSystem *sys, const double *kappa,
+				double mass_coef, const double *f,
+				const double *g);
+
 /* Installs an already-assembled matrix instead (the rows PHG hands an OEM
  * solver, src/solver.c:223-285): CSR with int64 row pointers (PHG's
  * size_t packed_ind), int32 columns, and the right-hand side. */

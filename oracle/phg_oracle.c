@@ -461,12 +461,12 @@ int
 pho_assemble(int p, int64_t nvert, const double *verts, int64_t nelem,
 	     const int32_t *elems, const int32_t *e2l, int64_t ndof,
 	     const uint8_t *bdry, const double *f, const double *g,
-	     const double *kappa, pho_system *S)
+	     const double *kappa, double mass_coef, pho_system *S)
 {
     int N = pho_nbas(p), a, b;
     int64_t e, i, j;
     ROW *rows;
-    double A[400], B[20], R[20], x[12], fl[20];
+    double A[400], M[400], B[20], R[20], x[12], fl[20];
 
     if (N < 0)
 	return -1;
@@ -490,6 +490,12 @@ pho_assemble(int p, int64_t nvert, const double *verts, int64_t nelem,
 	    fl[a] = f != NULL ? f[I[a]] : 0.0;
 	}
 	pho_elem_stiffness(p, x, kappa != NULL ? kappa[e] : -1.0, A);
+	/* stiffness + c * mass (examples/simplest.c:68-72) */
+	if (mass_coef != 0.0) {
+	    pho_elem_mass(p, x, M);
+	    for (a = 0; a < N * N; a++)
+		A[a] = A[a] + mass_coef * M[a];
+	}
 	pho_elem_rhs(p, x, fl, R);
 	for (a = 0; a < N; a++) {
 	    if (bdry[I[a]]) {

@@ -29,7 +29,7 @@ def lib():
         L.pho_elem_mass.argtypes = [C.c_int, P, P]
         L.pho_elem_rhs.argtypes = [C.c_int, P, P, P]
         L.pho_assemble.argtypes = [C.c_int, C.c_int64, P, C.c_int64, P, P,
-                                   C.c_int64, P, P, P, P, P]
+                                   C.c_int64, P, P, P, P, C.c_double, P]
         L.pho_assemble.restype = C.c_int
         L.pho_system_free.argtypes = [P]
         L.pho_spmv.argtypes = [C.c_int64, P, P, P, P, P]
@@ -93,8 +93,9 @@ def elem_mass(p, x):
     return M
 
 
-def assemble(p, verts, elems, e2l, bdry, f, g=None, kappa=None):
-    """Returns a dict of numpy arrays (see pho_system in phg_oracle.h)."""
+def assemble(p, verts, elems, e2l, bdry, f, g=None, kappa=None, mass=0.0):
+    """Returns a dict of numpy arrays (see pho_system in phg_oracle.h).
+    mass != 0 adds mass * (element mass matrix) to each element matrix."""
     verts = np.ascontiguousarray(verts, np.float64)
     elems = np.ascontiguousarray(elems, np.int32)
     e2l = np.ascontiguousarray(e2l, np.int32)
@@ -106,7 +107,7 @@ def assemble(p, verts, elems, e2l, bdry, f, g=None, kappa=None):
     S = _System()
     rc = lib().pho_assemble(p, len(verts), _ptr(verts), len(elems),
                             _ptr(elems), _ptr(e2l), ndof, _ptr(bdry), _ptr(f),
-                            _ptr(g), _ptr(kappa), C.byref(S))
+                            _ptr(g), _ptr(kappa), C.c_double(mass), C.byref(S))
     if rc != 0:
         raise ValueError("pho_assemble failed: %d" % rc)
     n = S.n

@@ -35,6 +35,7 @@ static char *kappa_file = NULL;
 static INT rhs_case = 0;		/* 0: sine (g = 0), 1: linear u=x+y+z */
 static INT repeat = 1;			/* repeat the whole pipeline (timing) */
 static INT sample_maxit = 0;		/* > 0: cap PCG iterations after rep 0 */
+static FLOAT mass_coef = 0.;		/* != 0: add mass_coef * mass matrix */
 static const char *rhs_case_names[] = {"sine", "linear", NULL};
 
 static void
@@ -124,6 +125,9 @@ main(int argc, char *argv[])
     phgOptionsRegisterKeyword("-rhs_case", "Right-hand side / BC case",
 		rhs_case_names, &rhs_case);
     phgOptionsRegisterInt("-repeat", "Repeat the pipeline (timing)", &repeat);
+    phgOptionsRegisterFloat("-mass_coef",
+		"Coefficient c of the mass term (-div kappa grad u + c u = f)",
+		&mass_coef);
     phgOptionsRegisterInt("-sample_maxit",
 		"PCG iteration cap for repetitions after the first (timing samples)",
 		&sample_maxit);
@@ -187,6 +191,10 @@ main(int argc, char *argv[])
 		    else
 			A[a][b] = phgQuadGradBasAGradBas(e, u_h, b, kappa,
 							 u_h, a, QUAD_DEFAULT);
+		    /* stiffness + c * mass, as examples/simplest.c:68-72 */
+		    if (mass_coef != 0.)
+			A[a][b] = A[a][b] + mass_coef *
+			    phgQuadBasDotBas(e, u_h, b, u_h, a, QUAD_DEFAULT);
 		    A[b][a] = A[a][b];
 		}
 	    }
@@ -257,12 +265,12 @@ main(int argc, char *argv[])
 	    fp = fopen(path, "w");
 	    fprintf(fp, "nvert %d\nnelem %d\nndof %d\nnbas %d\norder %d\n"
 			"nits %d\nresidual %.17g\nrtol %.17g\nbtol %.17g\n"
-			"atol %.17g\nnedge %d\nnface %d\n",
+			"atol %.17g\nnedge %d\nnface %d\nmass_coef %.17g\n",
 		    (int)g->nvert, (int)g->nelem, (int)ndof, (int)nbas,
 		    (int)u_h->type->order, solver->nits,
 		    (double)solver->residual, (double)solver->rtol,
 		    (double)solver->btol, (double)solver->atol,
-		    (int)g->nedge, (int)g->nface);
+		    (int)g->nedge, (int)g->nface, (double)mass_coef);
 	    fclose(fp);
 	    phgFree(e2l);
 	    phgFree(elems);

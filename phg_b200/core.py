@@ -29,6 +29,7 @@ SIGNATURES = {
     "phgGpuSetMesh": (C.c_int, [_P, _I64, _P, _I64, _P]),
     "phgGpuSetDofMap": (C.c_int, [_P, C.c_int, _I64, _P, _P]),
     "phgGpuBuildLinearSystem": (C.c_int, [_P, _P, _P, _P]),
+    "phgGpuBuildLinearSystemMass": (C.c_int, [_P, _P, C.c_double, _P, _P]),
     "phgGpuSetMatrix": (C.c_int, [_P, _I64, _P, _P, _P, _P]),
     "phgGpuGetSizes": (C.c_int, [_P, C.POINTER(_I64), C.POINTER(_I64), C.POINTER(_I64)]),
     "phgGpuGetMatrix": (C.c_int, [_P, _P, _P, _P]),
@@ -146,9 +147,14 @@ class Solver:
         e2l, bdry = _np(e2l, np.int32), _np(bdry, np.uint8)
         _check(lib().phgGpuSetDofMap(self._h, int(order), len(bdry), _ptr(e2l), _ptr(bdry)))
 
-    def build_linear_system(self, kappa=None, f=None, g=None):
+    def build_linear_system(self, kappa=None, f=None, g=None, mass=0.0):
+        """Element loop + assembly; mass != 0 adds mass * (element mass
+        matrix) to every element matrix (-div(kappa grad u) + mass u = f)."""
         kappa, f, g = _np(kappa, np.float64), _np(f, np.float64), _np(g, np.float64)
-        _check(lib().phgGpuBuildLinearSystem(self._h, _ptr(kappa), _ptr(f), _ptr(g)))
+        if mass != 0.0:
+            _check(lib().phgGpuBuildLinearSystemMass(self._h, _ptr(kappa), float(mass), _ptr(f), _ptr(g)))
+        else:
+            _check(lib().phgGpuBuildLinearSystem(self._h, _ptr(kappa), _ptr(f), _ptr(g)))
 
     def set_matrix(self, ptr, cols, vals, rhs):
         ptr, cols = _np(ptr, np.int64), _np(cols, np.int32)

@@ -105,6 +105,10 @@ __device__ __forceinline__ void jacobian_vol(const double *x, double *J, double 
 //   Ke[e]   N x N stiffness, integral of grad phi_b . kappa grad phi_a with the
 //           order-2(p-1) rule (phgQuadGradBasAGradBas, quad.c:5260-5344, basis
 //           gradients as phgQuadGetBasisGradient, quad.c:3314-3421)
+//           plus, when c = mass != 0, c times the mass matrix, integral of
+//           phi_b phi_a with the order-2p rule (phgQuadBasABas with A = NULL,
+//           quad.c:5582-5625), added as stiffness + c * mass the way
+//           examples/simplest.c:68-72 writes the element matrix
 //   Re[e]   N right-hand side entries, integral of f_h phi_a with the order-2p
 //           rule (phgQuadDofTimesBas, quad.c:5481-5530; f_h at the points as
 //           phgDofEval_, dof-utils.c:59-300)
@@ -154,7 +158,7 @@ geometry_kernel(int64_t nelem, int64_t nvert, const double *__restrict__ verts, 
 template <int P>
 __global__ void __launch_bounds__(ElemDims<P>::WARPS * 32)
 element_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, const int32_t *__restrict__ e2l,
-               const double *__restrict__ kappa, const double *__restrict__ f,
+               const double *__restrict__ kappa, const double mass, const double *__restrict__ f,
                const double *__restrict__ wk, const double *__restrict__ gk,
                const double *__restrict__ wr, const double *__restrict__ br,
                double *__restrict__ Ke, double *__restrict__ Re, uint32_t *__restrict__ Km, int *status) {
@@ -228,7 +232,15 @@ element_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, cons
                 const double t = rn_mul(d0, wk[q]);
                 d = rn_add(d, kappa != nullptr ? rn_mul(t, kap) : t);
             }
-            const double v = rn_mul(d, vol);
+            double v = rn_mul(d, vol);
+            if (mass != 0.0) {
+                double dm = 0.;
+                for (int q = 0; q < QR; q++) {
+                    const double d0 = rn_add(0., rn_mul(br[q * N + b], br[q * N + a]));
+                    dm = rn_add(dm, rn_mul(d0, wr[q]));
+                }
+                v = rn_add(v, rn_mul(mass, rn_mul(dm, vol)));
+            }
             K[a * N + b] = v;
             K[b * N + a] = v;
         }
@@ -610,7 +622,7 @@ static void elem_launch(const ElemArgs &A, cudaStream_t s) {
     geometry_kernel<<<grid_for(A.nelem, 128, 148 * 64), 128, 0, s>>>(A.nelem, A.nvert, A.verts, A.elems, A.geo,
                                                                     A.status);
     const int blocks = grid_for(A.nelem, W, 148 * 64);
-    element_kernel<P><<<blocks, W * 32, 0, s>>>(A.nelem, A.ndof, A.geo, A.e2l, A.kappa, A.f, A.wk, A.gk, A.wr,
+    element_kernel<P><<<blocks, W * 32, 0, s>>>(A.nelem, A.ndof, A.geo, A.e2l, A.kappa, A.mass, A.f, A.wk, A.gk, A.wr,
                                                 A.br, A.Ke, A.Re, A.Km, A.status);
 }
 

@@ -10,6 +10,7 @@ struct ElemArgs {
     const double *verts;
     const int32_t *elems, *e2l;
     const double *kappa, *f;                 // may be null
+    double mass;                             // mass coefficient c (0: stiffness only)
     const double *wk, *gk, *wr, *br;         // element tables
     double *geo;                             // scratch: nelem * geometry_doubles
     double *Ke, *Re;

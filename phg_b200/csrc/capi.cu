@@ -160,6 +160,7 @@ struct phgGpuSystem_ {
     DevBuf<int32_t> rp, ci, brp, bci;
     DevBuf<double> va, bva, rhs, diag;
     bool assembled = false;
+    double mass = 0.0;   // mass coefficient of the built system
     bool have_bdry_cols = false;
 
     // solver
@@ -597,9 +598,10 @@ int phgGpuSetDofMap(phgGpuSystem *s, int order, int64_t ndof, const int32_t *e2l
     return PHG_GPU_OK;
 }
 
-int phgGpuBuildLinearSystem(phgGpuSystem *s, const double *kappa, const double *f, const double *g) {
+static int build_system(phgGpuSystem *s, const double *kappa, double mass, const double *f, const double *g) {
     if (s == nullptr) return fail(PHG_GPU_ERR_ARG, "null system");
     if (!s->have_dofs) return fail(PHG_GPU_ERR_STATE, "phgGpuBuildLinearSystem: call phgGpuSetDofMap first");
+    if (!isfinite(mass)) return fail(PHG_GPU_ERR_ARG, "phgGpuBuildLinearSystemMass: mass coefficient not finite");
     CHECK_RC(set_device(s));
     const int N = s->N;
     const int64_t ndof = s->ndof;
@@ -615,7 +617,7 @@ int phgGpuBuildLinearSystem(phgGpuSystem *s, const double *kappa, const double *
     ElemArgs ea{};
     ea.nelem = s->nelem; ea.nvert = s->nvert; ea.ndof = ndof;
     ea.verts = s->verts.p; ea.elems = s->elems.p; ea.e2l = s->e2l.p;
-    ea.kappa = dk; ea.f = df;
+    ea.kappa = dk; ea.f = df; ea.mass = mass;
     ea.wk = s->wk.p; ea.gk = s->gk.p; ea.wr = s->wr.p; ea.br = s->br.p;
     ea.Ke = s->Ke.p; ea.Re = s->Re.p; ea.Km = s->Km.p; ea.geo = s->geo.p; ea.status = s->status.p;
     CK(launch_element_kernel(s->order, ea, s->stream));
@@ -658,7 +660,17 @@ int phgGpuBuildLinearSystem(phgGpuSystem *s, const double *kappa, const double *
     s->sell_valid = false;
     s->sell2_valid = false;
     s->lpr = spmv_lanes_for((double)s->nnz / (double)ndof);
+    s->mass = mass;
     return PHG_GPU_OK;
+}
+
+int phgGpuBuildLinearSystem(phgGpuSystem *s, const double *kappa, const double *f, const double *g) {
+    return build_system(s, kappa, 0.0, f, g);
+}
+
+int phgGpuBuildLinearSystemMass(phgGpuSystem *s, const double *kappa, double mass_coef, const double *f,
+                                const double *g) {
+    return build_system(s, kappa, mass_coef, f, g);
 }
 
 int phgGpuSetMatrix(phgGpuSystem *s, int64_t n, const int64_t *ptr, const int32_t *cols, const double *vals,
@@ -1079,6 +1091,9 @@ int phgGpuAdjointGradient(phgGpuSystem *s, const double *u, const double *u_obs,
         return fail(PHG_GPU_ERR_ARG, "invalid arguments");
     if (!s->assembled || !s->have_bdry_cols)
         return fail(PHG_GPU_ERR_STATE, "phgGpuAdjointGradient: needs a system built by phgGpuBuildLinearSystem");
+    if (s->mass != 0.0)
+        return fail(PHG_GPU_ERR_STATE, "phgGpuAdjointGradient: the system has a mass term (only kappa-scaled "
+                                       "stiffness is differentiated)");
     if (maxit < 0) return fail(PHG_GPU_ERR_ARG, "maxit < 0");
     CHECK_RC(set_device(s));
     CHECK_RC(solver_buffers(s));

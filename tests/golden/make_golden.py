@@ -9,7 +9,9 @@ maps as PHG numbered them, f and g at the DOF nodes, Dirichlet flags, kappa)
 and outputs (matrix rows before and after boundary elimination, saved
 boundary columns, RHS before/after update_rhs, Jacobi diagonal, solution,
 iteration count, residual) in one compressed .npz per case, plus the
-reference's quadrature rules (quad_rules.npz).
+reference's quadrature rules (quad_rules.npz).  Cases with a mass
+coefficient c assemble -div(kappa grad u) + c u = f: each element matrix is
+stiffness + c * phgQuadBasDotBas, as in examples/simplest.c:68-72.
 
 Run here, where the reference is available:  python tests/golden/make_golden.py
 """
@@ -28,7 +30,7 @@ from phg_b200.mesh import kuhn_cube, write_medit  # noqa: E402
 DUMP = os.path.join(ROOT, "oracle", "_ref", "phg_dump")
 QDUMP = os.path.join(ROOT, "oracle", "_ref", "quad_dump")
 
-# name: (m, P, rhs case, kappa seed or None, rtol)
+# name: (m, P, rhs case, kappa seed or None, rtol[, mass coefficient])
 CASES = {
     "p1_m4_sine": (4, 1, "sine", None, 1e-10),
     "p1_m5_kappa": (5, 1, "sine", 11, 1e-10),
@@ -38,10 +40,13 @@ CASES = {
     "p3_m2_sine": (2, 3, "sine", None, 1e-10),
     "p3_m3_linear": (3, 3, "linear", None, 1e-10),
     "p3_m3_kappa": (3, 3, "sine", 13, 1e-10),
+    "p1_m5_mass": (5, 1, "sine", None, 1e-10, 3.7),
+    "p2_m4_kappa_mass": (4, 2, "sine", 14, 1e-10, 0.3),
+    "p3_m3_mass": (3, 3, "linear", None, 1e-10, 25.0),
 }
 
 
-def run_case(name, m, P, case, kseed, rtol):
+def run_case(name, m, P, case, kseed, rtol, mass=0.0):
     with tempfile.TemporaryDirectory() as d:
         v, e = kuhn_cube(m)
         write_medit(os.path.join(d, "m.mesh"), v, e)
@@ -49,6 +54,8 @@ def run_case(name, m, P, case, kseed, rtol):
                 "-solver", "pcg", "-pcg_pc_type", "jacobi", "-solver_rtol", repr(rtol),
                 "-solver_btol", "0", "-solver_atol", "0", "-solver_maxit", "10000",
                 "-map_reorder", "no", "-dump_dir", d, "-rhs_case", case]
+        if mass != 0.0:
+            args += ["-mass_coef", repr(mass)]
         kappa = None
         if kseed is not None:
             kappa = np.exp(np.random.default_rng(kseed).standard_normal(len(e)))
@@ -61,7 +68,7 @@ def run_case(name, m, P, case, kseed, rtol):
             return np.fromfile(os.path.join(d, n), t)
         N = int(meta["nbas"])
         out = dict(
-            order=P, m=m, rtol=rtol, nits=int(meta["nits"]),
+            order=P, m=m, rtol=rtol, nits=int(meta["nits"]), mass=float(meta["mass_coef"]),
             residual=float(meta["residual"]),
             verts=L("verts.f64", np.float64).reshape(-1, 3),
             elems=L("elems.i32", np.int32).reshape(-1, 4),
@@ -96,5 +103,7 @@ def quad_rules():
 
 if __name__ == "__main__":
     quad_rules()
+    only = sys.argv[1:]
     for name, args in CASES.items():
-        run_case(name, *args)
+        if not only or name in only:
+            run_case(name, *args)

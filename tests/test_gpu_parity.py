@@ -18,11 +18,11 @@ from conftest import golden_cases, load_golden
 pytestmark = pytest.mark.gpu
 
 
-def build(pb, order, verts, elems, e2l, bdry, f, g=None, kappa=None):
+def build(pb, order, verts, elems, e2l, bdry, f, g=None, kappa=None, mass=0.0):
     s = pb.Solver(0)
     s.set_mesh(verts, elems)
     s.set_dof_map(order, e2l, bdry)
-    s.build_linear_system(kappa=kappa, f=f, g=g)
+    s.build_linear_system(kappa=kappa, f=f, g=g, mass=mass)
     return s
 
 
@@ -35,7 +35,7 @@ def solution_tol(rtol):
 def test_golden_assembly_bitexact(gpu, name):
     G = load_golden(name)
     s = build(gpu, int(G["order"]), G["verts"], G["elems"], G["e2l"], G["bdry"], G["f"], G["g"],
-              G.get("kappa"))
+              G.get("kappa"), float(G.get("mass", 0.0)))
     ptr, cols, vals = s.get_matrix()
     assert np.array_equal(ptr, G["rows_ptr"])
     assert np.array_equal(cols, G["rows_cols"])
@@ -53,7 +53,7 @@ def test_golden_assembly_bitexact(gpu, name):
 def test_golden_pcg(gpu, name):
     G = load_golden(name)
     s = build(gpu, int(G["order"]), G["verts"], G["elems"], G["e2l"], G["bdry"], G["f"], G["g"],
-              G.get("kappa"))
+              G.get("kappa"), float(G.get("mass", 0.0)))
     rtol = float(G["rtol"])
     x, nits, res, hist = s.solve_pcg(rtol=rtol, btol=0.0, atol=0.0, history=True)
     assert abs(nits - int(G["nits"])) <= 2
@@ -87,6 +87,41 @@ def test_larger_meshes_vs_oracle(gpu, oracle, p, m):
     # the GPU's own residual, recomputed independently in FP64 by the oracle
     r = o["rhs"] - oracle.spmv(o["ptr"], o["cols"], o["vals"], x)
     assert np.linalg.norm(r) <= 2 * rtol * np.linalg.norm(o["rhs"])
+    s.close()
+
+
+@pytest.mark.parametrize("p,m,mass", [(1, 24, 1e3), (2, 10, 0.7), (3, 5, 42.0)])
+def test_mass_term_vs_oracle(gpu, oracle, p, m, mass):
+    """-div(kappa grad u) + c u = f: element matrices stiffness + c * mass
+    (examples/simplest.c:68-72), bit for bit against the oracle on meshes
+    larger than the golden cases; the mass term makes the system better
+    conditioned, so PCG needs fewer iterations than without it."""
+    v, e = gpu.kuhn_cube(m)
+    e2l, bdry, nodes = gpu.lagrange_dofs(v, e, p)
+    f = gpu.sine_source(nodes)
+    kappa = np.exp(0.5 * np.random.default_rng(p * 1000 + m).standard_normal(len(e)))
+    o = oracle.assemble(p, v, e, e2l, bdry, f, None, kappa, mass)
+    s = build(gpu, p, v, e, e2l, bdry, f, None, kappa, mass)
+    ptr, cols, vals = s.get_matrix()
+    assert np.array_equal(ptr, o["ptr"])
+    assert np.array_equal(cols, o["cols"])
+    assert np.array_equal(vals, o["vals"])
+    bptr, bcols, bvals = s.get_bdry_columns()
+    assert np.array_equal(bcols, o["bcols"]) and np.array_equal(bvals, o["bvals"])
+    assert np.array_equal(s.get_rhs(), o["rhs"])
+    assert np.array_equal(s.get_diagonal(), o["diag"])
+    xo, no, _, _ = oracle.pcg(o["ptr"], o["cols"], o["vals"], o["diag"], o["rhs"], rtol=1e-10,
+                              btol=0.0, atol=0.0)
+    x, nits, _ = s.solve_pcg(rtol=1e-10, btol=0.0, atol=0.0)
+    assert abs(nits - no) <= 2
+    assert np.linalg.norm(x - xo) <= solution_tol(1e-10) * np.linalg.norm(xo)
+    # the adjoint differentiates kappa-scaled stiffness only: a mass term is refused
+    with pytest.raises(gpu.PhgGpuError) as ei:
+        s.adjoint_gradient(x, x, rtol=1e-8)
+    assert ei.value.code == -3
+    s.build_linear_system(kappa=kappa, f=f)
+    _, n0, _ = s.solve_pcg(rtol=1e-10, btol=0.0, atol=0.0)
+    assert nits <= n0
     s.close()
 
 

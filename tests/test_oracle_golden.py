@@ -20,7 +20,7 @@ def test_quadrature_rules_bitexact(oracle):
 def test_assembly_bitexact(oracle, name):
     G = load_golden(name)
     o = oracle.assemble(int(G["order"]), G["verts"], G["elems"], G["e2l"], G["bdry"], G["f"],
-                        G["g"], G.get("kappa"))
+                        G["g"], G.get("kappa"), float(G.get("mass", 0.0)))
     for pre, op in (("rows_raw", "raw_"), ("rows", ""), ("bdry_rows", "b")):
         assert np.array_equal(G[pre + "_ptr"], o[op + "ptr"]), pre
         assert np.array_equal(G[pre + "_cols"], o[op + "cols"]), pre
