@@ -133,6 +133,18 @@ int phgGpuSolverPCG(phgGpuSystem *sys, double rtol, double btol,
 		    double atol, int maxit, double *x, double *residual,
 		    double *hist);
 
+/* Jacobi-preconditioned BiCGstab, FP64 (solver_BiCGstab,
+ * src/solver-phg.c:606-781, what phgSolverSolve runs with -solver bicgstab;
+ * same stopping rule and arguments as phgGpuSolverPCG).  For matrices that
+ * are not symmetric positive definite (the reference flags it M_UNSYM,
+ * :2542-2547), e.g. installed with phgGpuSetMatrix.  Where the reference
+ * stops because rho = r.rh is 0 ("method failed", :676-680) the call
+ * returns the iteration count as the reference does; a zero rh.v or t.t,
+ * where the reference would divide by zero, is PHG_GPU_ERR_BREAKDOWN. */
+int phgGpuSolverBiCGstab(phgGpuSystem *sys, double rtol, double btol,
+			 double atol, int maxit, double *x, double *residual,
+			 double *hist);
+
 /* Jacobi-PCG for many right-hand sides at once: column k of B (n x nrhs,
  * row major: B[i * nrhs + k]) is solved by its own PCG recurrence and
  * stopping rule (rtol relative to ||b_k||, from x = 0), and the columns share

@@ -717,3 +717,123 @@ pho_pcg(int64_t n, const int64_t *ptr, const int32_t *cols,
 	*res = residual;
     return nits;
 }
+
+/* y = b y + a x with the rounding of phgVecAXPBY (matvec.c:1237-1295): the
+ * special cases a, b = +-1 there give the same values as the general form. */
+static void
+axpby(int64_t n, double a, const double *x, double b, double *y)
+{
+    int64_t i;
+    if (b != 1.0)
+	for (i = 0; i < n; i++)
+	    y[i] = b * y[i];
+    if (a == 0.0)
+	return;
+    for (i = 0; i < n; i++)
+	y[i] += a * x[i];
+}
+
+int
+pho_bicgstab(int64_t n, const int64_t *ptr, const int32_t *cols,
+	     const double *vals, const double *diag, const double *b,
+	     double *x, int maxit, double rtol, double btol, double atol,
+	     double *res, double *hist, int *status)
+/* solver_BiCGstab (solver-phg.c:606-781) with jacobi_pc (:207-245).
+ * *status: 0 normal end, 1 rho == 0 ("method failed"), 2 ||s|| <= 1e-60
+ * (x corrected and the residual recomputed from b - A x). */
+{
+    double *r1 = malloc(n * sizeof(double)), *rg = malloc(n * sizeof(double));
+    double *rh = malloc(n * sizeof(double)), *pg = malloc(n * sizeof(double));
+    double *ph = calloc(n, sizeof(double)), *sg = malloc(n * sizeof(double));
+    double *sh = calloc(n, sizeof(double)), *tg = malloc(n * sizeof(double));
+    double *vg = malloc(n * sizeof(double));
+    double rb, r0, residual, tol, rho0 = 0., rho1, alpha = 0., beta, omega = 0.;
+    double x1 = 0.0;
+    int64_t i;
+    int nits = 0;
+
+    if (status != NULL)
+	*status = 0;
+    rb = norm2(n, b);
+    if (IS_ZERO(rb)) {
+	memset(x, 0, n * sizeof(double));
+	residual = 0.0;
+	goto done;
+    }
+    for (i = 0; i < n; i++)
+	x1 += fabs(x[i]);
+    if (!IS_ZERO(x1 / n)) {
+	pho_spmv(n, ptr, cols, vals, x, r1);
+	memcpy(rg, r1, n * sizeof(double));
+	axpby(n, 1.0, b, -1.0, rg);
+    }
+    else
+	memcpy(rg, b, n * sizeof(double));
+    r0 = residual = norm2(n, rg);
+    tol = r0 * rtol;
+    if (tol < rb * btol)
+	tol = rb * btol;
+    if (tol < atol)
+	tol = atol;
+    if (hist != NULL)
+	hist[0] = residual;
+    memcpy(rh, rg, n * sizeof(double));
+
+    while (residual > tol && nits < maxit) {
+	nits++;
+	rho1 = dot(n, rg, rh);
+	if (rho1 == 0.0) {
+	    if (status != NULL)
+		*status = 1;
+	    break;
+	}
+	if (nits == 1)
+	    memcpy(pg, rg, n * sizeof(double));
+	else {
+	    beta = (rho1 * alpha) / (rho0 * omega);
+	    memcpy(sg, pg, n * sizeof(double));
+	    axpby(n, -omega, vg, 1., sg);
+	    memcpy(pg, rg, n * sizeof(double));
+	    axpby(n, beta, sg, 1., pg);
+	}
+	rho0 = rho1;
+	for (i = 0; i < n; i++)
+	    ph[i] = pg[i] / diag[i];
+	pho_spmv(n, ptr, cols, vals, ph, vg);
+	alpha = rho1 / dot(n, rh, vg);
+	memcpy(sg, rg, n * sizeof(double));
+	axpby(n, -alpha, vg, 1., sg);
+	omega = norm2(n, sg);
+	if (omega <= 1e-60) {
+	    axpby(n, alpha, ph, 1., x);
+	    pho_spmv(n, ptr, cols, vals, x, r1);
+	    memcpy(rg, b, n * sizeof(double));
+	    axpby(n, -1, r1, 1., rg);
+	    residual = norm2(n, rg);
+	    if (hist != NULL)
+		hist[nits] = residual;
+	    if (status != NULL)
+		*status = 2;
+	    break;
+	}
+	for (i = 0; i < n; i++)
+	    sh[i] = sg[i] / diag[i];
+	pho_spmv(n, ptr, cols, vals, sh, tg);
+	omega = dot(n, tg, sg) / dot(n, tg, tg);
+	axpby(n, omega, sh, alpha, ph);
+	axpby(n, 1, ph, 1, x);
+	memcpy(rg, sg, n * sizeof(double));
+	axpby(n, -omega, tg, 1, rg);
+	residual = norm2(n, rg);
+	if (hist != NULL)
+	    hist[nits] = residual;
+	if (residual <= tol)
+	    break;
+    }
+done:
+    free(r1); free(rg); free(rh); free(pg); free(ph);
+    free(sg); free(sh); free(tg); free(vg);
+    if (res != NULL)
+	*res = residual;
+    return nits;
+}

@@ -96,6 +96,15 @@ int pho_pcg(int64_t n, const int64_t *ptr, const int32_t *cols,
 	    double *x, int maxit, double rtol, double btol, double atol,
 	    double *residual, double *hist);
 
+/* Jacobi-preconditioned BiCGstab (solver_BiCGstab, solver-phg.c:606-781):
+ * arguments as pho_pcg; hist[k] = ||r|| after iteration k.  *status (may be
+ * NULL): 0 normal end, 1 rho = 0 (the reference's "method failed" break),
+ * 2 ||s|| <= 1e-60 (x corrected, residual recomputed from b - A x). */
+int pho_bicgstab(int64_t n, const int64_t *ptr, const int32_t *cols,
+		 const double *vals, const double *diag, const double *b,
+		 double *x, int maxit, double rtol, double btol, double atol,
+		 double *residual, double *hist, int *status);
+
 #ifdef __cplusplus
 }
 #endif

@@ -39,6 +39,8 @@ SIGNATURES = {
     "phgGpuMatVec": (C.c_int, [_P, _P, _P]),
     "phgGpuSolverPCG": (C.c_int, [_P, C.c_double, C.c_double, C.c_double, C.c_int, _P,
                                   C.POINTER(C.c_double), _P]),
+    "phgGpuSolverBiCGstab": (C.c_int, [_P, C.c_double, C.c_double, C.c_double, C.c_int, _P,
+                                       C.POINTER(C.c_double), _P]),
     "phgGpuGetLaunchCount": (C.c_int, [_P, C.POINTER(_I64)]),
     "phgGpuGetSpMVPlan": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), _P]),
     "phgGpuSetSpMVPlan": (C.c_int, [_P, C.c_int, C.c_int]),
@@ -280,6 +282,22 @@ class Solver:
         res = C.c_double()
         nits = _check(lib().phgGpuSolverPCG(self._h, rtol, btol, atol, int(maxit), _ptr(x),
                                             C.byref(res), _ptr(hist)))
+        if history:
+            return x, nits, res.value, hist[:nits + 1]
+        return x, nits, res.value
+
+    def solve_bicgstab(self, x0=None, rtol=1e-10, btol=1e-10, atol=0.0, maxit=10000, history=False, out=None):
+        """phgSolverSolve with -solver bicgstab -pcg_pc_type jacobi.  Returns
+        (x, nits, residual) or (x, nits, residual, history)."""
+        n = self.sizes()[0]
+        if out is not None:
+            x = out
+        else:
+            x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+        hist = np.empty(maxit + 1) if history else None
+        res = C.c_double()
+        nits = _check(lib().phgGpuSolverBiCGstab(self._h, rtol, btol, atol, int(maxit), _ptr(x),
+                                                 C.byref(res), _ptr(hist)))
         if history:
             return x, nits, res.value, hist[:nits + 1]
         return x, nits, res.value

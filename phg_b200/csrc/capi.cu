@@ -8,6 +8,7 @@
 #include "solve.h"
 #include "adjoint.h"
 #include "block.h"
+#include "bicgstab.h"
 
 #include <math.h>
 #include <float.h>
@@ -221,6 +222,12 @@ struct phgGpuSystem_ {
     MixedState *h_mst = nullptr;
     cudaGraphExec_t graph_mixed = nullptr;
     GraphKey gkey_mixed{};
+    // BiCGstab: its seven working vectors in one buffer, its state
+    DevBuf<double> bicg_vecs;
+    DevBuf<BicgState> bicg_st;
+    BicgState *h_bst = nullptr;
+    cudaGraphExec_t graph_bicg = nullptr;
+    GraphKey gkey_bicg{};
 };
 
 namespace {
@@ -495,6 +502,10 @@ int phgGpuDestroy(phgGpuSystem *s) {
     if (s->graph != nullptr) cudaGraphExecDestroy(s->graph);
     if (s->graph_mixed != nullptr) cudaGraphExecDestroy(s->graph_mixed);
     if (s->h_mst) cudaFreeHost(s->h_mst);
+    if (s->graph_bicg != nullptr) cudaGraphExecDestroy(s->graph_bicg);
+    if (s->h_bst) cudaFreeHost(s->h_bst);
+    s->bicg_vecs.release();
+    s->bicg_st.release();
     DevBuf<float> *fbufs[] = {&s->r32, &s->p32, &s->Ap32, &s->y32, &s->D32, &s->sell_vals32, &s->sell2_vals};
     s->sell2_ssz.release(); s->sell2_sptr.release(); s->sell2_cols.release();
     for (auto *b : fbufs) b->release();
@@ -1059,6 +1070,107 @@ int pcg_core(phgGpuSystem *s, const double *drhs, double rtol, double btol, doub
     return nits;
 }
 
+// BiCGstab with the Jacobi preconditioner (solver_BiCGstab,
+// solver-phg.c:606-781) from the initial guess in s->x.
+int bicg_core(phgGpuSystem *s, double rtol, double btol, double atol, int maxit, double *dhist,
+              double *residual) {
+    const int64_t n = s->n;
+    const double *drhs = s->rhs.p;
+    CK(cudaMemsetAsync(s->ticket.p, 0, sizeof(unsigned), s->stream));
+    CK(launch_init_sums(n, 0, s->x.p, drhs, s->diag.p, s->partials.p, s->ticket.p, s->sums.p, s->stream));
+    s->launches += 1;
+    CK(cudaMemcpyAsync(s->h_sums, s->sums.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    const double x1 = s->h_sums[0], rb = sqrt(s->h_sums[1]);
+    auto is_zero = [](double a) { return fabs(a) < 10.0 * DBL_MIN; };   // utils.h:451
+    if (is_zero(rb)) {   // solver-phg.c:630-633
+        CK(cudaMemsetAsync(s->x.p, 0, sizeof(double) * n, s->stream));
+        if (residual) *residual = 0.0;
+        if (dhist) CK(cudaMemsetAsync(dhist, 0, sizeof(double), s->stream));
+        return 0;
+    }
+    CHECK_RC(tune_spmv(s));
+    const int64_t stride = bicg_stride(n);
+    CHECK_RC(s->bicg_vecs.ensure((size_t)stride * kBicgVectors));
+    CHECK_RC(s->bicg_st.ensure(1));
+    if (s->h_bst == nullptr) CK(cudaMallocHost((void **)&s->h_bst, sizeof(BicgState)));
+    double *V = s->bicg_vecs.p;
+    BicgBuffers B{n, s->x.p, s->r.p, V, V + stride, V + 2 * stride, V + 3 * stride, V + 4 * stride,
+                  V + 5 * stride, V + 6 * stride, s->diag.p, s->partials.p, s->bicg_st.p, dhist};
+    // r = b - A x, or b when x = 0 (solver-phg.c:645-653)
+    if (!is_zero(x1 / (double)n)) {
+        CK(launch_spmv_plan(s->plan, s->x.p, s->Ap.p, s->stream));
+        CK(launch_residual(n, drhs, s->Ap.p, B.rg, s->stream));
+        s->launches += 2;
+    } else {
+        CK(cudaMemcpyAsync(B.rg, drhs, sizeof(double) * n, cudaMemcpyDeviceToDevice, s->stream));
+    }
+    CK(launch_init_sums(n, 1, s->x.p, B.rg, s->diag.p, s->partials.p, s->ticket.p, s->sums.p, s->stream));
+    s->launches += 1;
+    CK(cudaMemcpyAsync(B.rh, B.rg, sizeof(double) * n, cudaMemcpyDeviceToDevice, s->stream));
+    CK(cudaMemcpyAsync(s->h_sums, s->sums.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    const double rr0 = s->h_sums[0], r0 = sqrt(rr0);
+    double tol = r0 * rtol;   // get_tol (solver-phg.c:104-115)
+    if (tol < rb * btol) tol = rb * btol;
+    if (tol < atol) tol = atol;
+
+    BicgState init{};
+    init.rho1 = rr0;   // r.rh with rh = r
+    init.residual = r0;
+    init.tol = tol;
+    init.maxit = maxit;
+    init.done = !(r0 > tol && 0 < maxit);
+    *s->h_bst = init;
+    CK(cudaMemcpyAsync(B.st, s->h_bst, sizeof(BicgState), cudaMemcpyHostToDevice, s->stream));
+    if (dhist) CK(cudaMemcpyAsync(dhist, &s->h_bst->residual, sizeof(double), cudaMemcpyHostToDevice, s->stream));
+
+    phgGpuSystem_::GraphKey key{};
+    key.x = B.x; key.r = B.rg; key.p = B.rh; key.D = B.D; key.hist = dhist;
+    key.n = n; key.lpr = s->plan.kind * 100 + s->plan.lpr * 10 + s->plan.unroll; key.s = s->stream;
+    key.va = s->plan.kind == SPMV_CSR ? (const void *)s->va.p : (const void *)s->sell_vals.p;
+    if (s->graph_bicg == nullptr || !(s->gkey_bicg == key)) {
+        if (s->graph_bicg != nullptr) { cudaGraphExecDestroy(s->graph_bicg); s->graph_bicg = nullptr; }
+        cudaGraph_t gr;
+        CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+        for (int i = 0; i < kGraphChunk; i++) launch_bicg_iteration(B, s->plan, s->stream);
+        CK(cudaStreamEndCapture(s->stream, &gr));
+        cudaError_t e = cudaGraphInstantiate(&s->graph_bicg, gr, 0);
+        cudaGraphDestroy(gr);
+        CK(e);
+        s->gkey_bicg = key;
+    }
+    while (!s->h_bst->done) {
+        CK(cudaGraphLaunch(s->graph_bicg, s->stream));
+        s->launches += 5 * kGraphChunk;
+        CK(cudaMemcpyAsync(s->h_bst, B.st, sizeof(BicgState), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+    }
+    const int nits = s->h_bst->nits;
+    double res = s->h_bst->residual;
+    if (s->h_bst->status == BICG_SMALL_S) {
+        // x += alpha p^, then the residual of b - A x (solver-phg.c:717-729)
+        CK(launch_bicg_small_s(B, s->stream));
+        CK(launch_spmv_plan(s->plan, s->x.p, s->Ap.p, s->stream));
+        CK(launch_residual(n, drhs, s->Ap.p, B.rg, s->stream));
+        CK(launch_init_sums(n, 1, s->x.p, B.rg, s->diag.p, s->partials.p, s->ticket.p, s->sums.p, s->stream));
+        s->launches += 4;
+        CK(cudaMemcpyAsync(s->h_sums, s->sums.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        res = sqrt(s->h_sums[0]);
+        s->h_bst->residual = res;
+        if (dhist)
+            CK(cudaMemcpyAsync(dhist + nits, &s->h_bst->residual, sizeof(double), cudaMemcpyHostToDevice,
+                               s->stream));
+    }
+    if (residual) *residual = res;
+    if (s->h_bst->status == BICG_BREAKDOWN)
+        return fail(PHG_GPU_ERR_BREAKDOWN, "BiCGstab breakdown after %d iterations (rh.v = 0 or t.t = 0)", nits);
+    if (s->h_bst->status == BICG_NONFINITE)
+        return fail(PHG_GPU_ERR_NAN, "BiCGstab: non-finite values after %d iterations", nits);
+    return nits;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1078,6 +1190,28 @@ int phgGpuSolverPCG(phgGpuSystem *s, double rtol, double btol, double atol, int 
         dhist = s->hist.p;
     }
     const int nits = pcg_core(s, s->rhs.p, rtol, btol, atol, maxit, dhist, residual);
+    if (nits < 0) return nits;
+    CHECK_RC(copy_out(s, x, s->x.p, (size_t)n));
+    if (hist) CHECK_RC(copy_out(s, hist, dhist, (size_t)nits + 1));
+    CK(cudaStreamSynchronize(s->stream));
+    return nits;
+}
+
+int phgGpuSolverBiCGstab(phgGpuSystem *s, double rtol, double btol, double atol, int maxit, double *x,
+                         double *residual, double *hist) {
+    if (s == nullptr || x == nullptr) return fail(PHG_GPU_ERR_ARG, "invalid arguments");
+    if (!s->assembled) return fail(PHG_GPU_ERR_STATE, "no assembled system");
+    if (maxit < 0) return fail(PHG_GPU_ERR_ARG, "maxit < 0");
+    CHECK_RC(set_device(s));
+    CHECK_RC(solver_buffers(s));
+    const int64_t n = s->n;
+    CHECK_RC(copy_in(s, s->x.p, x, (size_t)n));
+    double *dhist = nullptr;
+    if (hist != nullptr) {
+        CHECK_RC(s->hist.ensure((size_t)maxit + 1));
+        dhist = s->hist.p;
+    }
+    const int nits = bicg_core(s, rtol, btol, atol, maxit, dhist, residual);
     if (nits < 0) return nits;
     CHECK_RC(copy_out(s, x, s->x.p, (size_t)n));
     if (hist) CHECK_RC(copy_out(s, hist, dhist, (size_t)nits + 1));

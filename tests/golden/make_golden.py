@@ -3,7 +3,7 @@ reference (PHG 0.9.7) built from its own sources by `make -C oracle ref`.
 
 For every case it writes the mesh as Medit, runs oracle/_ref/phg_dump (the
 reference's element loop + phgSolverAssemble + phgSolverUpdateRHS +
-phgSolverSolve with -solver pcg, see oracle/ref_driver/phg_dump.c) and stores
+phgSolverSolve with -solver pcg or bicgstab, see oracle/ref_driver/phg_dump.c) and stores
 the reference's own inputs (coordinates, element vertices and element->DOF
 maps as PHG numbered them, f and g at the DOF nodes, Dirichlet flags, kappa)
 and outputs (matrix rows before and after boundary elimination, saved
@@ -30,7 +30,7 @@ from phg_b200.mesh import kuhn_cube, write_medit  # noqa: E402
 DUMP = os.path.join(ROOT, "oracle", "_ref", "phg_dump")
 QDUMP = os.path.join(ROOT, "oracle", "_ref", "quad_dump")
 
-# name: (m, P, rhs case, kappa seed or None, rtol[, mass coefficient])
+# name: (m, P, rhs case, kappa seed or None, rtol[, mass coefficient[, solver]])
 CASES = {
     "p1_m4_sine": (4, 1, "sine", None, 1e-10),
     "p1_m5_kappa": (5, 1, "sine", 11, 1e-10),
@@ -43,15 +43,18 @@ CASES = {
     "p1_m5_mass": (5, 1, "sine", None, 1e-10, 3.7),
     "p2_m4_kappa_mass": (4, 2, "sine", 14, 1e-10, 0.3),
     "p3_m3_mass": (3, 3, "linear", None, 1e-10, 25.0),
+    "p1_m6_bicgstab": (6, 1, "sine", None, 1e-10, 0.0, "bicgstab"),
+    "p2_m5_kappa_bicgstab": (5, 2, "sine", 12, 1e-10, 0.0, "bicgstab"),
+    "p3_m3_mass_bicgstab": (3, 3, "linear", None, 1e-12, 25.0, "bicgstab"),
 }
 
 
-def run_case(name, m, P, case, kseed, rtol, mass=0.0):
+def run_case(name, m, P, case, kseed, rtol, mass=0.0, solver="pcg"):
     with tempfile.TemporaryDirectory() as d:
         v, e = kuhn_cube(m)
         write_medit(os.path.join(d, "m.mesh"), v, e)
         args = [DUMP, "-mesh_file", os.path.join(d, "m.mesh"), "-dof_type", "P%d" % P,
-                "-solver", "pcg", "-pcg_pc_type", "jacobi", "-solver_rtol", repr(rtol),
+                "-solver", solver, "-pcg_pc_type", "jacobi", "-solver_rtol", repr(rtol),
                 "-solver_btol", "0", "-solver_atol", "0", "-solver_maxit", "10000",
                 "-map_reorder", "no", "-dump_dir", d, "-rhs_case", case]
         if mass != 0.0:
@@ -68,7 +71,7 @@ def run_case(name, m, P, case, kseed, rtol, mass=0.0):
             return np.fromfile(os.path.join(d, n), t)
         N = int(meta["nbas"])
         out = dict(
-            order=P, m=m, rtol=rtol, nits=int(meta["nits"]), mass=float(meta["mass_coef"]),
+            order=P, m=m, rtol=rtol, nits=int(meta["nits"]), mass=float(meta["mass_coef"]), solver=solver,
             residual=float(meta["residual"]),
             verts=L("verts.f64", np.float64).reshape(-1, 3),
             elems=L("elems.i32", np.int32).reshape(-1, 4),

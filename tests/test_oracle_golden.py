@@ -29,11 +29,21 @@ def test_assembly_bitexact(oracle, name):
         assert np.array_equal(G[k], o[k]), k
 
 
+def solver_of(G):
+    return str(G["solver"]) if "solver" in G else "pcg"
+
+
 @pytest.mark.parametrize("name", golden_cases())
-def test_pcg_bitexact(oracle, name):
+def test_solver_bitexact(oracle, name):
+    """Iteration count, final residual and solution of the reference's
+    solve_pcg or solver_BiCGstab, bit for bit."""
     G = load_golden(name)
-    x, nits, res, hist = oracle.pcg(G["rows_ptr"], G["rows_cols"], G["rows_vals"], G["diag"],
-                                    G["rhs"], rtol=float(G["rtol"]), btol=0.0, atol=0.0)
+    args = (G["rows_ptr"], G["rows_cols"], G["rows_vals"], G["diag"], G["rhs"])
+    if solver_of(G) == "bicgstab":
+        x, nits, res, hist, status = oracle.bicgstab(*args, rtol=float(G["rtol"]), btol=0.0, atol=0.0)
+        assert status == 0
+    else:
+        x, nits, res, hist = oracle.pcg(*args, rtol=float(G["rtol"]), btol=0.0, atol=0.0)
     assert nits == int(G["nits"])
     assert res == float(G["residual"])
     assert np.array_equal(x, G["x"])
