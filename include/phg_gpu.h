@@ -145,6 +145,18 @@ int phgGpuSolverBiCGstab(phgGpuSystem *sys, double rtol, double btol,
 			 double atol, int maxit, double *x, double *residual,
 			 double *hist);
 
+/* Restarted right-preconditioned GMRES with the Jacobi preconditioner,
+ * FP64 (solver_GMRES_r, src/solver-phg.c:1050-1260: what phgSolverSolve
+ * runs with -solver gmres -gmres_type gmres_r -gmres_pc_type jacobi
+ * -gmres_restart `restart`; modified Gram-Schmidt, Givens rotations, same
+ * stopping rule as phgGpuSolverPCG).  restart in 1..64 (the reference's
+ * restart <= 0, "never restart", has no counterpart here).  *residual is
+ * the reference's: the rotated residual estimate on convergence, ||r0||
+ * when maxit ends the solve.  Returns the iteration count. */
+int phgGpuSolverGMRES(phgGpuSystem *sys, int restart, double rtol,
+		      double btol, double atol, int maxit, double *x,
+		      double *residual);
+
 /* Jacobi-PCG for many right-hand sides at once: column k of B (n x nrhs,
  * row major: B[i * nrhs + k]) is solved by its own PCG recurrence and
  * stopping rule (rtol relative to ||b_k||, from x = 0), and the columns share

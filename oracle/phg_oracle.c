@@ -837,3 +837,159 @@ done:
 	*res = residual;
     return nits;
 }
+
+/* y = alpha x (+ y when accumulate): phgMatVec with A = NULL
+ * (matvec.c:606-760); the special cases alpha = +-1 give the same values. */
+static void
+scale_add(int64_t n, double alpha, const double *x, int accumulate, double *y)
+{
+    int64_t i;
+    if (accumulate)
+	for (i = 0; i < n; i++)
+	    y[i] += alpha * x[i];
+    else
+	for (i = 0; i < n; i++)
+	    y[i] = alpha * x[i];
+}
+
+/* z = b - A x as phgVecCopy(b, &z) + phgMatVec(MAT_OP_N, -1.0, A, x, 1.0,
+ * &z) (matvec.c:840-928): each row adds sum_j a_ij (-x_j), which equals
+ * b_i - sum_j a_ij x_j exactly. */
+static void
+residual_vec(int64_t n, const int64_t *ptr, const int32_t *cols,
+	     const double *vals, const double *b, const double *x, double *z)
+{
+    int64_t i, j;
+    for (i = 0; i < n; i++) {
+	double s;
+	z[i] = b[i];
+	if (ptr[i + 1] == ptr[i])
+	    continue;
+	s = vals[ptr[i]] * -x[cols[ptr[i]]];
+	for (j = ptr[i] + 1; j < ptr[i + 1]; j++)
+	    s += vals[j] * -x[cols[j]];
+	z[i] += s;
+    }
+}
+
+int
+pho_gmres(int64_t n, const int64_t *ptr, const int32_t *cols,
+	  const double *vals, const double *diag, const double *b, double *x,
+	  int restart, int maxit, double rtol, double btol, double atol,
+	  double *res)
+/* solver_GMRES_r (solver-phg.c:1050-1260): right-preconditioned restarted
+ * GMRES with modified Gram-Schmidt and Givens rotations, Jacobi PC.  The
+ * residual reported is the rotated estimate |s[i+1]| at convergence and
+ * ||r0|| when maxit ends the run, as in the reference. */
+{
+    int R, nits = 0, i, j, k;
+    double b_norm, r0_norm, r_norm, residual, tol, tmp, h1, h2, x1 = 0.0;
+    double **V, *H, *y, *s, *c1, *c2, *z, *r;
+    int64_t l;
+
+    if (restart <= 0)
+	restart = maxit + 1;
+    R = restart + 2;
+    b_norm = norm2(n, b);
+    if (IS_ZERO(b_norm)) {
+	memset(x, 0, n * sizeof(double));
+	if (res != NULL)
+	    *res = 0.0;
+	return 0;
+    }
+    V = malloc(R * sizeof(*V));
+    for (i = 0; i < R; i++)
+	V[i] = malloc(n * sizeof(double));
+    H = malloc((size_t)R * R * sizeof(double));
+    y = malloc(4 * R * sizeof(double));
+    s = y + R;
+    c1 = y + 2 * R;
+    c2 = y + 3 * R;
+    z = malloc(n * sizeof(double));
+    r = V[0];
+#define Hij(a, b) H[(size_t)(a) * R + (b)]
+
+    for (l = 0; l < n; l++)
+	x1 += fabs(x[l]);
+    if (x1 != 0.)
+	residual_vec(n, ptr, cols, vals, b, x, z);
+    else
+	memcpy(z, b, n * sizeof(double));
+    r0_norm = r_norm = residual = norm2(n, z);
+    tol = r0_norm * rtol;
+    if (tol < b_norm * btol)
+	tol = b_norm * btol;
+    if (tol < atol)
+	tol = atol;
+
+    s[0] = 1.;
+    while (nits < maxit) {
+	s[1] = r_norm = norm2(n, z);
+	scale_add(n, 1.0 / r_norm, z, 0, V[1]);
+	i = 0;
+	memset(H, 0, (size_t)R * R * sizeof(double));
+	while (i < restart && r_norm > tol && nits < maxit) {
+	    double *v1;
+	    i++, nits++;
+	    v1 = V[i + 1];
+	    for (l = 0; l < n; l++)
+		r[l] = V[i][l] / diag[l];
+	    pho_spmv(n, ptr, cols, vals, r, v1);
+	    for (k = 1; k <= i; k++) {
+		Hij(i, k) = dot(n, v1, V[k]);
+		scale_add(n, -Hij(i, k), V[k], 1, v1);
+	    }
+	    Hij(i, i + 1) = norm2(n, v1);
+	    if (IS_ZERO(Hij(i, i + 1))) {
+		i--;
+		break;
+	    }
+	    tmp = 1.0 / Hij(i, i + 1);
+	    for (l = 0; l < n; l++)
+		v1[l] *= tmp;
+	    for (j = 1; j < i; j++) {
+		h1 = c1[j] * Hij(i, j) + c2[j] * Hij(i, j + 1);
+		h2 = -c2[j] * Hij(i, j) + c1[j] * Hij(i, j + 1);
+		Hij(i, j) = h1;
+		Hij(i, j + 1) = h2;
+	    }
+	    tmp = sqrt(Hij(i, i) * Hij(i, i) + Hij(i, i + 1) * Hij(i, i + 1));
+	    if (IS_ZERO(tmp))
+		tmp = 1.e-16;
+	    c1[i] = Hij(i, i) / tmp;
+	    c2[i] = Hij(i, i + 1) / tmp;
+	    s[i + 1] = -c2[i] * s[i];
+	    s[i] = c1[i] * s[i];
+	    Hij(i, i) = c1[i] * Hij(i, i) + c2[i] * Hij(i, i + 1);
+	    r_norm = fabs(s[i + 1]);
+	    if (r_norm <= tol)
+		break;
+	}
+	for (j = i; j > 0; j--) {
+	    y[j] = s[j] / Hij(j, j);
+	    for (k = j - 1; k > 0; k--)
+		s[k] -= Hij(j, k) * y[j];
+	}
+	if (i > 0) {
+	    scale_add(n, y[1], V[1], 0, z);
+	    for (j = 2; j <= i; j++)
+		scale_add(n, y[j], V[j], 1, z);
+	}
+	for (l = 0; l < n; l++)
+	    r[l] = z[l] / diag[l];
+	for (l = 0; l < n; l++)
+	    x[l] += r[l];
+	if (r_norm <= tol) {
+	    residual = r_norm;
+	    break;
+	}
+	residual_vec(n, ptr, cols, vals, b, x, z);
+    }
+#undef Hij
+    for (i = 0; i < R; i++)
+	free(V[i]);
+    free(V); free(H); free(y); free(z);
+    if (res != NULL)
+	*res = residual;
+    return nits;
+}

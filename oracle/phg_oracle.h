@@ -105,6 +105,15 @@ int pho_bicgstab(int64_t n, const int64_t *ptr, const int32_t *cols,
 		 double *x, int maxit, double rtol, double btol, double atol,
 		 double *residual, double *hist, int *status);
 
+/* Restarted right-preconditioned GMRES with the Jacobi PC (solver_GMRES_r,
+ * solver-phg.c:1050-1260; -solver gmres -gmres_type gmres_r).  restart <= 0
+ * means no restart.  *residual: the rotated residual estimate at
+ * convergence, ||r0|| when maxit ends the run (as the reference). */
+int pho_gmres(int64_t n, const int64_t *ptr, const int32_t *cols,
+	      const double *vals, const double *diag, const double *b,
+	      double *x, int restart, int maxit, double rtol, double btol,
+	      double atol, double *residual);
+
 #ifdef __cplusplus
 }
 #endif

@@ -41,6 +41,9 @@ def lib():
                                    C.c_double, C.c_double, C.c_double,
                                    C.POINTER(C.c_double), P, C.POINTER(C.c_int)]
         L.pho_bicgstab.restype = C.c_int
+        L.pho_gmres.argtypes = [C.c_int64, P, P, P, P, P, P, C.c_int, C.c_int,
+                                C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)]
+        L.pho_gmres.restype = C.c_int
         _LIB = L
     return _LIB
 
@@ -169,3 +172,18 @@ def bicgstab(ptr, cols, vals, diag, b, x0=None, maxit=10000, rtol=1e-10, btol=0.
                               _ptr(np.ascontiguousarray(b, np.float64)), _ptr(x),
                               maxit, rtol, btol, atol, C.byref(res), _ptr(hist), C.byref(st))
     return x, nits, res.value, hist[:nits + 1], st.value
+
+
+def gmres(ptr, cols, vals, diag, b, x0=None, restart=10, maxit=10000, rtol=1e-10, btol=0.0,
+          atol=0.0):
+    """Restarted right-preconditioned Jacobi-GMRES.  Returns (x, nits, residual)."""
+    n = len(ptr) - 1
+    x = np.zeros(n) if x0 is None else np.array(x0, np.float64)
+    res = C.c_double()
+    nits = lib().pho_gmres(n, _ptr(np.ascontiguousarray(ptr, np.int64)),
+                           _ptr(np.ascontiguousarray(cols, np.int32)),
+                           _ptr(np.ascontiguousarray(vals, np.float64)),
+                           _ptr(np.ascontiguousarray(diag, np.float64)),
+                           _ptr(np.ascontiguousarray(b, np.float64)), _ptr(x),
+                           restart, maxit, rtol, btol, atol, C.byref(res))
+    return x, nits, res.value

@@ -41,6 +41,8 @@ SIGNATURES = {
                                   C.POINTER(C.c_double), _P]),
     "phgGpuSolverBiCGstab": (C.c_int, [_P, C.c_double, C.c_double, C.c_double, C.c_int, _P,
                                        C.POINTER(C.c_double), _P]),
+    "phgGpuSolverGMRES": (C.c_int, [_P, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, _P,
+                                    C.POINTER(C.c_double)]),
     "phgGpuGetLaunchCount": (C.c_int, [_P, C.POINTER(_I64)]),
     "phgGpuGetSpMVPlan": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), _P]),
     "phgGpuSetSpMVPlan": (C.c_int, [_P, C.c_int, C.c_int]),
@@ -300,6 +302,21 @@ class Solver:
                                                  C.byref(res), _ptr(hist)))
         if history:
             return x, nits, res.value, hist[:nits + 1]
+        return x, nits, res.value
+
+
+    def solve_gmres(self, x0=None, restart=10, rtol=1e-10, btol=1e-10, atol=0.0, maxit=10000, out=None):
+        """phgSolverSolve with -solver gmres -gmres_type gmres_r
+        -gmres_pc_type jacobi -gmres_restart `restart`.  Returns
+        (x, nits, residual)."""
+        n = self.sizes()[0]
+        if out is not None:
+            x = out
+        else:
+            x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+        res = C.c_double()
+        nits = _check(lib().phgGpuSolverGMRES(self._h, int(restart), rtol, btol, atol, int(maxit), _ptr(x),
+                                              C.byref(res)))
         return x, nits, res.value
 
 

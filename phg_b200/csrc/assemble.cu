@@ -387,7 +387,7 @@ __device__ __forceinline__ double bdry_rhs(const double *g, int32_t k, int mult)
 }
 
 template <int N, bool PASS2>
-__global__ void __launch_bounds__(WalkCfg<N>::WARPS * 32)
+__global__ void __launch_bounds__(WalkCfg<N>::WARPS * 32, 4)
 row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t *__restrict__ inc,
                 const int32_t *__restrict__ e2l, const uint8_t *__restrict__ bdry,
                 const double *__restrict__ Ke, const uint32_t *__restrict__ Km, const double *__restrict__ Re,
@@ -453,31 +453,49 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
         int L = 0;
         bool overflow = false;
 
-        // prefetched data of incidence ii
-        int32_t col = -1;
-        double v = 0.0;
-        bool nz = false;
-        auto load = [&](int ii, int32_t &c_, double &v_, bool &nz_) {
-            c_ = -1; v_ = 0.0; nz_ = false;
-            if (ii < nwalk && gl < N) {
-                const int32_t kk = inc[i0 + ii];
+        // Incidence keys come G at a time: lane gl of the group holds entry
+        // gl of the current chunk (incA) and of the next one (incB); a key is
+        // read with a shuffle.  The element data of incidence ii + kPf is
+        // loaded while incidence ii is processed; the loaded words are only
+        // inspected when they are used, so the loads stay in flight.
+        auto inc_at = [&](int j) -> int32_t { return j < nwalk ? __ldg(&inc[i0 + j]) : 0; };
+        int32_t incA = inc_at(gl), incB = inc_at(G + gl);
+        struct Pf {
+            int32_t c;
+            double v;       // pass 2: the entry
+            uint32_t m;     // pass 1: the mask word holding the entry's bit
+            int sh;
+            int ok;
+        };
+        auto load = [&](int j, Pf &f) {
+            const int32_t kk = __shfl_sync(0xffffffffu, incA, j % G, G);
+            f.ok = (j < nwalk && gl < N) ? 1 : 0;
+            f.c = -1; f.v = 0.0; f.m = 0u; f.sh = 0;
+            if (f.ok) {
                 const int32_t e = kk / N, a = kk - e * N;
-                c_ = e2l[(size_t)e * N + gl];
+                f.c = e2l[(size_t)e * N + gl];
                 if (PASS2) {
-                    v_ = Ke[((size_t)e * N + a) * N + gl];
-                    nz_ = v_ != 0.0;
+                    f.v = Ke[((size_t)e * N + a) * N + gl];
                 } else {
                     const int bit = a * N + gl;
-                    nz_ = (Km[(size_t)e * MW + (bit >> 5)] >> (bit & 31)) & 1u;
+                    f.m = Km[(size_t)e * MW + (bit >> 5)];
+                    f.sh = bit & 31;
                 }
             }
         };
-        load(0, col, v, nz);
+        constexpr int kPf = 3;   // prefetch distance (incidences)
+        Pf f0, f1, f2;
+        load(0, f0);
+        load(1, f1);
+        load(2, f2);
         for (int ii = 0; ii < maxwalk; ii++) {
-            int32_t ncol;
-            double nv;
-            bool nnz;
-            load(ii + 1, ncol, nv, nnz);
+            const int j = ii + kPf;
+            if (j % G == 0) { incA = incB; incB = inc_at(j + G + gl); }
+            Pf f3;
+            load(j, f3);
+            const int32_t col = f0.c;
+            const double v = f0.v;
+            const bool nz = f0.ok != 0 && (PASS2 ? (v != 0.0) : (((f0.m >> f0.sh) & 1u) != 0u));
             int pos = -1;
             if (nz) {
                 unsigned h = hash32(col) & (HS - 1);
@@ -505,7 +523,7 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
                 sval[pos] = rn_add(sval[pos], v);
             }
             L += __popc(newm);
-            col = ncol; v = nv; nz = nnz;
+            f0 = f1; f1 = f2; f2 = f3;
             __syncwarp();
         }
         const bool bad = overflow || L > MAXROW;

@@ -12,6 +12,7 @@
 // several iterations becomes a no-op after the stopping rule is met.
 #include "common.cuh"
 #include "reduce.cuh"
+#include "spmv_epi.cuh"
 #include "bicgstab.h"
 
 #include <math.h>
@@ -76,11 +77,22 @@ bicg_dir_kernel(int64_t n, const double *__restrict__ rg, const double *__restri
     }
 }
 
-// The two SpMV epilogues: MODE 1 sums w.y (w = rh) and sets alpha; MODE 2
-// sums w.y (w = s) and y.y and sets omega.
-template <int MODE>
-__device__ __forceinline__ void spmv_final(double a, double b, BicgState *st) {
-    if (MODE == 1) {
+// SpMV epilogues (spmv_epi.cuh).  Alpha: v = A p^, sums rh.v and sets
+// alpha = rho / rh.v.  Omega: t = A s^, sums t.s and t.t and sets
+// omega = t.s / t.t.  A zero denominator, where the reference would divide
+// by zero, ends the solve with BICG_BREAKDOWN.
+struct EpiAlpha {
+    double *y;
+    const double *w;
+    double *partials;
+    unsigned *ticket;
+    BicgState *st;
+    __device__ bool skip() const { return st->done != 0; }
+    __device__ void row(int64_t r, double acc, double &sa, double &) const {
+        y[r] = acc;
+        sa += w[r] * acc;
+    }
+    __device__ void final(double a, double) const {
         st->rhv = a;
         if (a == 0.0 || !isfinite(a)) {
             st->done = 1;
@@ -90,7 +102,22 @@ __device__ __forceinline__ void spmv_final(double a, double b, BicgState *st) {
             st->alpha = st->rho1 / a;
             st->rho0 = st->rho1;
         }
-    } else {
+    }
+};
+
+struct EpiOmega {
+    double *y;
+    const double *w;
+    double *partials;
+    unsigned *ticket;
+    BicgState *st;
+    __device__ bool skip() const { return st->done != 0; }
+    __device__ void row(int64_t r, double acc, double &sa, double &sb) const {
+        y[r] = acc;
+        sa += w[r] * acc;
+        sb += acc * acc;
+    }
+    __device__ void final(double a, double b) const {
         if (b == 0.0 || !isfinite(a) || !isfinite(b)) {
             st->done = 1;
             st->status = b == 0.0 ? BICG_BREAKDOWN : BICG_NONFINITE;
@@ -99,79 +126,7 @@ __device__ __forceinline__ void spmv_final(double a, double b, BicgState *st) {
             st->omega = a / b;
         }
     }
-}
-
-template <int MODE, int U>
-__global__ void __launch_bounds__(kThreads)
-bicg_sell_kernel(int64_t nslices, const int32_t *__restrict__ perm, const uint16_t *__restrict__ len,
-                 const int32_t *__restrict__ sptr, const int32_t *__restrict__ cols, const double *__restrict__ vals,
-                 const double *__restrict__ x, double *__restrict__ y, const double *__restrict__ w,
-                 double *partials, BicgState *st) {
-    if (st->done) return;
-    grid_sum_init();
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * kThreads) >> 5;
-    double sa = 0.0, sb = 0.0;
-    for (int64_t s = warp; s < nslices; s += nwarps) {
-        const int64_t pos = s * 32 + lane;
-        const int32_t row = perm[pos];
-        const int l = len[pos];
-        const int wl = __shfl_sync(0xffffffffu, l, 0);
-        const int64_t b = (int64_t)sptr[s] + lane;
-        double acc = 0.0;
-        for (int j = 0; j < wl; j += U) {
-            int32_t c[U];
-            double v[U];
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                const bool ok = j + u < l;
-                c[u] = ok ? __ldcs(&cols[b + 32 * (j + u)]) : 0;
-                v[u] = ok ? __ldcs(&vals[b + 32 * (j + u)]) : 0.0;
-            }
-#pragma unroll
-            for (int u = 0; u < U; u++)
-                if (j + u < l) acc += v[u] * __ldg(&x[c[u]]);
-        }
-        if (row >= 0) {
-            y[row] = acc;
-            sa += w[row] * acc;
-            if (MODE == 2) sb += acc * acc;
-        }
-    }
-    if (grid_sum2(sa, sb, partials, &st->ticket)) spmv_final<MODE>(sa, sb, st);
-}
-
-template <int MODE, int LPR>
-__global__ void __launch_bounds__(kThreads)
-bicg_csr_kernel(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
-                const double *__restrict__ va, const double *__restrict__ x, double *__restrict__ y,
-                const double *__restrict__ w, double *partials, BicgState *st) {
-    if (st->done) return;
-    grid_sum_init();
-    const int lane = threadIdx.x % LPR;
-    constexpr int RPW = 32 / LPR;
-    const int64_t warp = ((int64_t)blockIdx.x * kThreads + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * kThreads) >> 5;
-    const int sub = (threadIdx.x & 31) / LPR;
-    double sa = 0.0, sb = 0.0;
-    for (int64_t base = warp * RPW; base < n; base += nwarps * RPW) {
-        const int64_t row = base + sub;
-        double s = 0.0;
-        if (row < n) {
-            const int32_t b = rp[row], e = rp[row + 1];
-            for (int32_t j = b + lane; j < e; j += LPR) s += va[j] * __ldg(&x[ci[j]]);
-        }
-#pragma unroll
-        for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o, LPR);
-        if (lane == 0 && row < n) {
-            y[row] = s;
-            sa += w[row] * s;
-            if (MODE == 2) sb += s * s;
-        }
-    }
-    if (grid_sum2(sa, sb, partials, &st->ticket)) spmv_final<MODE>(sa, sb, st);
-}
+};
 
 __global__ void __launch_bounds__(kThreads)
 bicg_s_kernel(int64_t n, const double *__restrict__ rg, const double *__restrict__ vg, const double *__restrict__ D,
@@ -270,29 +225,6 @@ __global__ void bicg_small_s_kernel(int64_t n, double *__restrict__ x, const dou
         x[i] = x[i] + al * ph[i];
 }
 
-template <int MODE>
-void spmv(const SpmvPlan &P, const double *x, double *y, const double *w, double *partials, BicgState *st,
-          cudaStream_t s) {
-    if (P.kind == SPMV_CSR) {
-        const CsrView &A = P.csr;
-        const int blocks = sgrid(A.n * P.lpr);
-        switch (P.lpr) {
-        case 4: bicg_csr_kernel<MODE, 4><<<blocks, kThreads, 0, s>>>(A.n, A.rp, A.ci, A.va, x, y, w, partials, st); break;
-        case 8: bicg_csr_kernel<MODE, 8><<<blocks, kThreads, 0, s>>>(A.n, A.rp, A.ci, A.va, x, y, w, partials, st); break;
-        case 16: bicg_csr_kernel<MODE, 16><<<blocks, kThreads, 0, s>>>(A.n, A.rp, A.ci, A.va, x, y, w, partials, st); break;
-        default: bicg_csr_kernel<MODE, 32><<<blocks, kThreads, 0, s>>>(A.n, A.rp, A.ci, A.va, x, y, w, partials, st); break;
-        }
-        return;
-    }
-    const SellView &S = P.sell;
-    const int blocks = sgrid(S.nslices * 32);
-    switch (P.unroll) {
-    case 2: bicg_sell_kernel<MODE, 2><<<blocks, kThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals, x, y, w, partials, st); break;
-    case 8: bicg_sell_kernel<MODE, 8><<<blocks, kThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals, x, y, w, partials, st); break;
-    default: bicg_sell_kernel<MODE, 4><<<blocks, kThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals, x, y, w, partials, st); break;
-    }
-}
-
 }  // namespace
 
 int64_t bicg_stride(int64_t n) { return (n + 31) / 32 * 32; }
@@ -300,9 +232,9 @@ int64_t bicg_stride(int64_t n) { return (n + 31) / 32 * 32; }
 cudaError_t launch_bicg_iteration(const BicgBuffers &B, const SpmvPlan &P, cudaStream_t s) {
     const int vb = vgrid(B.n);
     bicg_dir_kernel<<<vb, kThreads, 0, s>>>(B.n, B.rg, B.vg, B.D, B.pg, B.ph, B.st);
-    spmv<1>(P, B.ph, B.vg, B.rh, B.partials, B.st, s);
+    launch_spmv_epi(P, B.ph, EpiAlpha{B.vg, B.rh, B.partials, &B.st->ticket, B.st}, s);
     bicg_s_kernel<<<vb, kThreads, 0, s>>>(B.n, B.rg, B.vg, B.D, B.sg, B.sh, B.partials, B.st);
-    spmv<2>(P, B.sh, B.tg, B.sg, B.partials, B.st, s);
+    launch_spmv_epi(P, B.sh, EpiOmega{B.tg, B.sg, B.partials, &B.st->ticket, B.st}, s);
     bicg_update_kernel<<<vb, kThreads, 0, s>>>(B.n, B.x, B.ph, B.sh, B.sg, B.tg, B.rg, B.rh, B.partials, B.st,
                                                B.hist);
     return cudaGetLastError();

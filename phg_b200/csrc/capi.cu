@@ -9,6 +9,7 @@
 #include "adjoint.h"
 #include "block.h"
 #include "bicgstab.h"
+#include "gmres.h"
 
 #include <math.h>
 #include <float.h>
@@ -228,6 +229,12 @@ struct phgGpuSystem_ {
     BicgState *h_bst = nullptr;
     cudaGraphExec_t graph_bicg = nullptr;
     GraphKey gkey_bicg{};
+    // GMRES: z and the restart + 2 basis vectors, the small dense arrays, state
+    DevBuf<double> gm_vecs, gm_small;
+    DevBuf<GmresState> gm_st;
+    GmresState *h_gst = nullptr;
+    cudaGraphExec_t graph_gmres = nullptr;
+    GraphKey gkey_gmres{};
 };
 
 namespace {
@@ -504,6 +511,11 @@ int phgGpuDestroy(phgGpuSystem *s) {
     if (s->h_mst) cudaFreeHost(s->h_mst);
     if (s->graph_bicg != nullptr) cudaGraphExecDestroy(s->graph_bicg);
     if (s->h_bst) cudaFreeHost(s->h_bst);
+    if (s->graph_gmres != nullptr) cudaGraphExecDestroy(s->graph_gmres);
+    if (s->h_gst) cudaFreeHost(s->h_gst);
+    s->gm_vecs.release();
+    s->gm_small.release();
+    s->gm_st.release();
     s->bicg_vecs.release();
     s->bicg_st.release();
     DevBuf<float> *fbufs[] = {&s->r32, &s->p32, &s->Ap32, &s->y32, &s->D32, &s->sell_vals32, &s->sell2_vals};
@@ -1193,6 +1205,87 @@ int phgGpuSolverPCG(phgGpuSystem *s, double rtol, double btol, double atol, int 
     if (nits < 0) return nits;
     CHECK_RC(copy_out(s, x, s->x.p, (size_t)n));
     if (hist) CHECK_RC(copy_out(s, hist, dhist, (size_t)nits + 1));
+    CK(cudaStreamSynchronize(s->stream));
+    return nits;
+}
+
+int phgGpuSolverGMRES(phgGpuSystem *s, int restart, double rtol, double btol, double atol, int maxit, double *x,
+                      double *residual) {
+    if (s == nullptr || x == nullptr) return fail(PHG_GPU_ERR_ARG, "invalid arguments");
+    if (!s->assembled) return fail(PHG_GPU_ERR_STATE, "no assembled system");
+    if (maxit < 0) return fail(PHG_GPU_ERR_ARG, "maxit < 0");
+    if (restart < 1 || restart > kGmresMaxRestart)
+        return fail(PHG_GPU_ERR_LIMIT, "phgGpuSolverGMRES: restart must be in 1..%d", kGmresMaxRestart);
+    CHECK_RC(set_device(s));
+    CHECK_RC(solver_buffers(s));
+    const int64_t n = s->n;
+    CHECK_RC(copy_in(s, s->x.p, x, (size_t)n));
+    // ||b|| (solver-phg.c:1071-1075)
+    CK(cudaMemsetAsync(s->ticket.p, 0, sizeof(unsigned), s->stream));
+    CK(launch_init_sums(n, 0, s->x.p, s->rhs.p, s->diag.p, s->partials.p, s->ticket.p, s->sums.p, s->stream));
+    s->launches += 1;
+    CK(cudaMemcpyAsync(s->h_sums, s->sums.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    const double b_norm = sqrt(s->h_sums[1]);
+    if (fabs(b_norm) < 10.0 * DBL_MIN) {
+        CK(cudaMemsetAsync(s->x.p, 0, sizeof(double) * n, s->stream));
+        CHECK_RC(copy_out(s, x, s->x.p, (size_t)n));
+        CK(cudaStreamSynchronize(s->stream));
+        if (residual) *residual = 0.0;
+        return 0;
+    }
+    CHECK_RC(tune_spmv(s));
+    const int64_t stride = bicg_stride(n);
+    CHECK_RC(s->gm_vecs.ensure((size_t)stride * (restart + 3)));
+    CHECK_RC(s->gm_small.ensure((size_t)gmres_small_doubles(restart)));
+    CHECK_RC(s->gm_st.ensure(1));
+    if (s->h_gst == nullptr) CK(cudaMallocHost((void **)&s->h_gst, sizeof(GmresState)));
+    const int R2 = restart + 2;
+    GmresState init{};
+    init.rtol = rtol;
+    init.btol_bnorm = b_norm * btol;
+    init.atol = atol;
+    init.maxit = maxit;
+    init.restart = restart;
+    init.first = 1;
+    init.H = s->gm_small.p;
+    init.c1 = init.H + (size_t)R2 * R2;
+    init.c2 = init.c1 + R2;
+    init.s = init.c2 + R2;
+    init.y = init.s + R2;
+    *s->h_gst = init;
+    CK(cudaMemsetAsync(s->gm_small.p, 0, sizeof(double) * (size_t)gmres_small_doubles(restart), s->stream));
+    CK(cudaMemcpyAsync(s->gm_st.p, s->h_gst, sizeof(GmresState), cudaMemcpyHostToDevice, s->stream));
+
+    GmresBuffers B{n, s->x.p, s->rhs.p, s->diag.p, s->gm_vecs.p, s->gm_vecs.p + stride, stride, s->partials.p,
+                   s->gm_st.p};
+    phgGpuSystem_::GraphKey key{};
+    key.x = B.x; key.r = B.z; key.p = B.V; key.D = B.D; key.Ap = B.st;
+    key.n = n * 100 + restart; key.lpr = s->plan.kind * 100 + s->plan.lpr * 10 + s->plan.unroll; key.s = s->stream;
+    key.va = s->plan.kind == SPMV_CSR ? (const void *)s->va.p : (const void *)s->sell_vals.p;
+    if (s->graph_gmres == nullptr || !(s->gkey_gmres == key)) {
+        if (s->graph_gmres != nullptr) { cudaGraphExecDestroy(s->graph_gmres); s->graph_gmres = nullptr; }
+        cudaGraph_t gr;
+        CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+        launch_gmres_cycle(B, s->plan, restart, s->stream);
+        CK(cudaStreamEndCapture(s->stream, &gr));
+        cudaError_t e = cudaGraphInstantiate(&s->graph_gmres, gr, 0);
+        cudaGraphDestroy(gr);
+        CK(e);
+        s->gkey_gmres = key;
+    }
+    const int per_cycle = 3 + restart * 2 + restart * (restart + 1) / 2;
+    do {
+        CK(cudaGraphLaunch(s->graph_gmres, s->stream));
+        s->launches += per_cycle;
+        CK(cudaMemcpyAsync(s->h_gst, s->gm_st.p, sizeof(GmresState), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+    } while (!s->h_gst->finished);
+    const int nits = s->h_gst->nits;
+    if (residual) *residual = s->h_gst->residual;
+    if (s->h_gst->status == GMRES_NONFINITE)
+        return fail(PHG_GPU_ERR_NAN, "GMRES: non-finite values after %d iterations", nits);
+    CHECK_RC(copy_out(s, x, s->x.p, (size_t)n));
     CK(cudaStreamSynchronize(s->stream));
     return nits;
 }

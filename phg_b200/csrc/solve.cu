@@ -86,21 +86,30 @@ pcg_dir_kernel(int64_t n, const VT *__restrict__ r, const VT *__restrict__ dinv_
         beta = st->rz_cur / st->rz_prev;
     }
     const VT vb = (VT)beta;
-    constexpr int V = Vec16<VT>::V;
-    const int64_t nfull = aligned16(r, dinv_or_d, p) ? n / V : 0;
-    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nfull; c += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = c * V;
-        const VArr<VT> rr = vload_ro(r + i), dd = vload_ro(dinv_or_d + i);
-        VArr<VT> pp;
-        if (k == 1) {
+    constexpr int V = Vec16<VT>::V, UN = 2;   // UN vectors per thread in flight
+    const int nfull = aligned16(r, dinv_or_d, p) ? (int)(n / V) : 0;   // n < 2^31
+    const int stride = gridDim.x * blockDim.x;
+    for (int c0 = blockIdx.x * blockDim.x + threadIdx.x; c0 < nfull; c0 += UN * stride) {
+        VArr<VT> rr[UN], dd[UN], pp[UN];
 #pragma unroll
-            for (int q = 0; q < V; q++) pp.v[q] = rr.v[q] / dd.v[q];
-        } else {
-            pp = vload(p + i);
-#pragma unroll
-            for (int q = 0; q < V; q++) pp.v[q] = vb * pp.v[q] + rr.v[q] / dd.v[q];
+        for (int u = 0; u < UN; u++) {
+            const int c = c0 + u * stride;
+            if (c < nfull) {
+                rr[u] = vload_ro(r + c * V);
+                dd[u] = vload_ro(dinv_or_d + c * V);
+                if (k > 1) pp[u] = vload(p + c * V);
+            }
         }
-        vstore(p + i, pp);
+#pragma unroll
+        for (int u = 0; u < UN; u++) {
+            const int c = c0 + u * stride;
+            if (c < nfull) {
+#pragma unroll
+                for (int q = 0; q < V; q++)
+                    pp[u].v[q] = k == 1 ? rr[u].v[q] / dd[u].v[q] : vb * pp[u].v[q] + rr[u].v[q] / dd[u].v[q];
+                vstore(p + c * V, pp[u]);
+            }
+        }
     }
     for (int64_t i = nfull * V + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -121,24 +130,41 @@ pcg_update_kernel(int64_t n, XT *__restrict__ x, VT *__restrict__ r, const VT *_
     const double alpha = st->alpha;
     const VT va = (VT)alpha;
     double rr = 0.0, rz = 0.0;
-    constexpr int V = Vec16<VT>::V;
-    const int64_t nfull = aligned16(x, r, p, Ap, D) ? n / V : 0;
-    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nfull; c += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = c * V;
-        const VArr<VT> pp = vload_ro(p + i), aa = vload_ro(Ap + i), dd = vload_ro(D + i);
-        VArr<VT> rv = vload(r + i);
-        VArr<XT> xv = vload(x + i);
+    constexpr int V = Vec16<VT>::V, UN = 2;   // UN vectors per thread in flight
+    const int nfull = aligned16(x, r, p, Ap, D) ? (int)(n / V) : 0;   // n < 2^31
+    const int stride = gridDim.x * blockDim.x;
+    for (int c0 = blockIdx.x * blockDim.x + threadIdx.x; c0 < nfull; c0 += UN * stride) {
+        VArr<VT> pp[UN], aa[UN], dd[UN], rv[UN];
+        VArr<XT> xv[UN];
 #pragma unroll
-        for (int q = 0; q < V; q++) {
-            xv.v[q] += (XT)(alpha * (double)pp.v[q]);
-            const VT ri = rv.v[q] - va * aa.v[q];
-            rv.v[q] = ri;
-            const double rd = (double)ri;
-            rr += rd * rd;
-            rz += rd * (double)(ri / dd.v[q]);
+        for (int u = 0; u < UN; u++) {
+            const int c = c0 + u * stride;
+            if (c < nfull) {
+                const int i = c * V;
+                pp[u] = vload_ro(p + i);
+                aa[u] = vload_ro(Ap + i);
+                dd[u] = vload_ro(D + i);
+                rv[u] = vload(r + i);
+                xv[u] = vload(x + i);
+            }
         }
-        vstore(r + i, rv);
-        vstore(x + i, xv);
+#pragma unroll
+        for (int u = 0; u < UN; u++) {
+            const int c = c0 + u * stride;
+            if (c < nfull) {
+#pragma unroll
+                for (int q = 0; q < V; q++) {
+                    xv[u].v[q] += (XT)(alpha * (double)pp[u].v[q]);
+                    const VT ri = rv[u].v[q] - va * aa[u].v[q];
+                    rv[u].v[q] = ri;
+                    const double rd = (double)ri;
+                    rr += rd * rd;
+                    rz += rd * (double)(ri / dd[u].v[q]);
+                }
+                vstore(r + c * V, rv[u]);
+                vstore(x + c * V, xv[u]);
+            }
+        }
     }
     for (int64_t i = nfull * V + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -201,11 +227,12 @@ int vec_blocks(int64_t n) {
     return (int)b;
 }
 
-// Grid of the vectorised element-wise kernels: one 16-byte vector per thread
-// and step, at most 4 blocks per SM (fewer partial sums to combine).
+// Grid of the vectorised element-wise kernels: 16-byte vectors, two per
+// thread and step, at most 3 blocks per SM (all resident at once with up to
+// 80 registers per thread; fewer partial sums to combine).
 static int vvec_blocks(int64_t n, int V) {
-    int64_t b = ceil_div(ceil_div(n, V), kVecThreads);
-    if (b > 148 * 4) b = 148 * 4;
+    int64_t b = ceil_div(ceil_div(n, 2 * V), kVecThreads);
+    if (b > 148 * 3) b = 148 * 3;
     if (b < 1) b = 1;
     return (int)b;
 }
@@ -432,22 +459,39 @@ mixed_update_kernel(int64_t n, float *__restrict__ y, float *__restrict__ r, con
     const float a = (float)st->alpha;
     const bool reset = ms->y_reset != 0;
     double rr = 0.0, rz = 0.0;
-    const int64_t nfull = aligned16(y, r, p, Ap, D) ? n / 4 : 0;
-    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nfull; c += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = c * 4;
-        const VArr<float> pp = vload_ro(p + i), aa = vload_ro(Ap + i), dd = vload_ro(D + i);
-        VArr<float> yv = reset ? VArr<float>{{0.0f, 0.0f, 0.0f, 0.0f}} : vload(y + i);
-        VArr<float> rv = vload(r + i);
+    constexpr int UN = 2;   // vectors per thread in flight
+    const int nfull = aligned16(y, r, p, Ap, D) ? (int)(n / 4) : 0;   // n < 2^31
+    const int stride = gridDim.x * blockDim.x;
+    for (int c0 = blockIdx.x * blockDim.x + threadIdx.x; c0 < nfull; c0 += UN * stride) {
+        VArr<float> pp[UN], aa[UN], dd[UN], yv[UN], rv[UN];
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            yv.v[q] = yv.v[q] + a * pp.v[q];
-            const float ri = rv.v[q] - a * aa.v[q];
-            rv.v[q] = ri;
-            rr += (double)ri * (double)ri;
-            rz += (double)ri * (double)(ri / dd.v[q]);
+        for (int u = 0; u < UN; u++) {
+            const int c = c0 + u * stride;
+            if (c < nfull) {
+                const int i = c * 4;
+                pp[u] = vload_ro(p + i);
+                aa[u] = vload_ro(Ap + i);
+                dd[u] = vload_ro(D + i);
+                yv[u] = reset ? VArr<float>{{0.0f, 0.0f, 0.0f, 0.0f}} : vload(y + i);
+                rv[u] = vload(r + i);
+            }
         }
-        vstore(y + i, yv);
-        vstore(r + i, rv);
+#pragma unroll
+        for (int u = 0; u < UN; u++) {
+            const int c = c0 + u * stride;
+            if (c < nfull) {
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    yv[u].v[q] = yv[u].v[q] + a * pp[u].v[q];
+                    const float ri = rv[u].v[q] - a * aa[u].v[q];
+                    rv[u].v[q] = ri;
+                    rr += (double)ri * (double)ri;
+                    rz += (double)ri * (double)(ri / dd[u].v[q]);
+                }
+                vstore(y + c * 4, yv[u]);
+                vstore(r + c * 4, rv[u]);
+            }
+        }
     }
     for (int64_t i = nfull * 4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {

@@ -3,7 +3,7 @@ reference (PHG 0.9.7) built from its own sources by `make -C oracle ref`.
 
 For every case it writes the mesh as Medit, runs oracle/_ref/phg_dump (the
 reference's element loop + phgSolverAssemble + phgSolverUpdateRHS +
-phgSolverSolve with -solver pcg or bicgstab, see oracle/ref_driver/phg_dump.c) and stores
+phgSolverSolve with -solver pcg, bicgstab or gmres (gmres_r), see oracle/ref_driver/phg_dump.c) and stores
 the reference's own inputs (coordinates, element vertices and element->DOF
 maps as PHG numbered them, f and g at the DOF nodes, Dirichlet flags, kappa)
 and outputs (matrix rows before and after boundary elimination, saved
@@ -46,7 +46,11 @@ CASES = {
     "p1_m6_bicgstab": (6, 1, "sine", None, 1e-10, 0.0, "bicgstab"),
     "p2_m5_kappa_bicgstab": (5, 2, "sine", 12, 1e-10, 0.0, "bicgstab"),
     "p3_m3_mass_bicgstab": (3, 3, "linear", None, 1e-12, 25.0, "bicgstab"),
+    "p1_m6_gmres": (6, 1, "sine", None, 1e-10, 0.0, "gmres_r"),
+    "p2_m5_kappa_gmres": (5, 2, "sine", 12, 1e-10, 0.0, "gmres_r"),
+    "p3_m3_mass_gmres": (3, 3, "linear", None, 1e-12, 25.0, "gmres_r"),
 }
+GMRES_RESTART = 10   # the reference's default (-gmres_restart)
 
 
 def run_case(name, m, P, case, kseed, rtol, mass=0.0, solver="pcg"):
@@ -54,11 +58,14 @@ def run_case(name, m, P, case, kseed, rtol, mass=0.0, solver="pcg"):
         v, e = kuhn_cube(m)
         write_medit(os.path.join(d, "m.mesh"), v, e)
         args = [DUMP, "-mesh_file", os.path.join(d, "m.mesh"), "-dof_type", "P%d" % P,
-                "-solver", solver, "-pcg_pc_type", "jacobi", "-solver_rtol", repr(rtol),
+                "-solver", "gmres" if solver == "gmres_r" else solver, "-pcg_pc_type", "jacobi", "-solver_rtol", repr(rtol),
                 "-solver_btol", "0", "-solver_atol", "0", "-solver_maxit", "10000",
                 "-map_reorder", "no", "-dump_dir", d, "-rhs_case", case]
         if mass != 0.0:
             args += ["-mass_coef", repr(mass)]
+        if solver == "gmres_r":
+            args += ["-gmres_type", "gmres_r", "-gmres_pc_type", "jacobi",
+                     "-gmres_restart", str(GMRES_RESTART)]
         kappa = None
         if kseed is not None:
             kappa = np.exp(np.random.default_rng(kseed).standard_normal(len(e)))
@@ -72,6 +79,7 @@ def run_case(name, m, P, case, kseed, rtol, mass=0.0, solver="pcg"):
         N = int(meta["nbas"])
         out = dict(
             order=P, m=m, rtol=rtol, nits=int(meta["nits"]), mass=float(meta["mass_coef"]), solver=solver,
+            restart=GMRES_RESTART,
             residual=float(meta["residual"]),
             verts=L("verts.f64", np.float64).reshape(-1, 3),
             elems=L("elems.i32", np.int32).reshape(-1, 4),

@@ -51,12 +51,20 @@ def test_golden_assembly_bitexact(gpu, name):
 
 @pytest.mark.parametrize("name", golden_cases())
 def test_golden_solve(gpu, name):
-    """The reference's solver of each golden case (PCG or BiCGstab)."""
+    """The reference's solver of each golden case (PCG, BiCGstab or GMRES)."""
     G = load_golden(name)
     s = build(gpu, int(G["order"]), G["verts"], G["elems"], G["e2l"], G["bdry"], G["f"], G["g"],
               G.get("kappa"), float(G.get("mass", 0.0)))
     rtol = float(G["rtol"])
-    solve = s.solve_bicgstab if ("solver" in G and str(G["solver"]) == "bicgstab") else s.solve_pcg
+    solver = str(G["solver"]) if "solver" in G else "pcg"
+    if solver == "gmres_r":
+        x, nits, res = s.solve_gmres(restart=int(G["restart"]), rtol=rtol, btol=0.0, atol=0.0)
+        assert abs(nits - int(G["nits"])) <= 2
+        ref = G["x"]
+        assert np.linalg.norm(x - ref) <= solution_tol(rtol) * np.linalg.norm(ref)
+        s.close()
+        return
+    solve = s.solve_bicgstab if solver == "bicgstab" else s.solve_pcg
     x, nits, res, hist = solve(rtol=rtol, btol=0.0, atol=0.0, history=True)
     assert abs(nits - int(G["nits"])) <= 2
     ref = G["x"]

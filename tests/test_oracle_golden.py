@@ -36,18 +36,23 @@ def solver_of(G):
 @pytest.mark.parametrize("name", golden_cases())
 def test_solver_bitexact(oracle, name):
     """Iteration count, final residual and solution of the reference's
-    solve_pcg or solver_BiCGstab, bit for bit."""
+    solve_pcg, solver_BiCGstab or solver_GMRES_r, bit for bit."""
     G = load_golden(name)
     args = (G["rows_ptr"], G["rows_cols"], G["rows_vals"], G["diag"], G["rhs"])
     if solver_of(G) == "bicgstab":
         x, nits, res, hist, status = oracle.bicgstab(*args, rtol=float(G["rtol"]), btol=0.0, atol=0.0)
         assert status == 0
+    elif solver_of(G) == "gmres_r":
+        x, nits, res = oracle.gmres(*args, restart=int(G["restart"]), rtol=float(G["rtol"]), btol=0.0,
+                                    atol=0.0)
+        hist = None
     else:
         x, nits, res, hist = oracle.pcg(*args, rtol=float(G["rtol"]), btol=0.0, atol=0.0)
     assert nits == int(G["nits"])
     assert res == float(G["residual"])
     assert np.array_equal(x, G["x"])
-    assert hist[-1] == res and len(hist) == nits + 1
+    if hist is not None:
+        assert hist[-1] == res and len(hist) == nits + 1
 
 
 def test_linear_solution_reproduced():
