@@ -322,7 +322,10 @@ def impl_ours(args):
     # the dominant kernels, timed alone on the launching stream
     spmv32_ms = s.time_spmv(fp32=True, reps=50)
     spmv64_ms = s.time_spmv(fp32=False, reps=50)
-    b32 = 8 * nnz + 4 * (n + 1) + 8 * n
+    # bytes one FP32 product must move: 4-byte values and columns, per row
+    # the slice position's row index (4) and length (2), x and y once (4 + 4)
+    b32 = 8 * nnz + 14 * n
+    b32_csr = 8 * nnz + 4 * (n + 1) + 8 * n     # the same product from int32 CSR
     b64 = 12 * nnz + 4 * (n + 1) + 16 * n
     peak, peak_kind = measured_hbm_peak()
     ach32 = b32 / (spmv32_ms * 1e-3) / 1e9
@@ -339,7 +342,9 @@ def impl_ours(args):
         "roofline": {"bound": "hbm", "kernel": "FP32 SpMV (%s layout, unroll %d)" % (tune.get("fp32_layout"), tune.get("fp32_unroll", 0)),
                      "achieved": round(ach32, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": round(ach32 / peak, 4), "traffic": committed_traffic("spmv32_p2_m64"),
-                     "algorithmic_bytes": int(b32), "launch_ms": round(spmv32_ms, 5)},
+                     "algorithmic_bytes": int(b32), "launch_ms": round(spmv32_ms, 5),
+                     "csr_formula_bytes": int(b32_csr),
+                     "csr_equivalent_gbs": round(b32_csr / (spmv32_ms * 1e-3) / 1e9, 1)},
         "fp64": {"ms": round(ms64, 3), "mixed_over_fp64": round(ms / ms64, 4), "nits": int(nits64),
                  "spmv_ms": round(spmv64_ms, 5), "spmv_gbs": round(ach64, 1),
                  "spmv_frac": round(ach64 / peak, 4), "traffic": committed_traffic("spmv64_p2_m64")},

@@ -216,6 +216,12 @@ int phgGpuSolverPCGMixed(phgGpuSystem *sys, double rtol, double btol,
 int phgGpuGetSpMVPlan(phgGpuSystem *sys, int *kind, int *param,
 		      double *times_ms);
 
+/* Forces the FP32 product layout of the mixed solver for the current matrix
+ * instead of the autotuner's choice (no counterpart in the reference):
+ * layout 0 = SELL (unroll 4/8/16), 1 = pair SELL (unroll 2/4/8).  A new
+ * matrix is tuned again. */
+int phgGpuSetSpMVPlan32(phgGpuSystem *sys, int layout, int unroll);
+
 /* Average device time of one SpMV with the chosen layout, FP64 values
  * (fp32 = 0) or the FP32 values of the mixed solver (fp32 = 1), over `reps`
  * back-to-back launches on the system's stream (no counterpart in the

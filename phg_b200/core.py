@@ -43,6 +43,7 @@ SIGNATURES = {
                                        C.POINTER(C.c_double), _P]),
     "phgGpuSolverGMRES": (C.c_int, [_P, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, _P,
                                     C.POINTER(C.c_double)]),
+    "phgGpuSetSpMVPlan32": (C.c_int, [_P, C.c_int, C.c_int]),
     "phgGpuGetLaunchCount": (C.c_int, [_P, C.POINTER(_I64)]),
     "phgGpuGetSpMVPlan": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), _P]),
     "phgGpuSetSpMVPlan": (C.c_int, [_P, C.c_int, C.c_int]),
@@ -224,6 +225,11 @@ class Solver:
     def set_spmv_plan(self, layout, param):
         _check(lib().phgGpuSetSpMVPlan(self._h, 0 if layout == "csr" else 1, int(param)))
 
+    def set_spmv_plan32(self, layout, unroll):
+        """Forces the mixed solver's FP32 product: layout "sell" or "pair"
+        with the given unroll."""
+        _check(lib().phgGpuSetSpMVPlan32(self._h, ("sell", "pair").index(layout), int(unroll)))
+
     def solve_block_pcg(self, B, rtol=1e-8, maxit=10000, mixed=False, out=None):
         """Block PCG on the columns of B (n x nrhs).  Returns (X, nits[nrhs],
         residuals[nrhs])."""
@@ -260,11 +266,13 @@ class Solver:
         nc = _check(lib().phgGpuGetSpMVPlan(self._h, C.byref(kind), C.byref(param), _ptr(times)))
         names = ["csr4", "csr8", "csr16", "csr32", "sell_u2", "sell_u4", "sell_u8"][:nc]
         info = dict(zip(names, times[:nc].tolist()))
-        for i, name in enumerate(("fp32_sell_u4", "fp32_sell_u8", "fp32_sell_u16", "fp32_pair_u2",
-                                  "fp32_pair_u4", "fp32_pair_u8")):
+        names32 = ("fp32_sell_u4", "fp32_sell_u8", "fp32_sell_u16", "fp32_pair_u2", "fp32_pair_u4",
+                   "fp32_pair_u8")
+        for i, name in enumerate(names32):
             info[name] = float(times[nc + i])
-        info["fp32_unroll"] = int(times[nc + 6])
-        info["fp32_layout"] = "pair" if int(times[nc + 7]) == 1 else "sell"
+        k = nc + len(names32)
+        info["fp32_unroll"] = int(times[k])
+        info["fp32_layout"] = ("sell", "pair")[int(times[k + 1])]
         return ("csr" if kind.value == 0 else "sell"), param.value, info
 
     def launch_count(self):

@@ -125,6 +125,21 @@ struct ElemDims {
 
 constexpr int kGeo = 18;   // doubles of geometry per element: J (16), volume, pad
 
+// Row a of symmetric pair idx = a (a + 1) / 2 + b (b <= a), for N <= 20.
+__device__ const unsigned char g_pair_a[210] = {
+    0, 1, 1, 2, 2, 2, 3, 3, 3, 3, 4, 4, 4, 4, 4, 5, 5, 5, 5, 5, 5,
+    6, 6, 6, 6, 6, 6, 6, 7, 7, 7, 7, 7, 7, 7, 7, 8, 8, 8, 8, 8, 8, 8, 8, 8,
+    9, 9, 9, 9, 9, 9, 9, 9, 9, 9, 10, 10, 10, 10, 10, 10, 10, 10, 10, 10, 10,
+    11, 11, 11, 11, 11, 11, 11, 11, 11, 11, 11, 11, 12, 12, 12, 12, 12, 12, 12, 12, 12, 12, 12, 12, 12,
+    13, 13, 13, 13, 13, 13, 13, 13, 13, 13, 13, 13, 13, 13,
+    14, 14, 14, 14, 14, 14, 14, 14, 14, 14, 14, 14, 14, 14, 14,
+    15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15, 15,
+    16, 16, 16, 16, 16, 16, 16, 16, 16, 16, 16, 16, 16, 16, 16, 16, 16,
+    17, 17, 17, 17, 17, 17, 17, 17, 17, 17, 17, 17, 17, 17, 17, 17, 17, 17,
+    18, 18, 18, 18, 18, 18, 18, 18, 18, 18, 18, 18, 18, 18, 18, 18, 18, 18, 18,
+    19, 19, 19, 19, 19, 19, 19, 19, 19, 19, 19, 19, 19, 19, 19, 19, 19, 19, 19, 19,
+};
+
 // Geometry: one thread per element, J (16) and the volume into geo[e][0..16].
 __global__ void __launch_bounds__(128)
 geometry_kernel(int64_t nelem, int64_t nvert, const double *__restrict__ verts, const int32_t *__restrict__ elems,
@@ -216,11 +231,9 @@ element_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, cons
         }
         __syncwarp();
 
-        // symmetric pairs b <= a
+        // symmetric pairs b <= a (pair idx = a (a + 1) / 2 + b, from a table)
         for (int idx = lane; idx < N * (N + 1) / 2; idx += 32) {
-            int a = (int)((sqrtf(8.0f * idx + 1.0f) - 1.0f) * 0.5f);
-            while (a * (a + 1) / 2 > idx) a--;
-            while ((a + 1) * (a + 2) / 2 <= idx) a++;
+            const int a = __ldg(&g_pair_a[idx]);   // lanes read different entries: L1, not constant cache
             const int b = idx - a * (a + 1) / 2;
             double d = 0.;
 #pragma unroll 4
@@ -250,15 +263,16 @@ element_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, cons
             Re[(size_t)e * N + lane] = rn_mul(d, vol);
         }
         __syncwarp();
+        // store the matrix; word w of the nonzero mask is the ballot of
+        // entries 32w..32w+31 (lane i holds entry 32w + i)
         double *ke = Ke + (size_t)e * N * N;
-        for (int t = lane; t < N * N; t += 32) ke[t] = K[t];
-        if (lane < MW) {
-            uint32_t m = 0;
-            for (int bit = 0; bit < 32; bit++) {
-                const int t = lane * 32 + bit;
-                if (t < N * N && K[t] != 0.0) m |= 1u << bit;
-            }
-            Km[(size_t)e * MW + lane] = m;
+#pragma unroll
+        for (int w = 0; w < MW; w++) {
+            const int t = w * 32 + lane;
+            const double v = t < N * N ? K[t] : 0.0;
+            if (t < N * N) ke[t] = v;
+            const uint32_t m = __ballot_sync(0xffffffffu, v != 0.0);
+            if (lane == 0) Km[(size_t)e * MW + w] = m;
         }
         __syncwarp();
     }

@@ -119,6 +119,7 @@ constexpr int kGraphChunk = 16;
 // SpMV autotuner candidates: CSR with 4/8/16/32 lanes per row, SELL-C-sigma
 // with the inner loop unrolled 2/4/8 times.
 constexpr int kTuneCandidates = 7;
+constexpr int kTune32 = 6;   // FP32 candidates of the mixed solver
 const int kTuneKind[kTuneCandidates] = {SPMV_CSR, SPMV_CSR, SPMV_CSR, SPMV_CSR, SPMV_SELL, SPMV_SELL, SPMV_SELL};
 const int kTuneParam[kTuneCandidates] = {4, 8, 16, 32, 2, 4, 8};
 
@@ -197,7 +198,7 @@ struct phgGpuSystem_ {
     int64_t tuned_n = -1, tuned_nnz = -1;
     int unroll32 = 0;                 // FP32 product unroll (0: not tuned yet)
     int kind32 = 0;                   // FP32 product layout: 0 SELL, 1 pair SELL
-    double tune32_ms[6] = {};
+    double tune32_ms[kTune32] = {};
     bool sell2_valid = false;
     DevBuf<int32_t> sell2_ssz, sell2_sptr, sell2_cols;
     DevBuf<float> sell2_vals;
@@ -384,10 +385,10 @@ int tune_spmv32(phgGpuSystem *s) {
     cudaEvent_t a, b;
     CK(cudaEventCreate(&a));
     CK(cudaEventCreate(&b));
-    const int ckind[6] = {0, 0, 0, 1, 1, 1}, cu[6] = {4, 8, 16, 2, 4, 8};
+    const int ckind[kTune32] = {0, 0, 0, 1, 1, 1}, cu[kTune32] = {4, 8, 16, 2, 4, 8};
     int best = 0;
     const int reps = 5;
-    for (int c = 0; c < 6; c++) {
+    for (int c = 0; c < kTune32; c++) {
         for (int i = 0; i < 2; i++) CK(launch_spmv32k(S, S2, ckind[c], cu[c], s->r32.p, s->Ap32.p, s->stream));
         CK(cudaEventRecord(a, s->stream));
         for (int i = 0; i < reps; i++) CK(launch_spmv32k(S, S2, ckind[c], cu[c], s->r32.p, s->Ap32.p, s->stream));
@@ -941,6 +942,8 @@ int phgGpuTimeSpMV(phgGpuSystem *s, int fp32, int reps, double *ms_per_launch) {
     SpmvPlan P = make_plan(s, s->plan.kind, s->plan.kind == SPMV_CSR ? s->plan.lpr : s->plan.unroll);
     if (fp32) {
         CHECK_RC(tune_spmv32(s));
+        CHECK_RC(s->r32.ensure((size_t)s->n));
+        CHECK_RC(s->Ap32.ensure((size_t)s->n));
         CK(cudaMemsetAsync(s->r32.p, 0, sizeof(float) * s->n, s->stream));
     }
     cudaEvent_t a, b;
@@ -977,6 +980,23 @@ int phgGpuSetSpMVPlan(phgGpuSystem *s, int kind, int param) {
     return PHG_GPU_OK;
 }
 
+int phgGpuSetSpMVPlan32(phgGpuSystem *s, int layout, int unroll) {
+    if (s == nullptr) return fail(PHG_GPU_ERR_ARG, "null system");
+    if (!s->assembled) return fail(PHG_GPU_ERR_STATE, "no assembled system");
+    const bool ok = (layout == 0 && (unroll == 4 || unroll == 8 || unroll == 16)) ||
+                    (layout == 1 && (unroll == 2 || unroll == 4 || unroll == 8));
+    if (!ok) return fail(PHG_GPU_ERR_ARG, "no FP32 SpMV layout (%d, %d)", layout, unroll);
+    CHECK_RC(set_device(s));
+    CHECK_RC(tune_spmv(s));   // FP64 layout for this matrix (returns at once if chosen)
+    CHECK_RC(ensure_sell(s));
+    CHECK_RC(ensure_sell2(s));
+    s->kind32 = layout;
+    s->unroll32 = unroll;
+    s->tuned_n = s->n;
+    s->tuned_nnz = s->nnz;
+    return PHG_GPU_OK;
+}
+
 int phgGpuGetSpMVPlan(phgGpuSystem *s, int *kind, int *param, double *times_ms) {
     if (s == nullptr) return fail(PHG_GPU_ERR_ARG, "null system");
     if (!s->tuned) return fail(PHG_GPU_ERR_STATE, "the SpMV layout is chosen at the first solve or product");
@@ -984,9 +1004,9 @@ int phgGpuGetSpMVPlan(phgGpuSystem *s, int *kind, int *param, double *times_ms) 
     if (param) *param = s->plan.kind == SPMV_CSR ? s->plan.lpr : s->plan.unroll;
     if (times_ms) {
         for (int c = 0; c < kTuneCandidates; c++) times_ms[c] = s->tune_ms[c];
-        for (int c = 0; c < 6; c++) times_ms[kTuneCandidates + c] = s->tune32_ms[c];
-        times_ms[kTuneCandidates + 6] = s->unroll32;
-        times_ms[kTuneCandidates + 7] = s->kind32;
+        for (int c = 0; c < kTune32; c++) times_ms[kTuneCandidates + c] = s->tune32_ms[c];
+        times_ms[kTuneCandidates + kTune32] = s->unroll32;
+        times_ms[kTuneCandidates + kTune32 + 1] = s->kind32;
     }
     return kTuneCandidates;
 }

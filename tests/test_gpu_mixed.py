@@ -87,3 +87,53 @@ def test_mixed_zero_rhs_and_breakdown(gpu):
         s.solve_pcg_mixed(rtol=1e-10)
     assert ei.value.code == -5
     s.close()
+
+
+def far_coupled_spd(n, offsets, seed):
+    """Symmetric, diagonally dominant matrix coupling row i with i +- 1 and
+    i +- o (mod n) for each o in offsets: the rows' columns lie in clusters
+    far apart."""
+    import scipy.sparse as sp
+    rng = np.random.default_rng(seed)
+    i = np.arange(n)
+    rows, cols = [i], [i]
+    vals = [np.full(n, 2.0 + 3 * (1 + len(offsets)))]   # > the largest off-diagonal row sum
+    for o in (1,) + tuple(offsets):
+        w = -0.5 - rng.random(n)
+        rows += [i, (i + o) % n]
+        cols += [(i + o) % n, i]
+        vals += [w, w]
+    A = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(n, n))
+    A.sum_duplicates()
+    A.sort_indices()
+    return A.indptr.astype(np.int64), A.indices.astype(np.int32), A.data, rng.standard_normal(n)
+
+
+LAYOUTS32 = [("sell", 4), ("sell", 8), ("sell", 16), ("pair", 2), ("pair", 4), ("pair", 8)]
+
+
+@pytest.mark.parametrize("case", ["p2_m16", "far_coupled"])
+def test_every_fp32_layout_in_mixed_pcg(gpu, oracle, case):
+    """The mixed solver with each FP32 product layout forced: the FP64
+    residual (recomputed by the oracle) meets the stopping rule and the
+    iteration counts agree within a few iterations (the layouts differ only
+    in the FP32 summation order).  "far_coupled" is a matrix given through
+    phgGpuSetMatrix whose rows couple columns far apart."""
+    if case == "p2_m16":
+        s = system(gpu, 2, 16)
+        ptr, cols, vals = s.get_matrix()
+        rhs = s.get_rhs()
+    else:
+        ptr, cols, vals, rhs = far_coupled_spd(200003, (70001, 140003), seed=5)
+        s = gpu.Solver(0)
+        s.set_matrix(ptr, cols, vals, rhs)
+    its = {}
+    for layout, u in LAYOUTS32:
+        s.set_spmv_plan32(layout, u)
+        x, nits, res, nupd = s.solve_pcg_mixed(rtol=1e-8)
+        r = rhs - oracle.spmv(ptr, cols, vals, x)
+        assert np.linalg.norm(r) <= 1e-8 * np.linalg.norm(rhs) * (1 + 1e-9), (layout, u)
+        its[(layout, u)] = nits
+        assert s.spmv_plan()[2]["fp32_layout"] == layout
+    s.close()
+    assert max(its.values()) - min(its.values()) <= max(3, min(its.values()) // 20), its
