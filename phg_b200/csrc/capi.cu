@@ -200,7 +200,8 @@ struct phgGpuSystem_ {
     int kind32 = 0;                   // FP32 product layout: 0 SELL, 1 pair SELL
     double tune32_ms[kTune32] = {};
     bool sell2_valid = false;
-    DevBuf<int32_t> sell2_ssz, sell2_sptr, sell2_cols;
+    DevBuf<int32_t> sell2_ssz, sell2_sptr, sell2_cols, sell2_order, sell2_perm;
+    DevBuf<uint16_t> sell2_width, sell2_len;
     DevBuf<float> sell2_vals;
     double tune_ms[kTuneCandidates] = {};
 
@@ -350,7 +351,24 @@ int ensure_sell2(phgGpuSystem *s) {
     CHECK_RC(s->scan_ws.ensure((size_t)scan_workspace_elems(nsl)));
     const SellView S{s->n, nsl, s->sell_perm.p, s->sell_len.p, s->sell_sptr.p, s->sell_cols.p, s->sell_vals.p,
                      s->sell_vals32.p};
-    CK(launch_sell2_sizes(S, s->sell2_ssz.p, s->stream));
+    // store the slices widest first: a stable counting sort of the widths
+    CHECK_RC(s->sell2_width.ensure((size_t)nsl));
+    CHECK_RC(s->sell2_order.ensure((size_t)nsl));
+    CK(launch_sell2_heads(S, s->sell2_width.p, s->stream));
+    {
+        std::vector<uint16_t> w((size_t)nsl);
+        std::vector<int32_t> order((size_t)nsl);
+        CK(cudaMemcpyAsync(w.data(), s->sell2_width.p, sizeof(uint16_t) * nsl, cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        std::vector<int64_t> start(65537, 0);
+        for (int64_t i = 0; i < nsl; i++) start[65535 - w[i] + 1]++;
+        for (int b = 1; b <= 65536; b++) start[b] += start[b - 1];
+        for (int64_t i = 0; i < nsl; i++) order[start[65535 - w[i]]++] = (int32_t)i;
+        CK(cudaMemcpyAsync(s->sell2_order.p, order.data(), sizeof(int32_t) * nsl, cudaMemcpyHostToDevice,
+                           s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+    }
+    CK(launch_sell2_sizes(S, s->sell2_order.p, s->sell2_ssz.p, s->stream));
     CK(launch_scan(nsl, s->sell2_ssz.p, s->sell2_sptr.p, s->scan_ws.p, s->stream));
     int32_t total = 0;
     CK(cudaMemcpyAsync(&total, s->sell2_sptr.p + nsl, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
@@ -358,7 +376,10 @@ int ensure_sell2(phgGpuSystem *s) {
     if (total < 0) return fail(PHG_GPU_ERR_LIMIT, "pair SELL layout larger than 2^31 entries");
     CHECK_RC(s->sell2_cols.ensure((size_t)total));
     CHECK_RC(s->sell2_vals.ensure((size_t)total));
-    CK(launch_sell2_fill(S, s->rp.p, s->ci.p, s->va.p, s->sell2_sptr.p, s->sell2_cols.p, s->sell2_vals.p, s->stream));
+    CHECK_RC(s->sell2_perm.ensure((size_t)nsl * 32));
+    CHECK_RC(s->sell2_len.ensure((size_t)nsl * 32));
+    CK(launch_sell2_fill(S, s->rp.p, s->ci.p, s->va.p, s->sell2_order.p, s->sell2_sptr.p, s->sell2_perm.p,
+                         s->sell2_len.p, s->sell2_cols.p, s->sell2_vals.p, s->stream));
     s->launches += 5;
     s->sell2_valid = true;
     return PHG_GPU_OK;
@@ -369,7 +390,9 @@ SellView sell_view(phgGpuSystem *s) {
                     s->sell_cols.p, s->sell_vals.p, s->sell_vals32.p};
 }
 
-Sell2View sell2_view(phgGpuSystem *s) { return Sell2View{s->sell2_sptr.p, s->sell2_cols.p, s->sell2_vals.p}; }
+Sell2View sell2_view(phgGpuSystem *s) {
+    return Sell2View{s->sell2_sptr.p, s->sell2_cols.p, s->sell2_vals.p, s->sell2_perm.p, s->sell2_len.p};
+}
 
 // Layout and unroll of the FP32 product (mixed solver), timed once per
 // matrix shape: SELL unrolled 4/8/16, pair SELL unrolled 2/4/8.
@@ -521,6 +544,7 @@ int phgGpuDestroy(phgGpuSystem *s) {
     s->bicg_st.release();
     DevBuf<float> *fbufs[] = {&s->r32, &s->p32, &s->Ap32, &s->y32, &s->D32, &s->sell_vals32, &s->sell2_vals};
     s->sell2_ssz.release(); s->sell2_sptr.release(); s->sell2_cols.release();
+    s->sell2_order.release(); s->sell2_perm.release(); s->sell2_width.release(); s->sell2_len.release();
     for (auto *b : fbufs) b->release();
     s->sell_perm.release(); s->sell_ssz.release(); s->sell_sptr.release(); s->sell_cols.release();
     s->sell_len.release(); s->sell_vals.release(); s->mst.release();

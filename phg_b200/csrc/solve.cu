@@ -640,20 +640,33 @@ cudaError_t launch_mixed_iteration(const MixedBuffers &B, const SellView &S, int
 // FP32 values in "pair" SELL: the same slices as SELL-C-sigma, but each lane
 // keeps two consecutive entries of its row side by side, so a warp moves
 // 256 bytes of values and 256 bytes of column indices per load instruction
-// (float2 / int2).  Slice s holds ceil(w_s / 2) pairs of 64 entries.
-__global__ void sell2_sizes_kernel(int64_t nslices, const uint16_t *__restrict__ len, int32_t *__restrict__ size) {
+// (float2 / int2).  Slice s holds ceil(w_s / 2) pairs of 64 entries.  The
+// slices are stored widest first (order[k] = SELL slice stored k-th): warps
+// take slices k, k + nwarps, ..., so every warp gets a similar share of the
+// work and no long slices are left for the end of the launch.
+__global__ void sell2_heads_kernel(int64_t nslices, const uint16_t *__restrict__ len, uint16_t *__restrict__ width) {
     for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < nslices; s += (int64_t)gridDim.x * blockDim.x)
-        size[s] = 64 * ((len[s * 32] + 1) / 2);
+        width[s] = len[s * 32];   // rows are sorted by length: position 0 is the slice's widest
+}
+
+__global__ void sell2_sizes_kernel(int64_t nslices, const uint16_t *__restrict__ len, const int32_t *__restrict__ order,
+                                   int32_t *__restrict__ size) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nslices; k += (int64_t)gridDim.x * blockDim.x)
+        size[k] = 64 * ((len[(int64_t)order[k] * 32] + 1) / 2);
 }
 
 __global__ void sell2_fill_kernel(int64_t npos, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
                                   const double *__restrict__ va, const int32_t *__restrict__ perm,
-                                  const uint16_t *__restrict__ len, const int32_t *__restrict__ sptr2,
-                                  int32_t *__restrict__ cols2, float *__restrict__ vals2) {
+                                  const uint16_t *__restrict__ len, const int32_t *__restrict__ order,
+                                  const int32_t *__restrict__ sptr2, int32_t *__restrict__ perm2,
+                                  uint16_t *__restrict__ len2, int32_t *__restrict__ cols2, float *__restrict__ vals2) {
     for (int64_t pos = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pos < npos;
          pos += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t row = perm[pos];
-        const int l = len[pos];
+        const int64_t src = (int64_t)order[pos >> 5] * 32 + (pos & 31);
+        const int32_t row = perm[src];
+        const int l = len[src];
+        perm2[pos] = row;
+        len2[pos] = (uint16_t)l;
         const int64_t b = (int64_t)sptr2[pos >> 5] + 2 * (pos & 31);
         const int32_t r0 = row >= 0 ? rp[row] : 0;
         const int lp = (l + 1) & ~1;
@@ -725,15 +738,22 @@ sell2_spmv_kernel(int64_t nslices, const int32_t *__restrict__ perm, const uint1
     }
 }
 
-cudaError_t launch_sell2_sizes(const SellView &S, int32_t *sizes, cudaStream_t s) {
-    sell2_sizes_kernel<<<vec_blocks(S.nslices), kVecThreads, 0, s>>>(S.nslices, S.len, sizes);
+cudaError_t launch_sell2_heads(const SellView &S, uint16_t *width, cudaStream_t s) {
+    sell2_heads_kernel<<<vec_blocks(S.nslices), kVecThreads, 0, s>>>(S.nslices, S.len, width);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sell2_sizes(const SellView &S, const int32_t *order, int32_t *sizes, cudaStream_t s) {
+    sell2_sizes_kernel<<<vec_blocks(S.nslices), kVecThreads, 0, s>>>(S.nslices, S.len, order, sizes);
     return cudaGetLastError();
 }
 
 cudaError_t launch_sell2_fill(const SellView &S, const int32_t *rp, const int32_t *ci, const double *va,
-                              const int32_t *sptr2, int32_t *cols2, float *vals2, cudaStream_t s) {
+                              const int32_t *order, const int32_t *sptr2, int32_t *perm2, uint16_t *len2,
+                              int32_t *cols2, float *vals2, cudaStream_t s) {
     const int64_t npos = S.nslices * 32;
-    sell2_fill_kernel<<<vec_blocks(npos), kVecThreads, 0, s>>>(npos, rp, ci, va, S.perm, S.len, sptr2, cols2, vals2);
+    sell2_fill_kernel<<<vec_blocks(npos), kVecThreads, 0, s>>>(npos, rp, ci, va, S.perm, S.len, order, sptr2, perm2,
+                                                               len2, cols2, vals2);
     return cudaGetLastError();
 }
 
@@ -751,9 +771,9 @@ static void spmv32_dispatch(const SellView &S, const Sell2View &S2, int kind, in
         }
     } else {
         switch (u) {
-        case 2: sell2_spmv_kernel<DOT, 2><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S2.sptr2, S2.cols2, S2.vals2, x, y, partials, st); break;
-        case 8: sell2_spmv_kernel<DOT, 8><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S2.sptr2, S2.cols2, S2.vals2, x, y, partials, st); break;
-        default: sell2_spmv_kernel<DOT, 4><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S2.sptr2, S2.cols2, S2.vals2, x, y, partials, st); break;
+        case 2: sell2_spmv_kernel<DOT, 2><<<sb, kVecThreads, 0, s>>>(S.nslices, S2.perm2, S2.len2, S2.sptr2, S2.cols2, S2.vals2, x, y, partials, st); break;
+        case 8: sell2_spmv_kernel<DOT, 8><<<sb, kVecThreads, 0, s>>>(S.nslices, S2.perm2, S2.len2, S2.sptr2, S2.cols2, S2.vals2, x, y, partials, st); break;
+        default: sell2_spmv_kernel<DOT, 4><<<sb, kVecThreads, 0, s>>>(S.nslices, S2.perm2, S2.len2, S2.sptr2, S2.cols2, S2.vals2, x, y, partials, st); break;
         }
     }
 }

@@ -46,9 +46,11 @@ struct SellView {
 
 // FP32 pair layout of the same slices (see solve.cu).
 struct Sell2View {
-    const int32_t *sptr2;     // slice offsets in entries (nslices + 1)
+    const int32_t *sptr2;     // slice offsets in entries (nslices + 1), slices stored widest first
     const int32_t *cols2;
     const float *vals2;
+    const int32_t *perm2;     // row of each position in the stored slice order
+    const uint16_t *len2;     // its length
 };
 
 struct SpmvPlan {
@@ -77,9 +79,11 @@ struct MixedBuffers {
 int vec_blocks(int64_t n);
 cudaError_t launch_mixed_init(int64_t n, const double *rtrue, float *r32, float *y, const double *D64, float *D32,
                               double *partials, unsigned *ticket, double *out, cudaStream_t s);
-cudaError_t launch_sell2_sizes(const SellView &S, int32_t *sizes, cudaStream_t s);
+cudaError_t launch_sell2_heads(const SellView &S, uint16_t *width, cudaStream_t s);
+cudaError_t launch_sell2_sizes(const SellView &S, const int32_t *order, int32_t *sizes, cudaStream_t s);
 cudaError_t launch_sell2_fill(const SellView &S, const int32_t *rp, const int32_t *ci, const double *va,
-                              const int32_t *sptr2, int32_t *cols2, float *vals2, cudaStream_t s);
+                              const int32_t *order, const int32_t *sptr2, int32_t *perm2, uint16_t *len2,
+                              int32_t *cols2, float *vals2, cudaStream_t s);
 cudaError_t launch_spmv32k(const SellView &S, const Sell2View &S2, int kind, int u, const float *x, float *y,
                            cudaStream_t s);
 cudaError_t launch_mixed_iteration2(const MixedBuffers &B, const SellView &S, const Sell2View &S2, int kind, int u,
