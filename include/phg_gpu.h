@@ -95,6 +95,18 @@ int phgGpuBuildLinearSystemMass(phgGpuSystem *sys, const double *kappa,
 				double mass_coef, const double *f,
 				const double *g);
 
+/* The element loop's integrals alone: Ke[e][a][b] (nelem x N x N) is what
+ * phgQuadGradBasAGradBas(e, u, b, kappa, u, a, QUAD_DEFAULT) returns (plus
+ * mass_coef * phgQuadBasDotBas when mass_coef != 0; src/quad.c:5260-5344,
+ * 5582-5625) and Re[e][a] (nelem x N) what phgQuadDofTimesBas(e, f_h, u, a,
+ * QUAD_DEFAULT, &r) returns (src/quad.c:5481-5530), bit for bit, for every
+ * element at once.  Needs phgGpuSetMesh and phgGpuSetDofMap (the map locates
+ * f's values); Ke or Re may be NULL.  Serves per-element shims of those
+ * calls (phg_b200/shim). */
+int phgGpuElementMatrices(phgGpuSystem *sys, const double *kappa,
+			  double mass_coef, const double *f, double *Ke,
+			  double *Re);
+
 /* Installs an already-assembled matrix instead (the rows PHG hands an OEM
  * solver, src/solver.c:223-285): CSR with int64 row pointers (PHG's
  * size_t packed_ind), int32 columns, and the right-hand side. */

@@ -44,6 +44,7 @@ SIGNATURES = {
     "phgGpuSolverGMRES": (C.c_int, [_P, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, _P,
                                     C.POINTER(C.c_double)]),
     "phgGpuSetSpMVPlan32": (C.c_int, [_P, C.c_int, C.c_int]),
+    "phgGpuElementMatrices": (C.c_int, [_P, _P, C.c_double, _P, _P, _P]),
     "phgGpuGetLaunchCount": (C.c_int, [_P, C.POINTER(_I64)]),
     "phgGpuGetSpMVPlan": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), _P]),
     "phgGpuSetSpMVPlan": (C.c_int, [_P, C.c_int, C.c_int]),
@@ -150,6 +151,7 @@ class Solver:
 
     def set_dof_map(self, order, e2l, bdry):
         e2l, bdry = _np(e2l, np.int32), _np(bdry, np.uint8)
+        self.nbas = {1: 4, 2: 10, 3: 20}.get(int(order), 0)
         _check(lib().phgGpuSetDofMap(self._h, int(order), len(bdry), _ptr(e2l), _ptr(bdry)))
 
     def build_linear_system(self, kappa=None, f=None, g=None, mass=0.0):
@@ -160,6 +162,16 @@ class Solver:
             _check(lib().phgGpuBuildLinearSystemMass(self._h, _ptr(kappa), float(mass), _ptr(f), _ptr(g)))
         else:
             _check(lib().phgGpuBuildLinearSystem(self._h, _ptr(kappa), _ptr(f), _ptr(g)))
+
+    def element_matrices(self, kappa=None, f=None, mass=0.0):
+        """Element matrices (nelem, N, N) and right-hand sides (nelem, N)."""
+        n_el = self.nelem
+        N = self.nbas
+        kappa, f = _np(kappa, np.float64), _np(f, np.float64)
+        Ke = np.empty((n_el, N, N))
+        Re = np.empty((n_el, N))
+        _check(lib().phgGpuElementMatrices(self._h, _ptr(kappa), float(mass), _ptr(f), _ptr(Ke), _ptr(Re)))
+        return Ke, Re
 
     def set_matrix(self, ptr, cols, vals, rhs):
         ptr, cols = _np(ptr, np.int64), _np(cols, np.int32)

@@ -646,22 +646,18 @@ int phgGpuSetDofMap(phgGpuSystem *s, int order, int64_t ndof, const int32_t *e2l
     return PHG_GPU_OK;
 }
 
-static int build_system(phgGpuSystem *s, const double *kappa, double mass, const double *f, const double *g) {
-    if (s == nullptr) return fail(PHG_GPU_ERR_ARG, "null system");
-    if (!s->have_dofs) return fail(PHG_GPU_ERR_STATE, "phgGpuBuildLinearSystem: call phgGpuSetDofMap first");
-    if (!isfinite(mass)) return fail(PHG_GPU_ERR_ARG, "phgGpuBuildLinearSystemMass: mass coefficient not finite");
-    CHECK_RC(set_device(s));
+// Element matrices, right-hand sides and nonzero masks of every element
+// (the element loop's phgQuad* calls) into s->Ke, s->Re, s->Km.
+static int element_pass(phgGpuSystem *s, const double *kappa, double mass, const double *f) {
     const int N = s->N;
     const int64_t ndof = s->ndof;
-    const double *dk, *df, *dg;
+    const double *dk, *df;
     CHECK_RC(stage(s, kappa, (size_t)s->nelem, s->kappa, &dk));
     CHECK_RC(stage(s, f, (size_t)ndof, s->f, &df));
-    CHECK_RC(stage(s, g, (size_t)ndof, s->g, &dg));
     CHECK_RC(s->Ke.ensure((size_t)s->nelem * N * N));
     CHECK_RC(s->Re.ensure((size_t)s->nelem * N));
     CHECK_RC(s->Km.ensure((size_t)s->nelem * element_mask_words(s->order)));
     CHECK_RC(s->geo.ensure((size_t)geometry_doubles(s->nelem)));
-
     ElemArgs ea{};
     ea.nelem = s->nelem; ea.nvert = s->nvert; ea.ndof = ndof;
     ea.verts = s->verts.p; ea.elems = s->elems.p; ea.e2l = s->e2l.p;
@@ -670,6 +666,18 @@ static int build_system(phgGpuSystem *s, const double *kappa, double mass, const
     ea.Ke = s->Ke.p; ea.Re = s->Re.p; ea.Km = s->Km.p; ea.geo = s->geo.p; ea.status = s->status.p;
     CK(launch_element_kernel(s->order, ea, s->stream));
     s->launches += 2;
+    return PHG_GPU_OK;
+}
+
+static int build_system(phgGpuSystem *s, const double *kappa, double mass, const double *f, const double *g) {
+    if (s == nullptr) return fail(PHG_GPU_ERR_ARG, "null system");
+    if (!s->have_dofs) return fail(PHG_GPU_ERR_STATE, "phgGpuBuildLinearSystem: call phgGpuSetDofMap first");
+    if (!isfinite(mass)) return fail(PHG_GPU_ERR_ARG, "phgGpuBuildLinearSystemMass: mass coefficient not finite");
+    CHECK_RC(set_device(s));
+    const int64_t ndof = s->ndof;
+    const double *dg;
+    CHECK_RC(stage(s, g, (size_t)ndof, s->g, &dg));
+    CHECK_RC(element_pass(s, kappa, mass, f));
 
     CHECK_RC(s->cnt_keep.ensure((size_t)ndof));
     CHECK_RC(s->cnt_bdry.ensure((size_t)ndof));
@@ -714,6 +722,21 @@ static int build_system(phgGpuSystem *s, const double *kappa, double mass, const
 
 int phgGpuBuildLinearSystem(phgGpuSystem *s, const double *kappa, const double *f, const double *g) {
     return build_system(s, kappa, 0.0, f, g);
+}
+
+int phgGpuElementMatrices(phgGpuSystem *s, const double *kappa, double mass_coef, const double *f, double *Ke,
+                          double *Re) {
+    if (s == nullptr) return fail(PHG_GPU_ERR_ARG, "null system");
+    if (!s->have_dofs) return fail(PHG_GPU_ERR_STATE, "phgGpuElementMatrices: call phgGpuSetDofMap first");
+    if (!isfinite(mass_coef)) return fail(PHG_GPU_ERR_ARG, "phgGpuElementMatrices: mass coefficient not finite");
+    CHECK_RC(set_device(s));
+    CHECK_RC(element_pass(s, kappa, mass_coef, f));
+    CHECK_RC(check_status(s, "phgGpuElementMatrices"));
+    const size_t N = (size_t)s->N;
+    if (Ke != nullptr) CHECK_RC(copy_out(s, Ke, s->Ke.p, (size_t)s->nelem * N * N));
+    if (Re != nullptr) CHECK_RC(copy_out(s, Re, s->Re.p, (size_t)s->nelem * N));
+    CK(cudaStreamSynchronize(s->stream));
+    return PHG_GPU_OK;
 }
 
 int phgGpuBuildLinearSystemMass(phgGpuSystem *s, const double *kappa, double mass_coef, const double *f,
