@@ -112,14 +112,11 @@ __device__ __forceinline__ void jacobian_vol(const double *x, double *J, double 
 //   Re[e]   N right-hand side entries, integral of f_h phi_a with the order-2p
 //           rule (phgQuadDofTimesBas, quad.c:5481-5530; f_h at the points as
 //           phgDofEval_, dof-utils.c:59-300)
-//   Km[e]   bit (a*N + b) set iff Ke[e][a][b] != 0 (the entries the reference's
-//           phgMatAddEntries_ keeps), read by the first row-walk pass
 template <int P>
 struct ElemDims {
     static constexpr int N = P == 1 ? 4 : P == 2 ? 10 : 20;
     static constexpr int QK = P == 1 ? 1 : P == 2 ? 4 : 14;
     static constexpr int QR = P == 1 ? 4 : P == 2 ? 14 : 24;
-    static constexpr int MW = (N * N + 31) / 32;          // mask words per element
     static constexpr int WARPS = 4;                       // warps per block
 };
 
@@ -176,9 +173,9 @@ element_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, cons
                const double *__restrict__ kappa, const double mass, const double *__restrict__ f,
                const double *__restrict__ wk, const double *__restrict__ gk,
                const double *__restrict__ wr, const double *__restrict__ br,
-               double *__restrict__ Ke, double *__restrict__ Re, uint32_t *__restrict__ Km, int *status) {
+               double *__restrict__ Ke, double *__restrict__ Re, int *status) {
     using D = ElemDims<P>;
-    constexpr int N = D::N, QK = D::QK, QR = D::QR, MW = D::MW, W = D::WARPS;
+    constexpr int N = D::N, QK = D::QK, QR = D::QR, W = D::WARPS;
     __shared__ double s_geo[W][kGeo + 1];       // J (16), volume, kappa
     __shared__ double s_grad[W][N * QK * 3];
     __shared__ double s_K[W][N * N];
@@ -263,17 +260,8 @@ element_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, cons
             Re[(size_t)e * N + lane] = rn_mul(d, vol);
         }
         __syncwarp();
-        // store the matrix; word w of the nonzero mask is the ballot of
-        // entries 32w..32w+31 (lane i holds entry 32w + i)
         double *ke = Ke + (size_t)e * N * N;
-#pragma unroll
-        for (int w = 0; w < MW; w++) {
-            const int t = w * 32 + lane;
-            const double v = t < N * N ? K[t] : 0.0;
-            if (t < N * N) ke[t] = v;
-            const uint32_t m = __ballot_sync(0xffffffffu, v != 0.0);
-            if (lane == 0) Km[(size_t)e * MW + w] = m;
-        }
+        for (int t = lane; t < N * N; t += 32) ke[t] = K[t];
         __syncwarp();
     }
 }
@@ -367,24 +355,28 @@ __global__ void scan_add_kernel(int64_t n, int32_t *__restrict__ out, const int6
 }
 
 // ---------------------------------------------------------------------------
-// Row walk: G lanes per row (G >= N; 32/G rows per warp side by side).  For an
-// interior row the lane group visits the row's incidences in element order;
-// lane j handles element column j, skips exact zeros (phgMatAddEntries_,
-// matvec.c:5459-5461), finds or appends the column (add_columns_to_row,
-// matvec.c:3286-3321: first-touch order) through the group's open-addressing
-// table in shared memory, and (pass 2) accumulates the value.  Boundary
-// columns are then separated from the row as save_bdry_columns does
+// Row walk: G lanes per row (G >= N; 32/G rows per warp side by side), one
+// pass.  For an interior row the lane group visits the row's incidences in
+// element order; lane j handles element column j, skips exact zeros
+// (phgMatAddEntries_, matvec.c:5459-5461), finds or appends the column
+// (add_columns_to_row, matvec.c:3286-3321: first-touch order) through the
+// group's open-addressing table in shared memory, and accumulates the value.
+// Boundary columns are then separated from the row as save_bdry_columns does
 // (matvec.c:4430-4488) and lifted into the RHS as update_rhs does
 // (solver.c:707-725).  A Dirichlet row is the sum of the unit rows of its
-// elements (phgDofDirichletBC, dof-utils.c:1369-1392).  The next incidence's
-// loads are issued before the current one is processed.
+// elements (phgDofDirichletBC, dof-utils.c:1369-1392).
+//
+// The row's entries go to a scratch region sized by the row's incidences
+// (incidences x N slots, at inc_ptr[d] * N; the row cannot be longer):
+// kept entries from the front in first-touch order, saved boundary columns
+// from the back in reverse.  The counts are scanned into the CSR row
+// pointers and compact_kernel copies the regions into the CSR arrays.
 template <int N>
 struct WalkCfg {
     static constexpr int G = N <= 8 ? 8 : N <= 16 ? 16 : 32;   // lanes per row
     static constexpr int R = 32 / G;                            // rows per warp
     static constexpr int HS = N == 4 ? 128 : N == 10 ? 256 : 512;
     static constexpr int MAXROW = HS / 2;
-    static constexpr int MW = (N * N + 31) / 32;
     static constexpr int WARPS = 4;
 };
 
@@ -400,22 +392,20 @@ __device__ __forceinline__ double bdry_rhs(const double *g, int32_t k, int mult)
     return s;
 }
 
-template <int N, bool PASS2>
+template <int N>
 __global__ void __launch_bounds__(WalkCfg<N>::WARPS * 32, 4)
 row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t *__restrict__ inc,
                 const int32_t *__restrict__ e2l, const uint8_t *__restrict__ bdry,
-                const double *__restrict__ Ke, const uint32_t *__restrict__ Km, const double *__restrict__ Re,
-                const double *__restrict__ g,
+                const double *__restrict__ Ke, const double *__restrict__ Re, const double *__restrict__ g,
                 int32_t *__restrict__ cnt_keep, int32_t *__restrict__ cnt_bdry,
-                const int32_t *__restrict__ ptr, int32_t *__restrict__ cols, double *__restrict__ vals,
-                const int32_t *__restrict__ bptr, int32_t *__restrict__ bcols, double *__restrict__ bvals,
+                int32_t *__restrict__ sc_cols, double *__restrict__ sc_vals,
                 double *__restrict__ rhs, double *__restrict__ diag, int *status) {
     using C = WalkCfg<N>;
-    constexpr int G = C::G, R = C::R, HS = C::HS, MAXROW = C::MAXROW, MW = C::MW, W = C::WARPS;
+    constexpr int G = C::G, R = C::R, HS = C::HS, MAXROW = C::MAXROW, W = C::WARPS;
     __shared__ int32_t s_key[W][R][HS];
     __shared__ int16_t s_pos[W][R][HS];
-    __shared__ int32_t s_col[W][R][PASS2 ? MAXROW : 1];
-    __shared__ double s_val[W][R][PASS2 ? MAXROW : 1];
+    __shared__ int32_t s_col[W][R][MAXROW];
+    __shared__ double s_val[W][R][MAXROW];
 
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int grp = lane / G, gl = lane % G;
@@ -437,23 +427,22 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
             i1 = inc_ptr[d + 1];
             isb = bdry[d] != 0;
         }
+        // the scratch region of row d
+        const int64_t rbase = (int64_t)i0 * N, rcap = (int64_t)(i1 - i0) * N;
         if (active && isb && gl == 0) {
             const int mult = i1 - i0;
-            if (!PASS2) {
-                cnt_keep[d] = mult > 0 ? 1 : 0;
-                cnt_bdry[d] = mult > 0 ? 1 : 0;
-            } else {
-                double m = 0.0;
-                for (int i = 0; i < mult; i++) m = rn_add(m, 1.0);
-                if (mult > 0) {
-                    cols[ptr[d]] = (int32_t)d;
-                    vals[ptr[d]] = m;
-                    bcols[bptr[d]] = (int32_t)d;
-                    bvals[bptr[d]] = m;
-                }
-                diag[d] = m;
-                rhs[d] = bdry_rhs(g, (int32_t)d, mult);
+            double m = 0.0;
+            for (int i = 0; i < mult; i++) m = rn_add(m, 1.0);
+            if (mult > 0) {
+                sc_cols[rbase] = (int32_t)d;
+                sc_vals[rbase] = m;
+                sc_cols[rbase + rcap - 1] = (int32_t)d;
+                sc_vals[rbase + rcap - 1] = m;
             }
+            cnt_keep[d] = mult > 0 ? 1 : 0;
+            cnt_bdry[d] = mult > 0 ? 1 : 0;
+            diag[d] = m;
+            rhs[d] = bdry_rhs(g, (int32_t)d, mult);
         }
         const bool walk = active && !isb;
         const int nwalk = walk ? i1 - i0 : 0;
@@ -469,32 +458,25 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
 
         // Incidence keys come G at a time: lane gl of the group holds entry
         // gl of the current chunk (incA) and of the next one (incB); a key is
-        // read with a shuffle.  The element data of incidence ii + kPf is
-        // loaded while incidence ii is processed; the loaded words are only
+        // read with a shuffle.  The element data of incidence ii + 3 is loaded
+        // while incidence ii is processed; the loaded words are only
         // inspected when they are used, so the loads stay in flight.
         auto inc_at = [&](int j) -> int32_t { return j < nwalk ? __ldg(&inc[i0 + j]) : 0; };
         int32_t incA = inc_at(gl), incB = inc_at(G + gl);
         struct Pf {
             int32_t c;
-            double v;       // pass 2: the entry
-            uint32_t m;     // pass 1: the mask word holding the entry's bit
-            int sh;
+            double v;
             int ok;
         };
         auto load = [&](int j, Pf &f) {
             const int32_t kk = __shfl_sync(0xffffffffu, incA, j % G, G);
             f.ok = (j < nwalk && gl < N) ? 1 : 0;
-            f.c = -1; f.v = 0.0; f.m = 0u; f.sh = 0;
+            f.c = -1;
+            f.v = 0.0;
             if (f.ok) {
                 const int32_t e = kk / N, a = kk - e * N;
                 f.c = e2l[(size_t)e * N + gl];
-                if (PASS2) {
-                    f.v = Ke[((size_t)e * N + a) * N + gl];
-                } else {
-                    const int bit = a * N + gl;
-                    f.m = Km[(size_t)e * MW + (bit >> 5)];
-                    f.sh = bit & 31;
-                }
+                f.v = Ke[((size_t)e * N + a) * N + gl];
             }
         };
         constexpr int kPf = 3;   // prefetch distance (incidences)
@@ -509,7 +491,7 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
             load(j, f3);
             const int32_t col = f0.c;
             const double v = f0.v;
-            const bool nz = f0.ok != 0 && (PASS2 ? (v != 0.0) : (((f0.m >> f0.sh) & 1u) != 0u));
+            const bool nz = f0.ok != 0 && v != 0.0;
             int pos = -1;
             if (nz) {
                 unsigned h = hash32(col) & (HS - 1);
@@ -529,11 +511,12 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
                         if (atomicCAS(&key[h], -1, col) == -1) { hpos[h] = (int16_t)pos; break; }
                         h = (h + 1) & (HS - 1);
                     }
-                    if (PASS2) { scol[pos] = col; sval[pos] = v; }
+                    scol[pos] = col;
+                    sval[pos] = v;
                 } else {
                     overflow = true;
                 }
-            } else if (nz && PASS2) {
+            } else if (nz) {
                 sval[pos] = rn_add(sval[pos], v);
             }
             L += __popc(newm);
@@ -544,31 +527,11 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
         const unsigned badm = __ballot_sync(0xffffffffu, bad) & gmask;
         if (badm != 0 && gl == 0) atomicExch(status, PHGB_DEV_ROW_OVERFLOW);
 
-        if (!PASS2) {
-            int nk = 0, nb = 0;
-            if (walk && badm == 0)
-                for (int t = gl; t < HS; t += G) {
-                    const int32_t c = key[t];
-                    if (c < 0) continue;
-                    if (c != d && bdry[c]) nb++; else nk++;
-                }
-#pragma unroll
-            for (int o = G / 2; o > 0; o >>= 1) {
-                nk += __shfl_xor_sync(0xffffffffu, nk, o, G);
-                nb += __shfl_xor_sync(0xffffffffu, nb, o, G);
-            }
-            if (walk && badm == 0 && gl == 0) { cnt_keep[d] = nk; cnt_bdry[d] = nb; }
-            __syncwarp();
-            continue;
-        }
-
-        // pass 2: emit kept columns and saved boundary columns, in order.
-        // Lanes also evaluate, in parallel, the lift term of each boundary
-        // column (rhs_k * a_dk / D_kk, solver.c:716-724); it replaces the
-        // column's value in s_val once the value has been emitted.
+        // emit kept columns (front) and saved boundary columns (back, reversed),
+        // in first-touch order.  Lanes also evaluate, in parallel, the lift
+        // term of each boundary column (rhs_k * a_dk / D_kk, solver.c:716-724);
+        // it replaces the column's value in s_val once the value is emitted.
         const bool emit = walk && badm == 0;
-        int32_t p0 = 0, b0 = 0;
-        if (emit) { p0 = ptr[d]; b0 = bptr[d]; }
         int nk = 0, nb = 0;
         double dg = 0.0;
         int maxL = emit ? L : 0;
@@ -599,14 +562,14 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
             const unsigned km = __ballot_sync(0xffffffffu, valid && !isbc) & gmask;
             const unsigned bm = __ballot_sync(0xffffffffu, valid && isbc) & gmask;
             if (valid && !isbc) {
-                const int r = nk + __popc(km & lt_mask);
-                cols[p0 + r] = c;
-                vals[p0 + r] = val;
+                const int64_t q = rbase + nk + __popc(km & lt_mask);
+                sc_cols[q] = c;
+                sc_vals[q] = val;
             }
             if (valid && isbc) {
-                const int r = nb + __popc(bm & lt_mask);
-                bcols[b0 + r] = c;
-                bvals[b0 + r] = val;
+                const int64_t q = rbase + rcap - 1 - (nb + __popc(bm & lt_mask));
+                sc_cols[q] = c;
+                sc_vals[q] = val;
             }
             nk += __popc(km);
             nb += __popc(bm);
@@ -627,7 +590,8 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
         }
         __syncwarp();
         if (emit && gl == 0) {
-            if (p0 + nk != ptr[d + 1] || b0 + nb != bptr[d + 1]) atomicExch(status, PHGB_DEV_COUNT_MISMATCH);
+            cnt_keep[d] = nk;
+            cnt_bdry[d] = nb;
             diag[d] = dg;
             // lift the boundary columns in first-touch order: r -= term
             for (int t = 0; t < L; t++)
@@ -635,6 +599,31 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
             rhs[d] = r;
         }
         __syncwarp();
+    }
+}
+
+// Copies every row's scratch region into the CSR arrays: kept entries to
+// ptr[d].., saved boundary columns (stored reversed at the region's end) to
+// bptr[d]...  One warp per row.
+__global__ void __launch_bounds__(256)
+compact_kernel(int64_t ndof, int N, const int32_t *__restrict__ inc_ptr, const int32_t *__restrict__ sc_cols,
+               const double *__restrict__ sc_vals, const int32_t *__restrict__ ptr, int32_t *__restrict__ cols,
+               double *__restrict__ vals, const int32_t *__restrict__ bptr, int32_t *__restrict__ bcols,
+               double *__restrict__ bvals) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t d = warp; d < ndof; d += nwarps) {
+        const int64_t rbase = (int64_t)inc_ptr[d] * N, rcap = (int64_t)(inc_ptr[d + 1] - inc_ptr[d]) * N;
+        const int32_t p0 = ptr[d], nk = ptr[d + 1] - p0, b0 = bptr[d], nb = bptr[d + 1] - b0;
+        for (int j = lane; j < nk; j += 32) {
+            cols[p0 + j] = sc_cols[rbase + j];
+            vals[p0 + j] = sc_vals[rbase + j];
+        }
+        for (int j = lane; j < nb; j += 32) {
+            bcols[b0 + j] = sc_cols[rbase + rcap - 1 - j];
+            bvals[b0 + j] = sc_vals[rbase + rcap - 1 - j];
+        }
     }
 }
 
@@ -655,7 +644,7 @@ static void elem_launch(const ElemArgs &A, cudaStream_t s) {
                                                                     A.status);
     const int blocks = grid_for(A.nelem, W, 148 * 64);
     element_kernel<P><<<blocks, W * 32, 0, s>>>(A.nelem, A.ndof, A.geo, A.e2l, A.kappa, A.mass, A.f, A.wk, A.gk, A.wr,
-                                                A.br, A.Ke, A.Re, A.Km, A.status);
+                                                A.br, A.Ke, A.Re, A.status);
 }
 
 cudaError_t launch_element_kernel(int p, const ElemArgs &A, cudaStream_t s) {
@@ -667,7 +656,6 @@ cudaError_t launch_element_kernel(int p, const ElemArgs &A, cudaStream_t s) {
 
 int64_t geometry_doubles(int64_t nelem) { return nelem * kGeo; }
 
-int element_mask_words(int p) { return p == 1 ? ElemDims<1>::MW : p == 2 ? ElemDims<2>::MW : ElemDims<3>::MW; }
 
 cudaError_t launch_incidence(int N, int64_t nelem, int64_t ndof, const int32_t *e2l, int32_t *cnt,
                              int32_t *inc_ptr, int32_t *cursor, int32_t *inc, int64_t *scan_ws,
@@ -697,24 +685,26 @@ cudaError_t launch_scan(int64_t n, const int32_t *in, int32_t *out, int64_t *ws,
 }
 
 template <int N>
-static cudaError_t walk(bool pass2, const WalkArgs &A, cudaStream_t s) {
+static cudaError_t walk(const WalkArgs &A, cudaStream_t s) {
     constexpr int W = WalkCfg<N>::WARPS, R = WalkCfg<N>::R;
     const int blocks = grid_for(ceil_div(A.ndof, R), W, 148 * 32);
-    if (!pass2)
-        row_walk_kernel<N, false><<<blocks, W * 32, 0, s>>>(
-            A.ndof, A.inc_ptr, A.inc, A.e2l, A.bdry, A.Ke, A.Km, A.Re, A.g, A.cnt_keep, A.cnt_bdry,
-            nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, A.status);
-    else
-        row_walk_kernel<N, true><<<blocks, W * 32, 0, s>>>(
-            A.ndof, A.inc_ptr, A.inc, A.e2l, A.bdry, A.Ke, A.Km, A.Re, A.g, nullptr, nullptr, A.ptr,
-            A.cols, A.vals, A.bptr, A.bcols, A.bvals, A.rhs, A.diag, A.status);
+    row_walk_kernel<N><<<blocks, W * 32, 0, s>>>(A.ndof, A.inc_ptr, A.inc, A.e2l, A.bdry, A.Ke, A.Re, A.g,
+                                                 A.cnt_keep, A.cnt_bdry, A.sc_cols, A.sc_vals, A.rhs, A.diag,
+                                                 A.status);
     return cudaGetLastError();
 }
 
-cudaError_t launch_row_walk(int p, bool pass2, const WalkArgs &A, cudaStream_t s) {
-    if (p == 1) return walk<4>(pass2, A, s);
-    if (p == 2) return walk<10>(pass2, A, s);
-    return walk<20>(pass2, A, s);
+cudaError_t launch_row_walk(int p, const WalkArgs &A, cudaStream_t s) {
+    if (p == 1) return walk<4>(A, s);
+    if (p == 2) return walk<10>(A, s);
+    return walk<20>(A, s);
+}
+
+cudaError_t launch_compact(int N, const WalkArgs &A, cudaStream_t s) {
+    compact_kernel<<<grid_for(A.ndof * 32, 256, 148 * 16), 256, 0, s>>>(A.ndof, N, A.inc_ptr, A.sc_cols, A.sc_vals,
+                                                                      A.ptr, A.cols, A.vals, A.bptr, A.bcols,
+                                                                      A.bvals);
+    return cudaGetLastError();
 }
 
 int row_walk_max_row(int p) { return p == 1 ? WalkCfg<4>::MAXROW : p == 2 ? WalkCfg<10>::MAXROW : WalkCfg<20>::MAXROW; }

@@ -14,7 +14,6 @@ struct ElemArgs {
     const double *wk, *gk, *wr, *br;         // element tables
     double *geo;                             // scratch: nelem * geometry_doubles
     double *Ke, *Re;
-    uint32_t *Km;
     int *status;
 };
 
@@ -23,9 +22,10 @@ struct WalkArgs {
     const int32_t *inc_ptr, *inc, *e2l;
     const uint8_t *bdry;
     const double *Ke, *Re, *g;
-    const uint32_t *Km;
-    int32_t *cnt_keep, *cnt_bdry;            // pass 1
-    const int32_t *ptr, *bptr;               // pass 2
+    int32_t *cnt_keep, *cnt_bdry;            // entries kept / saved per row
+    int32_t *sc_cols;                        // scratch: nelem * N * N entries
+    double *sc_vals;
+    const int32_t *ptr, *bptr;               // compaction: CSR row pointers
     int32_t *cols, *bcols;
     double *vals, *bvals, *rhs, *diag;
     int *status;
@@ -38,9 +38,11 @@ cudaError_t launch_incidence(int N, int64_t nelem, int64_t ndof, const int32_t *
 int64_t scan_workspace_elems(int64_t n);
 // out[0..n] = exclusive prefix sums of in[0..n-1], out[n] = total (int32).
 cudaError_t launch_scan(int64_t n, const int32_t *in, int32_t *out, int64_t *ws, cudaStream_t s);
-cudaError_t launch_row_walk(int p, bool pass2, const WalkArgs &a, cudaStream_t s);
+// One pass over the rows into the scratch regions (counts, RHS, diagonal),
+// then, after the counts are scanned into ptr/bptr, the copy into the CSR.
+cudaError_t launch_row_walk(int p, const WalkArgs &a, cudaStream_t s);
+cudaError_t launch_compact(int N, const WalkArgs &a, cudaStream_t s);
 int row_walk_max_row(int p);
-int element_mask_words(int p);
 int64_t geometry_doubles(int64_t nelem);
 
 }  // namespace phgb

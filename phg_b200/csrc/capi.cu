@@ -155,7 +155,8 @@ struct phgGpuSystem_ {
 
     // assembly buffers
     DevBuf<double> Ke, Re, kappa, f, g, geo;
-    DevBuf<uint32_t> Km;
+    DevBuf<int32_t> sc_cols;          // row-walk scratch (nelem * N * N entries)
+    DevBuf<double> sc_vals;
     DevBuf<int32_t> cnt_keep, cnt_bdry;
 
     // assembled system
@@ -564,7 +565,8 @@ int phgGpuDestroy(phgGpuSystem *s) {
                                 &s->cnt_bdry, &s->rp, &s->ci, &s->brp, &s->bci};
     for (auto *b : ibufs) b->release();
     s->bdry.release();
-    s->Km.release();
+    s->sc_cols.release();
+    s->sc_vals.release();
     s->scan_ws.release();
     s->tmp64.release();
     s->st.release();
@@ -647,7 +649,7 @@ int phgGpuSetDofMap(phgGpuSystem *s, int order, int64_t ndof, const int32_t *e2l
 }
 
 // Element matrices, right-hand sides and nonzero masks of every element
-// (the element loop's phgQuad* calls) into s->Ke, s->Re, s->Km.
+// (the element loop's phgQuad* calls) into s->Ke, s->Re.
 static int element_pass(phgGpuSystem *s, const double *kappa, double mass, const double *f) {
     const int N = s->N;
     const int64_t ndof = s->ndof;
@@ -656,14 +658,13 @@ static int element_pass(phgGpuSystem *s, const double *kappa, double mass, const
     CHECK_RC(stage(s, f, (size_t)ndof, s->f, &df));
     CHECK_RC(s->Ke.ensure((size_t)s->nelem * N * N));
     CHECK_RC(s->Re.ensure((size_t)s->nelem * N));
-    CHECK_RC(s->Km.ensure((size_t)s->nelem * element_mask_words(s->order)));
     CHECK_RC(s->geo.ensure((size_t)geometry_doubles(s->nelem)));
     ElemArgs ea{};
     ea.nelem = s->nelem; ea.nvert = s->nvert; ea.ndof = ndof;
     ea.verts = s->verts.p; ea.elems = s->elems.p; ea.e2l = s->e2l.p;
     ea.kappa = dk; ea.f = df; ea.mass = mass;
     ea.wk = s->wk.p; ea.gk = s->gk.p; ea.wr = s->wr.p; ea.br = s->br.p;
-    ea.Ke = s->Ke.p; ea.Re = s->Re.p; ea.Km = s->Km.p; ea.geo = s->geo.p; ea.status = s->status.p;
+    ea.Ke = s->Ke.p; ea.Re = s->Re.p; ea.geo = s->geo.p; ea.status = s->status.p;
     CK(launch_element_kernel(s->order, ea, s->stream));
     s->launches += 2;
     return PHG_GPU_OK;
@@ -683,18 +684,25 @@ static int build_system(phgGpuSystem *s, const double *kappa, double mass, const
     CHECK_RC(s->cnt_bdry.ensure((size_t)ndof));
     CHECK_RC(s->rp.ensure((size_t)ndof + 1));
     CHECK_RC(s->brp.ensure((size_t)ndof + 1));
+    CHECK_RC(s->rhs.ensure((size_t)ndof));
+    CHECK_RC(s->diag.ensure((size_t)ndof));
+    const size_t nscratch = (size_t)s->nelem * s->N * s->N;   // every row fits in its incidences x N slots
+    CHECK_RC(s->sc_cols.ensure(nscratch));
+    CHECK_RC(s->sc_vals.ensure(nscratch));
     WalkArgs wa{};
     wa.ndof = ndof; wa.inc_ptr = s->inc_ptr.p; wa.inc = s->inc.p; wa.e2l = s->e2l.p; wa.bdry = s->bdry.p;
-    wa.Ke = s->Ke.p; wa.Re = s->Re.p; wa.g = dg; wa.Km = s->Km.p;
+    wa.Ke = s->Ke.p; wa.Re = s->Re.p; wa.g = dg;
     wa.cnt_keep = s->cnt_keep.p; wa.cnt_bdry = s->cnt_bdry.p; wa.status = s->status.p;
-    CK(launch_row_walk(s->order, false, wa, s->stream));
-    s->launches += 7;   // pass 1 + two scans
+    wa.sc_cols = s->sc_cols.p; wa.sc_vals = s->sc_vals.p;
+    wa.rhs = s->rhs.p; wa.diag = s->diag.p;
+    CK(launch_row_walk(s->order, wa, s->stream));
+    s->launches += 7;   // walk + two scans
     CK(launch_scan(ndof, s->cnt_keep.p, s->rp.p, s->scan_ws.p, s->stream));
     int32_t tot[2];
     CK(cudaMemcpyAsync(&tot[0], s->rp.p + ndof, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
     CK(launch_scan(ndof, s->cnt_bdry.p, s->brp.p, s->scan_ws.p, s->stream));
     CK(cudaMemcpyAsync(&tot[1], s->brp.p + ndof, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
-    CHECK_RC(check_status(s, "phgGpuBuildLinearSystem (count)"));
+    CHECK_RC(check_status(s, "phgGpuBuildLinearSystem (rows)"));
     if (tot[0] < 0 || tot[1] < 0) return fail(PHG_GPU_ERR_LIMIT, "matrix has more than 2^31 entries");
     s->nnz = tot[0];
     s->bnnz = tot[1];
@@ -702,12 +710,9 @@ static int build_system(phgGpuSystem *s, const double *kappa, double mass, const
     CHECK_RC(s->va.ensure((size_t)s->nnz));
     CHECK_RC(s->bci.ensure((size_t)s->bnnz));
     CHECK_RC(s->bva.ensure((size_t)s->bnnz));
-    CHECK_RC(s->rhs.ensure((size_t)ndof));
-    CHECK_RC(s->diag.ensure((size_t)ndof));
     wa.ptr = s->rp.p; wa.cols = s->ci.p; wa.vals = s->va.p;
     wa.bptr = s->brp.p; wa.bcols = s->bci.p; wa.bvals = s->bva.p;
-    wa.rhs = s->rhs.p; wa.diag = s->diag.p;
-    CK(launch_row_walk(s->order, true, wa, s->stream));
+    CK(launch_compact(s->N, wa, s->stream));
     s->launches += 1;
     CHECK_RC(check_status(s, "phgGpuBuildLinearSystem"));
     s->n = ndof;
