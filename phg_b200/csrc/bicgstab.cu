@@ -156,7 +156,7 @@ bicg_s_kernel(int64_t n, const double *__restrict__ rg, const double *__restrict
         sh[i] = sv / D[i];
         ss += sv * sv;
     }
-    if (grid_sum2(ss, dummy, partials, &st->ticket)) {
+    if (grid_sum2(ss, dummy, partials, st->ticket)) {
         const double s = sqrt(ss);
         st->snorm = s;
         if (s <= 1e-60) {   // solver-phg.c:717-729; the host finishes the step
@@ -202,7 +202,7 @@ bicg_update_kernel(int64_t n, double *__restrict__ x, double *__restrict__ ph, c
         rr += r * r;
         rrh += r * rh[i];
     }
-    if (grid_sum2(rr, rrh, partials, &st->ticket)) {
+    if (grid_sum2(rr, rrh, partials, st->ticket)) {
         const int k = st->nits + 1;
         const double res = sqrt(rr);
         st->residual = res;
@@ -232,9 +232,9 @@ int64_t bicg_stride(int64_t n) { return (n + 31) / 32 * 32; }
 cudaError_t launch_bicg_iteration(const BicgBuffers &B, const SpmvPlan &P, cudaStream_t s) {
     const int vb = vgrid(B.n);
     bicg_dir_kernel<<<vb, kThreads, 0, s>>>(B.n, B.rg, B.vg, B.D, B.pg, B.ph, B.st);
-    launch_spmv_epi(P, B.ph, EpiAlpha{B.vg, B.rh, B.partials, &B.st->ticket, B.st}, s);
+    launch_spmv_epi(P, B.ph, EpiAlpha{B.vg, B.rh, B.partials, B.st->ticket, B.st}, s);
     bicg_s_kernel<<<vb, kThreads, 0, s>>>(B.n, B.rg, B.vg, B.D, B.sg, B.sh, B.partials, B.st);
-    launch_spmv_epi(P, B.sh, EpiOmega{B.tg, B.sg, B.partials, &B.st->ticket, B.st}, s);
+    launch_spmv_epi(P, B.sh, EpiOmega{B.tg, B.sg, B.partials, B.st->ticket, B.st}, s);
     bicg_update_kernel<<<vb, kThreads, 0, s>>>(B.n, B.x, B.ph, B.sh, B.sg, B.tg, B.rg, B.rh, B.partials, B.st,
                                                B.hist);
     return cudaGetLastError();

@@ -9,7 +9,7 @@ namespace phgb {
 struct BicgState {
     double rho0, rho1, alpha, omega, rhv, residual, tol, snorm;
     int nits, done, status, maxit;
-    unsigned ticket;
+    unsigned ticket[kRedTickets];
     int pad;
 };
 

@@ -313,7 +313,7 @@ int solver_buffers(phgGpuSystem *s) {
     CHECK_RC(s->partials.ensure(2 * (size_t)vec_blocks((int64_t)n * 32) + 64));
     CHECK_RC(s->sums.ensure(2));
     CHECK_RC(s->st.ensure(1));
-    CHECK_RC(s->ticket.ensure(1));
+    CHECK_RC(s->ticket.ensure(kRedTickets));
     return PHG_GPU_OK;
 }
 
@@ -878,7 +878,7 @@ int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol,
     CHECK_RC(s->mst.ensure(1));
     if (s->h_mst == nullptr) CK(cudaMallocHost((void **)&s->h_mst, sizeof(MixedState)));
     CHECK_RC(copy_in(s, s->x.p, x, un));
-    CK(cudaMemsetAsync(s->ticket.p, 0, sizeof(unsigned), s->stream));
+    CK(cudaMemsetAsync(s->ticket.p, 0, sizeof(unsigned) * kRedTickets, s->stream));
     const SpmvPlan P = make_plan(s, s->plan.kind, s->plan.kind == SPMV_CSR ? s->plan.lpr : s->plan.unroll);
     CHECK_RC(tune_spmv32(s));
     const int unroll = s->unroll32;
@@ -1079,7 +1079,7 @@ namespace {
 int pcg_core(phgGpuSystem *s, const double *drhs, double rtol, double btol, double atol, int maxit,
              double *dhist, double *residual) {
     const int64_t n = s->n;
-    CK(cudaMemsetAsync(s->ticket.p, 0, sizeof(unsigned), s->stream));
+    CK(cudaMemsetAsync(s->ticket.p, 0, sizeof(unsigned) * kRedTickets, s->stream));
     // ||b|| and |x|_1 (solver-phg.c:498-518)
     CK(launch_init_sums(n, 0, s->x.p, drhs, s->diag.p, s->partials.p, s->ticket.p, s->sums.p, s->stream));
     s->launches += 1;
@@ -1160,7 +1160,7 @@ int bicg_core(phgGpuSystem *s, double rtol, double btol, double atol, int maxit,
               double *residual) {
     const int64_t n = s->n;
     const double *drhs = s->rhs.p;
-    CK(cudaMemsetAsync(s->ticket.p, 0, sizeof(unsigned), s->stream));
+    CK(cudaMemsetAsync(s->ticket.p, 0, sizeof(unsigned) * kRedTickets, s->stream));
     CK(launch_init_sums(n, 0, s->x.p, drhs, s->diag.p, s->partials.p, s->ticket.p, s->sums.p, s->stream));
     s->launches += 1;
     CK(cudaMemcpyAsync(s->h_sums, s->sums.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
@@ -1293,7 +1293,7 @@ int phgGpuSolverGMRES(phgGpuSystem *s, int restart, double rtol, double btol, do
     const int64_t n = s->n;
     CHECK_RC(copy_in(s, s->x.p, x, (size_t)n));
     // ||b|| (solver-phg.c:1071-1075)
-    CK(cudaMemsetAsync(s->ticket.p, 0, sizeof(unsigned), s->stream));
+    CK(cudaMemsetAsync(s->ticket.p, 0, sizeof(unsigned) * kRedTickets, s->stream));
     CK(launch_init_sums(n, 0, s->x.p, s->rhs.p, s->diag.p, s->partials.p, s->ticket.p, s->sums.p, s->stream));
     s->launches += 1;
     CK(cudaMemcpyAsync(s->h_sums, s->sums.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));

@@ -129,7 +129,7 @@ gmres_mgs_kernel(int64_t n, int i, int k, double *__restrict__ w, const double *
         w[l] = v;
         sa += v * (last ? v : vk[l]);
     }
-    if (!grid_sum2(sa, dummy, partials, &st->ticket)) return;
+    if (!grid_sum2(sa, dummy, partials, st->ticket)) return;
     if (!last) {
         Hat(st, i, k) = sa;
         return;
@@ -215,10 +215,10 @@ cudaError_t launch_gmres_cycle(const GmresBuffers &B, const SpmvPlan &P, int res
     const int vb = vgrid(n);
     double *V0 = B.V;
     auto Vi = [&](int i) { return B.V + (int64_t)i * B.stride; };
-    launch_spmv_epi(P, B.x, EpiResid{B.z, B.b, B.partials, &B.st->ticket, B.st}, s);
+    launch_spmv_epi(P, B.x, EpiResid{B.z, B.b, B.partials, B.st->ticket, B.st}, s);
     for (int i = 1; i <= restart; i++) {
         gmres_pc_kernel<<<vb, kThreads, 0, s>>>(n, i, i == 1 ? B.z : Vi(i), Vi(i), V0, B.D, B.st);
-        launch_spmv_epi(P, V0, EpiArnoldi{Vi(i + 1), Vi(1), B.partials, &B.st->ticket, B.st, i}, s);
+        launch_spmv_epi(P, V0, EpiArnoldi{Vi(i + 1), Vi(1), B.partials, B.st->ticket, B.st, i}, s);
         for (int k = 2; k <= i + 1; k++)
             gmres_mgs_kernel<<<vb, kThreads, 0, s>>>(n, i, k, Vi(i + 1), Vi(k - 1), k <= i ? Vi(k) : nullptr,
                                                      B.partials, B.st);

@@ -15,7 +15,7 @@ struct GmresState {
     double r_norm, tol, residual, rtol, btol_bnorm, atol;
     int nits, maxit, restart, ninner;
     int run, cycle_done, finished, first, status;
-    unsigned ticket;
+    unsigned ticket[kRedTickets];
     double *H, *c1, *c2, *s, *y;
 };
 

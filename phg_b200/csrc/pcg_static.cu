@@ -44,7 +44,7 @@ constexpr size_t kOffPartials = kOffRp + align_up(sizeof(int32_t) * (kMaxRows + 
 constexpr size_t kOffSums = kOffPartials + align_up(sizeof(double) * (2 * kMaxBlocks + 64));
 constexpr size_t kOffState = kOffSums + align_up(sizeof(double) * 2);
 constexpr size_t kOffTicket = kOffState + align_up(sizeof(phgb::PcgState));
-constexpr size_t kStaticScratchBytes = kOffTicket + align_up(sizeof(unsigned));
+constexpr size_t kStaticScratchBytes = kOffTicket + align_up(sizeof(unsigned) * phgb::kRedTickets);
 
 // The scratch memory.  In host code this name is only a stand-in for the
 // symbol, not a device address; the device address comes from
@@ -151,7 +151,7 @@ int solve(int64_t n, const int64_t *ptr, const int32_t *cols, const double *vals
         return fail(PHG_GPU_ERR_ARG, "phgGpuSolverPCGNoAlloc: bad row pointers");
 
     // the array keeps the previous call's contents: reset what must start at 0
-    CKS(cudaMemsetAsync(ticket, 0, sizeof(unsigned), s));
+    CKS(cudaMemsetAsync(ticket, 0, sizeof(unsigned) * phgb::kRedTickets, s));
     narrow_rows_kernel<<<vec_blocks(n + 1), 256, 0, s>>>(n + 1, ptr, rp);
     diagonal_kernel<<<vec_blocks(n), 256, 0, s>>>(n, rp, cols, vals, D);
     CKS(cudaGetLastError());

@@ -2,16 +2,26 @@
 // sums with a deterministic combination order, and 16-byte vector loads.
 #pragma once
 #include "common.cuh"
+#include "solve.h"
 
 namespace phgb {
 
 // Grid-wide sum of two values without block barriers: each warp reduces its
 // values (fixed butterfly), the last warp of a block to arrive adds the
-// block's warp sums in warp order and publishes them, and the last block to
-// arrive adds the block sums in block order.  Nobody waits: a warp that is
-// not last simply leaves.  Returns true in exactly one thread (lane 0 of the
-// final warp), which then holds the totals.  Kernels call grid_sum_init()
-// once, before any early exit that is not uniform across the block.
+// block's warp sums in warp order and publishes them; the last block of each
+// group of kRedGroup consecutive blocks adds the group's block sums, and the
+// last group adds the group sums.  Each stage is one round of loads issued
+// together, so the finishing block waits for two L2 round trips however large
+// the grid is (one warp summing 1184 block sums one after another took ~14 us
+// per launch; the two-stage tree ~5 us).  The combination order is fixed for
+// a given grid, so results are reproducible.  Nobody waits: a warp that is not
+// last simply leaves.  Returns true in exactly one thread (lane 0 of the final
+// warp), which then holds the totals.  Kernels call grid_sum_init() once,
+// before any early exit that is not uniform across the block.
+//
+// Workspace: partials holds 2 * (gridDim.x + ceil(gridDim.x / kRedGroup))
+// doubles at a 16-byte aligned address; tickets holds kRedTickets counters,
+// zero before the first launch (every stage resets its own counter).
 struct RedShared {
     double a[32], b[32];
     unsigned cnt;
@@ -27,7 +37,7 @@ __device__ __forceinline__ void grid_sum_init() {
     __syncthreads();
 }
 
-__device__ __forceinline__ bool grid_sum2(double &a, double &b, double *partials, unsigned *ticket) {
+__device__ __forceinline__ bool grid_sum2(double &a, double &b, double *partials, unsigned *tickets) {
     RedShared &R = red_smem();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     a = warp_sum(a);
@@ -46,34 +56,39 @@ __device__ __forceinline__ bool grid_sum2(double &a, double &b, double *partials
     double tb = lane < nw ? ((volatile double *)R.b)[lane] : 0.0;
     ta = warp_sum(ta);
     tb = warp_sum(tb);
+    // stage 1: block sums -> group sums
+    double2 *P = reinterpret_cast<double2 *>(partials);
+    const unsigned nb = gridDim.x, g = blockIdx.x / kRedGroup, g0 = g * kRedGroup;
+    const unsigned gs = min((unsigned)kRedGroup, nb - g0), ng = (nb + kRedGroup - 1) / kRedGroup;
     if (lane == 0) {
-        partials[2 * blockIdx.x] = ta;
-        partials[2 * blockIdx.x + 1] = tb;
+        P[blockIdx.x] = make_double2(ta, tb);
         __threadfence();
-        arrived = atomicAdd(ticket, 1u);
+        arrived = atomicAdd(&tickets[1 + g], 1u);
     }
     arrived = __shfl_sync(0xffffffffu, arrived, 0);
-    if (arrived != gridDim.x - 1) return false;
+    if (arrived != gs - 1) return false;
     __threadfence();
-    // four independent accumulators per lane keep several loads in flight;
-    // they are combined in a fixed order
-    double sa[4] = {0.0, 0.0, 0.0, 0.0}, sb[4] = {0.0, 0.0, 0.0, 0.0};
-    for (unsigned i0 = 0; i0 < gridDim.x; i0 += 128) {
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const unsigned i = i0 + q * 32 + lane;
-            if (i < gridDim.x) {
-                sa[q] += __ldcg(&partials[2 * i]);
-                sb[q] += __ldcg(&partials[2 * i + 1]);
-            }
-        }
-    }
-    double ta2 = warp_sum((sa[0] + sa[1]) + (sa[2] + sa[3]));
-    double tb2 = warp_sum((sb[0] + sb[1]) + (sb[2] + sb[3]));
+    double2 p0 = lane < gs ? __ldcg(&P[g0 + lane]) : make_double2(0.0, 0.0);
+    double2 p1 = lane + 32 < gs ? __ldcg(&P[g0 + lane + 32]) : make_double2(0.0, 0.0);
+    ta = warp_sum(p0.x + p1.x);
+    tb = warp_sum(p0.y + p1.y);
     if (lane == 0) {
-        a = ta2;
-        b = tb2;
-        *ticket = 0u;
+        tickets[1 + g] = 0u;
+        P[nb + g] = make_double2(ta, tb);
+        __threadfence();
+        arrived = atomicAdd(&tickets[0], 1u);
+    }
+    arrived = __shfl_sync(0xffffffffu, arrived, 0);
+    if (arrived != ng - 1) return false;
+    // stage 2: group sums -> total
+    __threadfence();
+    p0 = lane < ng ? __ldcg(&P[nb + lane]) : make_double2(0.0, 0.0);
+    ta = warp_sum(p0.x);
+    tb = warp_sum(p0.y);
+    if (lane == 0) {
+        a = ta;
+        b = tb;
+        tickets[0] = 0u;
     }
     return lane == 0;
 }

@@ -53,7 +53,7 @@ spmv_kernel(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict
         }
     }
     if (!DOT) return;
-    if (grid_sum2(dot, dummy, partials, &st->ticket)) {
+    if (grid_sum2(dot, dummy, partials, st->ticket)) {
         const int k = st->nits + 1;
         st->pAp = dot;
         if (dot == 0.0) {
@@ -175,7 +175,7 @@ pcg_update_kernel(int64_t n, XT *__restrict__ x, VT *__restrict__ r, const VT *_
         rr += rd * rd;
         rz += rd * (double)(ri / D[i]);
     }
-    if (grid_sum2(rr, rz, partials, &st->ticket)) {
+    if (grid_sum2(rr, rz, partials, st->ticket)) {
         const int k = st->nits + 1;
         const double res = sqrt(rr);
         st->nits = k;
@@ -220,6 +220,8 @@ __global__ void residual_kernel(int64_t n, const VT *__restrict__ b, const VT *_
 }
 
 // ---------------------------------------------------------------------------
+static_assert(148 * 8 <= kRedMaxBlocks, "grids of reducing kernels must fit the grid-sum workspace");
+
 int vec_blocks(int64_t n) {
     int64_t b = ceil_div(n, kVecThreads);
     if (b > 148 * 8) b = 148 * 8;
@@ -376,7 +378,7 @@ sell_spmv_kernel(int64_t nslices, const int32_t *__restrict__ perm, const uint16
         }
     }
     if (!DOT) return;
-    if (grid_sum2(dot, dummy, partials, &st->ticket)) {
+    if (grid_sum2(dot, dummy, partials, st->ticket)) {
         const int k = st->nits + 1;
         st->pAp = dot;
         if (dot == 0.0) {
@@ -501,7 +503,7 @@ mixed_update_kernel(int64_t n, float *__restrict__ y, float *__restrict__ r, con
         rr += (double)ri * (double)ri;
         rz += (double)ri * (double)(ri / D[i]);
     }
-    if (grid_sum2(rr, rz, partials, &st->ticket)) {
+    if (grid_sum2(rr, rz, partials, st->ticket)) {
         const int k = st->nits + 1;
         const double res = sqrt(rr);
         st->nits = k;
@@ -567,7 +569,7 @@ mixed_reliable_kernel(int64_t nslices, const int32_t *__restrict__ perm, const u
             rz += (double)rf * (double)(rf / D[row]);
         }
     }
-    if (grid_sum2(rr, rz, partials, &st->ticket)) {
+    if (grid_sum2(rr, rz, partials, st->ticket)) {
         const double res = sqrt(rr);
         st->residual = res;
         st->rz_cur = rz;
@@ -725,7 +727,7 @@ sell2_spmv_kernel(int64_t nslices, const int32_t *__restrict__ perm, const uint1
         }
     }
     if (!DOT) return;
-    if (grid_sum2(dot, dummy, partials, &st->ticket)) {
+    if (grid_sum2(dot, dummy, partials, st->ticket)) {
         const int k = st->nits + 1;
         st->pAp = dot;
         if (dot == 0.0) {

@@ -8,10 +8,17 @@ namespace phgb {
 enum { PCG_RUNNING = 0, PCG_BREAKDOWN = 1, PCG_NONFINITE = 2 };
 
 // Device-resident scalars of one PCG run.
+// Grid-wide sums (reduce.cuh) combine block sums in groups of kRedGroup
+// blocks, then the group sums; grids have at most kRedMaxBlocks blocks and a
+// sum needs kRedTickets counters.
+constexpr int kRedGroup = 64;
+constexpr int kRedMaxBlocks = 2048;   // at most 32 groups: one load per lane
+constexpr int kRedTickets = 1 + kRedMaxBlocks / kRedGroup;
+
 struct PcgState {
     double rz_cur, rz_prev, pAp, alpha, residual, tol;
     int nits, done, status, maxit;
-    unsigned ticket;
+    unsigned ticket[kRedTickets];
     int pad;
 };
 
