@@ -219,19 +219,22 @@ int phgGpuSolverPCGMixed(phgGpuSystem *sys, double rtol, double btol,
  * shape it times CSR with 4/8/16/32 lanes per row and SELL-C-sigma (32-row
  * slices, rows sorted by length in 256-row windows) with 2/4/8-fold
  * unrolling, and keeps the fastest.  kind: 0 = CSR (param = lanes per row),
- * 1 = SELL (param = unroll); times_ms (optional, 15 doubles) gets the
+ * 1 = SELL (param = unroll); times_ms (optional, 17 doubles) gets the
  * measured time of each candidate in that order, then the times of the FP32
  * products of the mixed solver (SELL unrolled 4/8/16, pair-SELL -- two
- * consecutive entries per lane -- unrolled 2/4/8), the unroll chosen for it
- * and its layout (0 SELL, 1 pair SELL); 0 before a mixed solve.  Returns the
+ * consecutive entries per lane -- unrolled 2/4/8, q16 -- four entries per
+ * lane with 16-bit column offsets from two per-row bases -- unrolled 1/2;
+ * 0 for a layout the matrix does not fit), the unroll chosen for it and its
+ * layout (0 SELL, 1 pair SELL, 2 q16); 0 before a mixed solve.  Returns the
  * number of FP64 candidates. */
 int phgGpuGetSpMVPlan(phgGpuSystem *sys, int *kind, int *param,
 		      double *times_ms);
 
 /* Forces the FP32 product layout of the mixed solver for the current matrix
  * instead of the autotuner's choice (no counterpart in the reference):
- * layout 0 = SELL (unroll 4/8/16), 1 = pair SELL (unroll 2/4/8).  A new
- * matrix is tuned again. */
+ * layout 0 = SELL (unroll 4/8/16), 1 = pair SELL (unroll 2/4/8), 2 = q16
+ * (unroll 1/2; PHG_GPU_ERR_ARG when a row of the matrix spans more than two
+ * 65536-column windows).  A matrix of another shape is tuned again. */
 int phgGpuSetSpMVPlan32(phgGpuSystem *sys, int layout, int unroll);
 
 /* Average device time of one SpMV with the chosen layout, FP64 values

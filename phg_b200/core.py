@@ -116,6 +116,10 @@ def _np(a, dtype):
     return np.ascontiguousarray(a, dtype=dtype)
 
 
+# FP32 product layouts of the mixed solver, by their C-ABI codes
+LAYOUTS32 = ("sell", "pair", "q16")
+
+
 class Solver:
     """One assembled linear system on one GPU (a phgGpuSystem)."""
 
@@ -238,9 +242,10 @@ class Solver:
         _check(lib().phgGpuSetSpMVPlan(self._h, 0 if layout == "csr" else 1, int(param)))
 
     def set_spmv_plan32(self, layout, unroll):
-        """Forces the mixed solver's FP32 product: layout "sell" or "pair"
-        with the given unroll."""
-        _check(lib().phgGpuSetSpMVPlan32(self._h, ("sell", "pair").index(layout), int(unroll)))
+        """Forces the mixed solver's FP32 product: layout "sell", "pair" or
+        "q16" (16-bit column offsets; only for matrices whose rows fit two
+        65536-column windows) with the given unroll."""
+        _check(lib().phgGpuSetSpMVPlan32(self._h, LAYOUTS32.index(layout), int(unroll)))
 
     def solve_block_pcg(self, B, rtol=1e-8, maxit=10000, mixed=False, out=None):
         """Block PCG on the columns of B (n x nrhs).  Returns (X, nits[nrhs],
@@ -279,12 +284,12 @@ class Solver:
         names = ["csr4", "csr8", "csr16", "csr32", "sell_u2", "sell_u4", "sell_u8"][:nc]
         info = dict(zip(names, times[:nc].tolist()))
         names32 = ("fp32_sell_u4", "fp32_sell_u8", "fp32_sell_u16", "fp32_pair_u2", "fp32_pair_u4",
-                   "fp32_pair_u8")
+                   "fp32_pair_u8", "fp32_q16_u1", "fp32_q16_u2")
         for i, name in enumerate(names32):
             info[name] = float(times[nc + i])
         k = nc + len(names32)
         info["fp32_unroll"] = int(times[k])
-        info["fp32_layout"] = ("sell", "pair")[int(times[k + 1])]
+        info["fp32_layout"] = LAYOUTS32[int(times[k + 1])]
         return ("csr" if kind.value == 0 else "sell"), param.value, info
 
     def launch_count(self):

@@ -6,6 +6,7 @@
 #include "common.cuh"
 #include "fe_tables.h"
 #include "solve.h"
+#include "q16.h"
 #include "adjoint.h"
 #include "block.h"
 #include "bicgstab.h"
@@ -119,7 +120,7 @@ constexpr int kGraphChunk = 16;
 // SpMV autotuner candidates: CSR with 4/8/16/32 lanes per row, SELL-C-sigma
 // with the inner loop unrolled 2/4/8 times.
 constexpr int kTuneCandidates = 7;
-constexpr int kTune32 = 6;   // FP32 candidates of the mixed solver
+constexpr int kTune32 = 8;   // FP32 candidates of the mixed solver
 const int kTuneKind[kTuneCandidates] = {SPMV_CSR, SPMV_CSR, SPMV_CSR, SPMV_CSR, SPMV_SELL, SPMV_SELL, SPMV_SELL};
 const int kTuneParam[kTuneCandidates] = {4, 8, 16, 32, 2, 4, 8};
 
@@ -179,6 +180,7 @@ struct phgGpuSystem_ {
     cudaGraphExec_t graph = nullptr;
     struct GraphKey {
         const void *x, *r, *p, *Ap, *D, *va, *hist;
+        const void *extra[8];   // further buffers a graph's kernels use (layout arrays)
         int64_t n;
         int lpr;
         cudaStream_t s;
@@ -204,6 +206,18 @@ struct phgGpuSystem_ {
     DevBuf<int32_t> sell2_ssz, sell2_sptr, sell2_cols, sell2_order, sell2_perm;
     DevBuf<uint16_t> sell2_width, sell2_len;
     DevBuf<float> sell2_vals;
+    bool sell_sorted = false;         // sell_perm / sell_len / sell_ssz of the current matrix
+    bool order_valid = false;         // sell2_order (slices widest first) of the current matrix
+    int64_t tuned32_n = -1, tuned32_nnz = -1;
+    // 16-bit-column layout (q16.h), built when every row fits two windows
+    bool q16_valid = false;           // built for the current matrix
+    bool q16_fits = false;            // ... and usable
+    DevBuf<int32_t> q16_ssz, q16_sptr, q16_perm, q16_b0, q16_b1;
+    DevBuf<uint16_t> q16_len, q16_split, q16_cols;
+    DevBuf<float> q16_v32;
+    DevBuf<double> q16_v64;
+    DevBuf<int> q16_nofit;
+    int *h_nofit = nullptr;
     double tune_ms[kTuneCandidates] = {};
 
     // mixed-precision solver
@@ -317,16 +331,36 @@ int solver_buffers(phgGpuSystem *s) {
     return PHG_GPU_OK;
 }
 
-// Builds the SELL-C-sigma copy of the current CSR (values in FP64 and FP32).
-int ensure_sell(phgGpuSystem *s) {
-    if (s->sell_valid) return PHG_GPU_OK;
+// Forgets every layout derived from the matrix (called when it changes).
+void invalidate_layouts(phgGpuSystem *s) {
+    s->sell_sorted = false;
+    s->order_valid = false;
+    s->sell_valid = false;
+    s->sell2_valid = false;
+    s->q16_valid = false;
+    s->q16_fits = false;
+}
+
+// Rows sorted by length in 256-row windows (the slices of every SELL layout).
+int ensure_sell_sort(phgGpuSystem *s) {
+    if (s->sell_sorted) return PHG_GPU_OK;
     const int64_t n = s->n, npos = sell_positions(n), nsl = npos / 32;
     CHECK_RC(s->sell_perm.ensure((size_t)npos));
     CHECK_RC(s->sell_len.ensure((size_t)npos));
     CHECK_RC(s->sell_ssz.ensure((size_t)nsl));
+    CK(launch_sell_sort(n, s->rp.p, s->sell_perm.p, s->sell_len.p, s->sell_ssz.p, s->stream));
+    s->launches += 1;
+    s->sell_sorted = true;
+    return PHG_GPU_OK;
+}
+
+// Builds the SELL-C-sigma copy of the current CSR (values in FP64 and FP32).
+int ensure_sell(phgGpuSystem *s) {
+    if (s->sell_valid) return PHG_GPU_OK;
+    CHECK_RC(ensure_sell_sort(s));
+    const int64_t n = s->n, npos = sell_positions(n), nsl = npos / 32;
     CHECK_RC(s->sell_sptr.ensure((size_t)nsl + 1));
     CHECK_RC(s->scan_ws.ensure((size_t)scan_workspace_elems(nsl)));
-    CK(launch_sell_sort(n, s->rp.p, s->sell_perm.p, s->sell_len.p, s->sell_ssz.p, s->stream));
     CK(launch_scan(nsl, s->sell_ssz.p, s->sell_sptr.p, s->scan_ws.p, s->stream));
     int32_t total = 0;
     CK(cudaMemcpyAsync(&total, s->sell_sptr.p + nsl, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
@@ -337,38 +371,46 @@ int ensure_sell(phgGpuSystem *s) {
     CHECK_RC(s->sell_vals32.ensure((size_t)total));
     CK(launch_sell_fill(n, s->rp.p, s->ci.p, s->va.p, s->sell_perm.p, s->sell_len.p, s->sell_sptr.p,
                         s->sell_cols.p, s->sell_vals.p, s->sell_vals32.p, s->stream));
-    s->launches += 5;
+    s->launches += 4;
     s->sell_total = total;
     s->sell_valid = true;
     return PHG_GPU_OK;
 }
 
-// The FP32 pair layout (mixed solver), built from the SELL slices.
+// The order in which the pair and q16 layouts store the slices: widest
+// first (a stable counting sort of the slice widths, on the host).
+int ensure_slice_order(phgGpuSystem *s) {
+    if (s->order_valid) return PHG_GPU_OK;
+    CHECK_RC(ensure_sell_sort(s));
+    const int64_t nsl = sell_positions(s->n) / 32;
+    const SellView S{s->n, nsl, s->sell_perm.p, s->sell_len.p, nullptr, nullptr, nullptr, nullptr};
+    CHECK_RC(s->sell2_width.ensure((size_t)nsl));
+    CHECK_RC(s->sell2_order.ensure((size_t)nsl));
+    CK(launch_sell2_heads(S, s->sell2_width.p, s->stream));
+    s->launches += 1;
+    std::vector<uint16_t> w((size_t)nsl);
+    std::vector<int32_t> order((size_t)nsl);
+    CK(cudaMemcpyAsync(w.data(), s->sell2_width.p, sizeof(uint16_t) * nsl, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    std::vector<int64_t> start(65537, 0);
+    for (int64_t i = 0; i < nsl; i++) start[65535 - w[i] + 1]++;
+    for (int b = 1; b <= 65536; b++) start[b] += start[b - 1];
+    for (int64_t i = 0; i < nsl; i++) order[start[65535 - w[i]]++] = (int32_t)i;
+    CK(cudaMemcpyAsync(s->sell2_order.p, order.data(), sizeof(int32_t) * nsl, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    s->order_valid = true;
+    return PHG_GPU_OK;
+}
+
+// The FP32 pair layout (mixed solver), built from CSR in the SELL slices.
 int ensure_sell2(phgGpuSystem *s) {
     if (s->sell2_valid) return PHG_GPU_OK;
+    CHECK_RC(ensure_slice_order(s));
     const int64_t nsl = sell_positions(s->n) / 32;
     CHECK_RC(s->sell2_ssz.ensure((size_t)nsl));
     CHECK_RC(s->sell2_sptr.ensure((size_t)nsl + 1));
     CHECK_RC(s->scan_ws.ensure((size_t)scan_workspace_elems(nsl)));
-    const SellView S{s->n, nsl, s->sell_perm.p, s->sell_len.p, s->sell_sptr.p, s->sell_cols.p, s->sell_vals.p,
-                     s->sell_vals32.p};
-    // store the slices widest first: a stable counting sort of the widths
-    CHECK_RC(s->sell2_width.ensure((size_t)nsl));
-    CHECK_RC(s->sell2_order.ensure((size_t)nsl));
-    CK(launch_sell2_heads(S, s->sell2_width.p, s->stream));
-    {
-        std::vector<uint16_t> w((size_t)nsl);
-        std::vector<int32_t> order((size_t)nsl);
-        CK(cudaMemcpyAsync(w.data(), s->sell2_width.p, sizeof(uint16_t) * nsl, cudaMemcpyDeviceToHost, s->stream));
-        CK(cudaStreamSynchronize(s->stream));
-        std::vector<int64_t> start(65537, 0);
-        for (int64_t i = 0; i < nsl; i++) start[65535 - w[i] + 1]++;
-        for (int b = 1; b <= 65536; b++) start[b] += start[b - 1];
-        for (int64_t i = 0; i < nsl; i++) order[start[65535 - w[i]]++] = (int32_t)i;
-        CK(cudaMemcpyAsync(s->sell2_order.p, order.data(), sizeof(int32_t) * nsl, cudaMemcpyHostToDevice,
-                           s->stream));
-        CK(cudaStreamSynchronize(s->stream));
-    }
+    const SellView S{s->n, nsl, s->sell_perm.p, s->sell_len.p, nullptr, nullptr, nullptr, nullptr};
     CK(launch_sell2_sizes(S, s->sell2_order.p, s->sell2_ssz.p, s->stream));
     CK(launch_scan(nsl, s->sell2_ssz.p, s->sell2_sptr.p, s->scan_ws.p, s->stream));
     int32_t total = 0;
@@ -381,8 +423,46 @@ int ensure_sell2(phgGpuSystem *s) {
     CHECK_RC(s->sell2_len.ensure((size_t)nsl * 32));
     CK(launch_sell2_fill(S, s->rp.p, s->ci.p, s->va.p, s->sell2_order.p, s->sell2_sptr.p, s->sell2_perm.p,
                          s->sell2_len.p, s->sell2_cols.p, s->sell2_vals.p, s->stream));
-    s->launches += 5;
+    s->launches += 3;
     s->sell2_valid = true;
+    return PHG_GPU_OK;
+}
+
+// The 16-bit-column layout with FP32 and FP64 values.  Sets q16_fits to
+// whether every row fits two column windows; the layout is used only then.
+int ensure_q16(phgGpuSystem *s) {
+    if (s->q16_valid) return PHG_GPU_OK;
+    CHECK_RC(ensure_slice_order(s));
+    const int64_t nsl = sell_positions(s->n) / 32, npos = nsl * 32;
+    CHECK_RC(s->q16_ssz.ensure((size_t)nsl));
+    CHECK_RC(s->q16_sptr.ensure((size_t)nsl + 1));
+    CHECK_RC(s->scan_ws.ensure((size_t)scan_workspace_elems(nsl)));
+    CHECK_RC(s->q16_nofit.ensure(1));
+    if (s->h_nofit == nullptr) CK(cudaMallocHost((void **)&s->h_nofit, sizeof(int)));
+    CK(launch_q16_sizes(nsl, s->sell_len.p, s->sell2_order.p, s->q16_ssz.p, s->stream));
+    CK(launch_scan(nsl, s->q16_ssz.p, s->q16_sptr.p, s->scan_ws.p, s->stream));
+    int32_t total = 0;
+    CK(cudaMemcpyAsync(&total, s->q16_sptr.p + nsl, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    if (total < 0) return fail(PHG_GPU_ERR_LIMIT, "q16 layout larger than 2^31 entries");
+    CHECK_RC(s->q16_cols.ensure((size_t)total));
+    CHECK_RC(s->q16_v32.ensure((size_t)total));
+    CHECK_RC(s->q16_v64.ensure((size_t)total));
+    CHECK_RC(s->q16_perm.ensure((size_t)npos));
+    CHECK_RC(s->q16_len.ensure((size_t)npos));
+    CHECK_RC(s->q16_split.ensure((size_t)npos));
+    CHECK_RC(s->q16_b0.ensure((size_t)npos));
+    CHECK_RC(s->q16_b1.ensure((size_t)npos));
+    CK(cudaMemsetAsync(s->q16_nofit.p, 0, sizeof(int), s->stream));
+    const Q16Out O{s->q16_sptr.p, s->q16_perm.p, s->q16_len.p, s->q16_split.p, s->q16_b0.p, s->q16_b1.p,
+                   s->q16_cols.p, s->q16_v32.p, s->q16_v64.p};
+    CK(launch_q16_fill(nsl, s->rp.p, s->ci.p, s->va.p, s->sell_perm.p, s->sell_len.p, s->sell2_order.p, O,
+                       s->q16_nofit.p, s->stream));
+    CK(cudaMemcpyAsync(s->h_nofit, s->q16_nofit.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    s->launches += 3;
+    s->q16_valid = true;
+    s->q16_fits = *s->h_nofit == 0;
     return PHG_GPU_OK;
 }
 
@@ -395,39 +475,74 @@ Sell2View sell2_view(phgGpuSystem *s) {
     return Sell2View{s->sell2_sptr.p, s->sell2_cols.p, s->sell2_vals.p, s->sell2_perm.p, s->sell2_len.p};
 }
 
+Q16View q16_view(phgGpuSystem *s) {
+    return Q16View{sell_positions(s->n) / 32, s->q16_sptr.p, s->q16_perm.p, s->q16_len.p, s->q16_split.p,
+                   s->q16_b0.p, s->q16_b1.p, s->q16_cols.p, s->q16_v32.p, s->q16_v64.p};
+}
+
+// FP32 product of the mixed solver on layout `kind` (0 SELL, 1 pair SELL,
+// 2 q16) with unroll `u`.
+int launch_fp32_product(phgGpuSystem *s, int kind, int u, const float *x, float *y) {
+    if (kind == 2) CK(launch_q16_spmv32(q16_view(s), u, x, y, s->stream));
+    else CK(launch_spmv32k(sell_view(s), sell2_view(s), kind, u, x, y, s->stream));
+    s->launches += 1;
+    return PHG_GPU_OK;
+}
+
+// The arrays the mixed solver's FP32 layout `kind` needs for the current
+// matrix (the reliable updates read the FP64 values of the same layout:
+// SELL for kinds 0 and 1).
+int ensure_layout32(phgGpuSystem *s, int kind) {
+    if (kind == 2) return ensure_q16(s);
+    CHECK_RC(ensure_sell(s));
+    if (kind == 1) CHECK_RC(ensure_sell2(s));
+    return PHG_GPU_OK;
+}
+
+const int kTune32Kind[kTune32] = {0, 0, 0, 1, 1, 1, 2, 2};
+const int kTune32Unroll[kTune32] = {4, 8, 16, 2, 4, 8, 1, 2};
+
 // Layout and unroll of the FP32 product (mixed solver), timed once per
-// matrix shape: SELL unrolled 4/8/16, pair SELL unrolled 2/4/8.
+// matrix shape: SELL unrolled 4/8/16, pair SELL unrolled 2/4/8, q16 unrolled
+// 1/2 (when every row fits its two windows).  Later matrices of the shape
+// build only the chosen layout; a q16 choice falls back to a new tuning when
+// a matrix does not fit it.
 int tune_spmv32(phgGpuSystem *s) {
+    if (s->unroll32 != 0 && s->tuned32_n == s->n && s->tuned32_nnz == s->nnz) {
+        CHECK_RC(ensure_layout32(s, s->kind32));
+        if (s->kind32 != 2 || s->q16_fits) return PHG_GPU_OK;
+    }
     CHECK_RC(ensure_sell(s));
     CHECK_RC(ensure_sell2(s));
-    if (s->unroll32 != 0 && s->tuned_n == s->n && s->tuned_nnz == s->nnz) return PHG_GPU_OK;
+    CHECK_RC(ensure_q16(s));
     CHECK_RC(s->r32.ensure((size_t)s->n));
     CHECK_RC(s->Ap32.ensure((size_t)s->n));
     CK(cudaMemsetAsync(s->r32.p, 0, sizeof(float) * s->n, s->stream));
-    const SellView S = sell_view(s);
-    const Sell2View S2 = sell2_view(s);
     cudaEvent_t a, b;
     CK(cudaEventCreate(&a));
     CK(cudaEventCreate(&b));
-    const int ckind[kTune32] = {0, 0, 0, 1, 1, 1}, cu[kTune32] = {4, 8, 16, 2, 4, 8};
-    int best = 0;
+    int best = -1;
     const int reps = 5;
     for (int c = 0; c < kTune32; c++) {
-        for (int i = 0; i < 2; i++) CK(launch_spmv32k(S, S2, ckind[c], cu[c], s->r32.p, s->Ap32.p, s->stream));
+        s->tune32_ms[c] = 0.0;
+        if (kTune32Kind[c] == 2 && !s->q16_fits) continue;
+        for (int i = 0; i < 2; i++) CHECK_RC(launch_fp32_product(s, kTune32Kind[c], kTune32Unroll[c], s->r32.p, s->Ap32.p));
         CK(cudaEventRecord(a, s->stream));
-        for (int i = 0; i < reps; i++) CK(launch_spmv32k(S, S2, ckind[c], cu[c], s->r32.p, s->Ap32.p, s->stream));
+        for (int i = 0; i < reps; i++)
+            CHECK_RC(launch_fp32_product(s, kTune32Kind[c], kTune32Unroll[c], s->r32.p, s->Ap32.p));
         CK(cudaEventRecord(b, s->stream));
         CK(cudaEventSynchronize(b));
         float ms = 0;
         CK(cudaEventElapsedTime(&ms, a, b));
         s->tune32_ms[c] = ms / reps;
-        s->launches += 2 + reps;
-        if (s->tune32_ms[c] < s->tune32_ms[best]) best = c;
+        if (best < 0 || s->tune32_ms[c] < s->tune32_ms[best]) best = c;
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    s->kind32 = ckind[best];
-    s->unroll32 = cu[best];
+    s->kind32 = kTune32Kind[best];
+    s->unroll32 = kTune32Unroll[best];
+    s->tuned32_n = s->n;
+    s->tuned32_nnz = s->nnz;
     return PHG_GPU_OK;
 }
 
@@ -443,10 +558,12 @@ SpmvPlan make_plan(phgGpuSystem *s, int kind, int param) {
 }
 
 // Chooses the fastest SpMV layout for the current matrix shape by timing
-// every candidate on the system's stream (once per (n, nnz)).
-int tune_spmv(phgGpuSystem *s) {
+// every candidate on the system's stream (once per (n, nnz)).  With
+// build_layout false a plan chosen before is kept without building its
+// layout for the current matrix (a caller that will not use the plan).
+int tune_spmv(phgGpuSystem *s, bool build_layout = true) {
     if (s->tuned && s->tuned_n == s->n && s->tuned_nnz == s->nnz) {
-        if (s->plan.kind == SPMV_SELL) CHECK_RC(ensure_sell(s));
+        if (build_layout && s->plan.kind == SPMV_SELL) CHECK_RC(ensure_sell(s));
         s->plan = make_plan(s, s->plan.kind, s->plan.kind == SPMV_CSR ? s->plan.lpr : s->plan.unroll);
         return PHG_GPU_OK;
     }
@@ -549,6 +666,12 @@ int phgGpuDestroy(phgGpuSystem *s) {
     for (auto *b : fbufs) b->release();
     s->sell_perm.release(); s->sell_ssz.release(); s->sell_sptr.release(); s->sell_cols.release();
     s->sell_len.release(); s->sell_vals.release(); s->mst.release();
+    DevBuf<int32_t> *qi[] = {&s->q16_ssz, &s->q16_sptr, &s->q16_perm, &s->q16_b0, &s->q16_b1};
+    for (auto *b : qi) b->release();
+    DevBuf<uint16_t> *qu[] = {&s->q16_len, &s->q16_split, &s->q16_cols};
+    for (auto *b : qu) b->release();
+    s->q16_v32.release(); s->q16_v64.release(); s->q16_nofit.release();
+    if (s->h_nofit) cudaFreeHost(s->h_nofit);
     s->adj_u.release(); s->adj_uobs.release(); s->adj_rhs.release(); s->adj_lambda.release(); s->adj_grad.release();
     if (s->graph_block != nullptr) cudaGraphExecDestroy(s->graph_block);
     DevBuf<double> *bb[] = {&s->bX, &s->bR, &s->bP, &s->bAP, &s->bB, &s->bscal, &s->bpart};
@@ -718,8 +841,7 @@ static int build_system(phgGpuSystem *s, const double *kappa, double mass, const
     s->n = ndof;
     s->assembled = true;
     s->have_bdry_cols = true;
-    s->sell_valid = false;
-    s->sell2_valid = false;
+    invalidate_layouts(s);
     s->lpr = spmv_lanes_for((double)s->nnz / (double)ndof);
     s->mass = mass;
     return PHG_GPU_OK;
@@ -780,8 +902,7 @@ int phgGpuSetMatrix(phgGpuSystem *s, int64_t n, const int64_t *ptr, const int32_
     s->bnnz = 0;
     s->assembled = true;
     s->have_bdry_cols = false;
-    s->sell_valid = false;
-    s->sell2_valid = false;
+    invalidate_layouts(s);
     s->lpr = spmv_lanes_for((double)nnz / (double)n);
     return PHG_GPU_OK;
 }
@@ -866,8 +987,7 @@ int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol,
     if (maxit < 0) return fail(PHG_GPU_ERR_ARG, "maxit < 0");
     CHECK_RC(set_device(s));
     CHECK_RC(solver_buffers(s));
-    CHECK_RC(tune_spmv(s));
-    CHECK_RC(ensure_sell(s));
+    CHECK_RC(tune_spmv(s, false));
     const int64_t n = s->n;
     const size_t un = (size_t)n;
     CHECK_RC(s->r32.ensure(un));
@@ -879,9 +999,16 @@ int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol,
     if (s->h_mst == nullptr) CK(cudaMallocHost((void **)&s->h_mst, sizeof(MixedState)));
     CHECK_RC(copy_in(s, s->x.p, x, un));
     CK(cudaMemsetAsync(s->ticket.p, 0, sizeof(unsigned) * kRedTickets, s->stream));
-    const SpmvPlan P = make_plan(s, s->plan.kind, s->plan.kind == SPMV_CSR ? s->plan.lpr : s->plan.unroll);
-    CHECK_RC(tune_spmv32(s));
+    CHECK_RC(tune_spmv32(s));   // builds the chosen FP32 layout for this matrix
     const int unroll = s->unroll32;
+    const bool q16 = s->kind32 == 2;
+    // FP64 products (residuals): the q16 layout's FP64 values, or the FP64
+    // plan (whose SELL arrays the kinds 0 and 1 have built)
+    const SpmvPlan P = make_plan(s, s->plan.kind, s->plan.kind == SPMV_CSR ? s->plan.lpr : s->plan.unroll);
+    const Q16View Q = q16_view(s);
+    auto product64 = [&](const double *xin, double *yout) -> cudaError_t {
+        return q16 ? launch_q16_spmv64(Q, xin, yout, s->stream) : launch_spmv_plan(P, xin, yout, s->stream);
+    };
 
     CK(launch_init_sums(n, 0, s->x.p, s->rhs.p, s->diag.p, s->partials.p, s->ticket.p, s->sums.p, s->stream));
     CK(cudaMemcpyAsync(s->h_sums, s->sums.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
@@ -907,7 +1034,7 @@ int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol,
     // that drifted above the tolerance restarts from it (at most twice)
     for (int restart = 0; restart < 3; restart++) {
         if (x_nonzero) {
-            CK(launch_spmv_plan(P, s->x.p, s->Ap.p, s->stream));
+            CK(product64(s->x.p, s->Ap.p));
             CK(launch_residual(n, s->rhs.p, s->Ap.p, s->r.p, s->stream));
             s->launches += 2;
         } else {
@@ -939,14 +1066,26 @@ int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol,
 
         phgGpuSystem_::GraphKey key{};
         key.x = s->x.p; key.r = s->r32.p; key.p = s->p32.p; key.Ap = s->Ap32.p; key.D = s->D32.p;
-        key.va = s->sell2_vals.p; key.hist = s->sell_cols.p; key.n = n; key.lpr = unroll + 100 * s->kind32;
+        key.n = n; key.lpr = unroll + 100 * s->kind32;
         key.s = s->stream;
+        if (q16) {
+            key.va = Q.vals32; key.hist = Q.vals64;
+            const void *e[8] = {Q.cols, Q.perm, Q.len, Q.split, Q.base0, Q.base1, Q.sptr, s->partials.p};
+            memcpy(key.extra, e, sizeof(e));
+        } else {
+            key.va = s->sell2_vals.p; key.hist = s->sell_cols.p;
+            const void *e[8] = {s->sell2_cols.p, s->sell2_perm.p, s->sell2_len.p, s->sell2_sptr.p,
+                                s->sell_vals.p, s->sell_vals32.p, s->sell_sptr.p, s->partials.p};
+            memcpy(key.extra, e, sizeof(e));
+        }
         if (s->graph_mixed == nullptr || !(s->gkey_mixed == key)) {
             if (s->graph_mixed != nullptr) { cudaGraphExecDestroy(s->graph_mixed); s->graph_mixed = nullptr; }
             cudaGraph_t gr;
             CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-            for (int i = 0; i < kGraphChunk; i++)
-                launch_mixed_iteration2(B, sell_view(s), sell2_view(s), s->kind32, unroll, s->stream);
+            for (int i = 0; i < kGraphChunk; i++) {
+                if (q16) launch_mixed_iteration_q16(B, Q, unroll, s->stream);
+                else launch_mixed_iteration2(B, sell_view(s), sell2_view(s), s->kind32, unroll, s->stream);
+            }
             CK(cudaStreamEndCapture(s->stream, &gr));
             cudaError_t e = cudaGraphInstantiate(&s->graph_mixed, gr, 0);
             cudaGraphDestroy(gr);
@@ -968,7 +1107,7 @@ int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol,
             return fail(PHG_GPU_ERR_BREAKDOWN, "mixed PCG breakdown: the matrix may not be SPD");
         if (hm.pcg.status == PCG_NONFINITE) return fail(PHG_GPU_ERR_NAN, "mixed PCG: non-finite residual");
         // explicit FP64 residual of the accumulated solution
-        CK(launch_spmv_plan(P, s->x.p, s->Ap.p, s->stream));
+        CK(product64(s->x.p, s->Ap.p));
         CK(launch_residual(n, s->rhs.p, s->Ap.p, s->r.p, s->stream));
         CK(launch_init_sums(n, 1, s->x.p, s->r.p, s->diag.p, s->partials.p, s->ticket.p, s->sums.p, s->stream));
         s->launches += 3;
@@ -1003,8 +1142,12 @@ int phgGpuTimeSpMV(phgGpuSystem *s, int fp32, int reps, double *ms_per_launch) {
     CK(cudaEventCreate(&b));
     for (int i = 0; i < reps + 3; i++) {
         if (i == 3) CK(cudaEventRecord(a, s->stream));
-        if (fp32) CK(launch_spmv32k(sell_view(s), sell2_view(s), s->kind32, s->unroll32, s->r32.p, s->Ap32.p, s->stream));
-        else CK(launch_spmv_plan(P, s->rhs.p, s->Ap.p, s->stream));
+        if (fp32) {
+            CHECK_RC(launch_fp32_product(s, s->kind32, s->unroll32, s->r32.p, s->Ap32.p));
+        } else {
+            CK(launch_spmv_plan(P, s->rhs.p, s->Ap.p, s->stream));
+            s->launches += 1;
+        }
     }
     CK(cudaEventRecord(b, s->stream));
     CK(cudaEventSynchronize(b));
@@ -1012,7 +1155,6 @@ int phgGpuTimeSpMV(phgGpuSystem *s, int fp32, int reps, double *ms_per_launch) {
     CK(cudaEventElapsedTime(&ms, a, b));
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    s->launches += reps + 3;
     *ms_per_launch = ms / reps;
     return PHG_GPU_OK;
 }
@@ -1035,17 +1177,19 @@ int phgGpuSetSpMVPlan(phgGpuSystem *s, int kind, int param) {
 int phgGpuSetSpMVPlan32(phgGpuSystem *s, int layout, int unroll) {
     if (s == nullptr) return fail(PHG_GPU_ERR_ARG, "null system");
     if (!s->assembled) return fail(PHG_GPU_ERR_STATE, "no assembled system");
-    const bool ok = (layout == 0 && (unroll == 4 || unroll == 8 || unroll == 16)) ||
-                    (layout == 1 && (unroll == 2 || unroll == 4 || unroll == 8));
+    bool ok = false;
+    for (int c = 0; c < kTune32; c++) ok = ok || (kTune32Kind[c] == layout && kTune32Unroll[c] == unroll);
     if (!ok) return fail(PHG_GPU_ERR_ARG, "no FP32 SpMV layout (%d, %d)", layout, unroll);
     CHECK_RC(set_device(s));
     CHECK_RC(tune_spmv(s));   // FP64 layout for this matrix (returns at once if chosen)
-    CHECK_RC(ensure_sell(s));
-    CHECK_RC(ensure_sell2(s));
+    CHECK_RC(ensure_layout32(s, layout));
+    if (layout == 2 && !s->q16_fits)
+        return fail(PHG_GPU_ERR_ARG, "the q16 layout does not fit this matrix: a row spans more than two "
+                    "65536-column windows");
     s->kind32 = layout;
     s->unroll32 = unroll;
-    s->tuned_n = s->n;
-    s->tuned_nnz = s->nnz;
+    s->tuned32_n = s->n;
+    s->tuned32_nnz = s->nnz;
     return PHG_GPU_OK;
 }
 

@@ -11,6 +11,8 @@
 // flag, so a captured graph of many iterations turns into no-ops once the
 // stopping rule of the reference (||r|| <= tol or nits == maxit) is met.
 #include "common.cuh"
+#include "pcg_final.cuh"
+#include "q16.h"
 #include "reduce.cuh"
 #include "solve.h"
 
@@ -18,13 +20,11 @@
 
 namespace phgb {
 
-constexpr int kVecThreads = 256;
-
 
 // ---------------------------------------------------------------------------
 // SpMV: LPR lanes per row (CSR vector form).  With DOT, also p.y -> state.
 template <int LPR, bool DOT, typename VT>
-__global__ void __launch_bounds__(kVecThreads)
+__global__ void __launch_bounds__(kVecThreads, kResidentBlocks)
 spmv_kernel(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
             const VT *__restrict__ va, const VT *__restrict__ x, VT *__restrict__ y,
             double *partials, PcgState *st) {
@@ -53,17 +53,7 @@ spmv_kernel(int64_t n, const int32_t *__restrict__ rp, const int32_t *__restrict
         }
     }
     if (!DOT) return;
-    if (grid_sum2(dot, dummy, partials, st->ticket)) {
-        const int k = st->nits + 1;
-        st->pAp = dot;
-        if (dot == 0.0) {
-            st->done = 1;
-            st->status = PCG_BREAKDOWN;
-            st->nits = k;
-        } else {
-            st->alpha = st->rz_cur / dot;
-        }
-    }
+    if (grid_sum2(dot, dummy, partials, st->ticket)) pcg_pap_final(dot, st);
 }
 
 // p = r / D (first iteration) or p = z + beta p; 16-byte vectors of rows.
@@ -342,7 +332,7 @@ __global__ void sell_fill_kernel(int64_t npos, const int32_t *__restrict__ rp, c
 }
 
 template <typename VT, bool DOT, int U>
-__global__ void __launch_bounds__(kVecThreads)
+__global__ void __launch_bounds__(kVecThreads, kResidentBlocks)
 sell_spmv_kernel(int64_t nslices, const int32_t *__restrict__ perm, const uint16_t *__restrict__ len,
                  const int32_t *__restrict__ sptr, const int32_t *__restrict__ cols, const VT *__restrict__ vals,
                  const VT *__restrict__ x, VT *__restrict__ y, double *partials, PcgState *st) {
@@ -378,17 +368,7 @@ sell_spmv_kernel(int64_t nslices, const int32_t *__restrict__ perm, const uint16
         }
     }
     if (!DOT) return;
-    if (grid_sum2(dot, dummy, partials, st->ticket)) {
-        const int k = st->nits + 1;
-        st->pAp = dot;
-        if (dot == 0.0) {
-            st->done = 1;
-            st->status = PCG_BREAKDOWN;
-            st->nits = k;
-        } else {
-            st->alpha = st->rz_cur / dot;
-        }
-    }
+    if (grid_sum2(dot, dummy, partials, st->ticket)) pcg_pap_final(dot, st);
 }
 
 int64_t sell_positions(int64_t n) { return ceil_div(n, kSellWin) * kSellWin; }
@@ -526,7 +506,7 @@ mixed_update_kernel(int64_t n, float *__restrict__ y, float *__restrict__ r, con
 // Reliable update on the SELL layout (FP64 values): x += y, r_true -= A y,
 // r32 = (float) r_true, ||r_true||^2 and r32.(r32/D).
 template <int U>
-__global__ void __launch_bounds__(kVecThreads)
+__global__ void __launch_bounds__(kVecThreads, kResidentBlocks)
 mixed_reliable_kernel(int64_t nslices, const int32_t *__restrict__ perm, const uint16_t *__restrict__ len,
                       const int32_t *__restrict__ sptr, const int32_t *__restrict__ cols,
                       const double *__restrict__ vals, double *__restrict__ x, const float *__restrict__ y,
@@ -569,20 +549,7 @@ mixed_reliable_kernel(int64_t nslices, const int32_t *__restrict__ perm, const u
             rz += (double)rf * (double)(rf / D[row]);
         }
     }
-    if (grid_sum2(rr, rz, partials, st->ticket)) {
-        const double res = sqrt(rr);
-        st->residual = res;
-        st->rz_cur = rz;
-        ms->maxr = res;
-        ms->y_reset = 1;
-        ms->ru_flag = 0;
-        ms->nupdates += 1;
-        if (hist != nullptr) hist[st->nits] = res;
-        if (ms->final_check) {
-            ms->final_check = 0;
-            if (!(res > st->tol) || st->nits >= st->maxit) st->done = 1;
-        }
-    }
+    if (grid_sum2(rr, rz, partials, st->ticket)) mixed_reliable_final(rr, rz, ms, hist);
 }
 
 // r32 = (float) rtrue, y = 0, and (||rtrue||^2, r32.(r32/D)).
@@ -686,7 +653,7 @@ __global__ void sell2_fill_kernel(int64_t npos, const int32_t *__restrict__ rp, 
 }
 
 template <bool DOT, int U>
-__global__ void __launch_bounds__(kVecThreads)
+__global__ void __launch_bounds__(kVecThreads, kResidentBlocks)
 sell2_spmv_kernel(int64_t nslices, const int32_t *__restrict__ perm, const uint16_t *__restrict__ len,
                   const int32_t *__restrict__ sptr2, const int32_t *__restrict__ cols2,
                   const float *__restrict__ vals2, const float *__restrict__ x, float *__restrict__ y,
@@ -727,17 +694,7 @@ sell2_spmv_kernel(int64_t nslices, const int32_t *__restrict__ perm, const uint1
         }
     }
     if (!DOT) return;
-    if (grid_sum2(dot, dummy, partials, st->ticket)) {
-        const int k = st->nits + 1;
-        st->pAp = dot;
-        if (dot == 0.0) {
-            st->done = 1;
-            st->status = PCG_BREAKDOWN;
-            st->nits = k;
-        } else {
-            st->alpha = st->rz_cur / dot;
-        }
-    }
+    if (grid_sum2(dot, dummy, partials, st->ticket)) pcg_pap_final(dot, st);
 }
 
 cudaError_t launch_sell2_heads(const SellView &S, uint16_t *width, cudaStream_t s) {
@@ -797,6 +754,18 @@ cudaError_t launch_mixed_iteration2(const MixedBuffers &B, const SellView &S, co
     mixed_reliable_kernel<4><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals, B.x, B.y32,
                                                          B.rtrue, B.r32, B.D32, B.partials, B.ms, B.hist);
     return cudaGetLastError();
+}
+
+cudaError_t launch_mixed_iteration_q16(const MixedBuffers &B, const Q16View &Q, int unroll, cudaStream_t s) {
+    const int vb = vvec_blocks(B.n, 4);
+    PcgState *st = &B.ms->pcg;
+    pcg_dir_kernel<float><<<vb, kVecThreads, 0, s>>>(B.n, B.r32, B.D32, B.p32, st);
+    cudaError_t e = launch_q16_spmv32_dot(Q, unroll, B.p32, B.Ap32, B.partials, st, s);
+    if (e != cudaSuccess) return e;
+    mixed_update_kernel<<<vb, kVecThreads, 0, s>>>(B.n, B.y32, B.r32, B.p32, B.Ap32, B.D32, B.partials, B.ms);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_q16_reliable(Q, B, s);
 }
 
 }  // namespace phgb

@@ -5,6 +5,12 @@
 
 namespace phgb {
 
+constexpr int kVecThreads = 256;   // threads per block of the solver kernels
+// Grid-stride kernels launched on vec_blocks() grids (148 x 8 blocks) declare
+// 8 resident blocks per SM (at most 32 registers a thread): with fewer, the
+// grid runs as two waves and the second leaves most of the GPU idle.
+constexpr int kResidentBlocks = 8;
+
 enum { PCG_RUNNING = 0, PCG_BREAKDOWN = 1, PCG_NONFINITE = 2 };
 
 // Device-resident scalars of one PCG run.

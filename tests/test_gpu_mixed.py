@@ -109,7 +109,8 @@ def far_coupled_spd(n, offsets, seed):
     return A.indptr.astype(np.int64), A.indices.astype(np.int32), A.data, rng.standard_normal(n)
 
 
-LAYOUTS32 = [("sell", 4), ("sell", 8), ("sell", 16), ("pair", 2), ("pair", 4), ("pair", 8)]
+LAYOUTS32 = [("sell", 4), ("sell", 8), ("sell", 16), ("pair", 2), ("pair", 4), ("pair", 8), ("q16", 1),
+             ("q16", 2)]
 
 
 @pytest.mark.parametrize("case", ["p2_m16", "far_coupled"])
@@ -129,6 +130,11 @@ def test_every_fp32_layout_in_mixed_pcg(gpu, oracle, case):
         s.set_matrix(ptr, cols, vals, rhs)
     its = {}
     for layout, u in LAYOUTS32:
+        if layout == "q16" and case == "far_coupled":
+            # rows span three 65536-column windows: the layout is refused
+            with pytest.raises(gpu.PhgGpuError):
+                s.set_spmv_plan32(layout, u)
+            continue
         s.set_spmv_plan32(layout, u)
         x, nits, res, nupd = s.solve_pcg_mixed(rtol=1e-8)
         r = rhs - oracle.spmv(ptr, cols, vals, x)
@@ -137,3 +143,34 @@ def test_every_fp32_layout_in_mixed_pcg(gpu, oracle, case):
         assert s.spmv_plan()[2]["fp32_layout"] == layout
     s.close()
     assert max(its.values()) - min(its.values()) <= max(3, min(its.values()) // 20), its
+
+
+def test_q16_layout_follows_the_matrix(gpu, oracle):
+    """The autotuner offers q16 only for matrices whose rows fit two column
+    windows; a matrix of the same shape that does not fit makes a q16 choice
+    fall back to a new tuning, and a new matrix that fits gets its own q16
+    arrays (the residual is recomputed by the oracle each time)."""
+    n = 200003
+    s = gpu.Solver(0)
+    # banded first: every row fits one window
+    ptr, cols, vals, rhs = far_coupled_spd(n, (3, 7), seed=1)
+    s.set_matrix(ptr, cols, vals, rhs)
+    s.set_spmv_plan32("q16", 1)
+    x, nits, res, _ = s.solve_pcg_mixed(rtol=1e-8)
+    assert np.linalg.norm(rhs - oracle.spmv(ptr, cols, vals, x)) <= 1e-8 * np.linalg.norm(rhs) * (1 + 1e-9)
+    assert s.spmv_plan()[2]["fp32_layout"] == "q16"
+    # same shape (n, nnz), rows spanning three windows
+    ptr2, cols2, vals2, rhs2 = far_coupled_spd(n, (70001, 140003), seed=2)
+    assert len(cols2) == len(cols)
+    s.set_matrix(ptr2, cols2, vals2, rhs2)
+    x, nits, res, _ = s.solve_pcg_mixed(rtol=1e-8)
+    assert np.linalg.norm(rhs2 - oracle.spmv(ptr2, cols2, vals2, x)) <= 1e-8 * np.linalg.norm(rhs2) * (1 + 1e-9)
+    info = s.spmv_plan()[2]
+    assert info["fp32_layout"] != "q16"
+    assert info["fp32_q16_u1"] == 0.0 and info["fp32_q16_u2"] == 0.0
+    # back to a matrix that fits: new values, same pattern as the first
+    s.set_matrix(ptr, cols, vals * 2.0, rhs)
+    s.set_spmv_plan32("q16", 2)
+    x, nits, res, _ = s.solve_pcg_mixed(rtol=1e-8)
+    assert np.linalg.norm(rhs - oracle.spmv(ptr, cols, vals * 2.0, x)) <= 1e-8 * np.linalg.norm(rhs) * (1 + 1e-9)
+    s.close()
