@@ -243,6 +243,13 @@ int phgGpuSetSpMVPlan32(phgGpuSystem *sys, int layout, int unroll);
  * reference; used to report the SpMV roofline). */
 int phgGpuTimeSpMV(phgGpuSystem *sys, int fp32, int reps, double *ms_per_launch);
 
+/* Bytes one product moves in the layout the solvers use for the current
+ * matrix, FP64 (fp32 = 0) or the mixed solver's FP32 product (fp32 = 1):
+ * values, column indices, per-row metadata and slice offsets as stored
+ * (padding included), x read once and y written once (no counterpart in the
+ * reference; the denominator of the layout's bandwidth). */
+int phgGpuSpMVBytes(phgGpuSystem *sys, int fp32, int64_t *bytes);
+
 /* Overrides the autotuner for the current matrix shape: kind 0 = CSR with
  * param = 4/8/16/32 lanes per row, kind 1 = SELL with param = 2/4/8
  * (no counterpart in the reference). */

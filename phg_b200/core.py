@@ -53,6 +53,7 @@ SIGNATURES = {
     "phgGpuAdjointGradient": (C.c_int, [_P, _P, _P, C.c_double, C.c_int, _P, C.POINTER(C.c_double),
                                         C.POINTER(C.c_int)]),
     "phgGpuTimeSpMV": (C.c_int, [_P, C.c_int, C.c_int, C.POINTER(C.c_double)]),
+    "phgGpuSpMVBytes": (C.c_int, [_P, C.c_int, C.POINTER(_I64)]),
     "phgGpuSolverPCGMixed": (C.c_int, [_P, C.c_double, C.c_double, C.c_double, C.c_int, _P,
                                        C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     "phgGpuSolverPCGNoAlloc": (C.c_int, [_I64, _P, _P, _P, _P, _P, C.c_double, C.c_double,
@@ -237,6 +238,13 @@ class Solver:
         ms = C.c_double()
         _check(lib().phgGpuTimeSpMV(self._h, 1 if fp32 else 0, int(reps), C.byref(ms)))
         return ms.value
+
+    def spmv_bytes(self, fp32=False):
+        """Bytes one product moves in the layout in use (values, indices,
+        metadata as stored, x read once, y written once)."""
+        b = _I64()
+        _check(lib().phgGpuSpMVBytes(self._h, 1 if fp32 else 0, C.byref(b)))
+        return b.value
 
     def set_spmv_plan(self, layout, param):
         _check(lib().phgGpuSetSpMVPlan(self._h, 0 if layout == "csr" else 1, int(param)))

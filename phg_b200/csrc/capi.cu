@@ -218,6 +218,7 @@ struct phgGpuSystem_ {
     DevBuf<double> q16_v64;
     DevBuf<int> q16_nofit;
     int *h_nofit = nullptr;
+    int64_t sell2_total = 0, q16_total = 0;   // stored entries (padding included)
     double tune_ms[kTuneCandidates] = {};
 
     // mixed-precision solver
@@ -424,6 +425,7 @@ int ensure_sell2(phgGpuSystem *s) {
     CK(launch_sell2_fill(S, s->rp.p, s->ci.p, s->va.p, s->sell2_order.p, s->sell2_sptr.p, s->sell2_perm.p,
                          s->sell2_len.p, s->sell2_cols.p, s->sell2_vals.p, s->stream));
     s->launches += 3;
+    s->sell2_total = total;
     s->sell2_valid = true;
     return PHG_GPU_OK;
 }
@@ -461,6 +463,7 @@ int ensure_q16(phgGpuSystem *s) {
     CK(cudaMemcpyAsync(s->h_nofit, s->q16_nofit.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
     s->launches += 3;
+    s->q16_total = total;
     s->q16_valid = true;
     s->q16_fits = *s->h_nofit == 0;
     return PHG_GPU_OK;
@@ -1205,6 +1208,26 @@ int phgGpuGetSpMVPlan(phgGpuSystem *s, int *kind, int *param, double *times_ms) 
         times_ms[kTuneCandidates + kTune32 + 1] = s->kind32;
     }
     return kTuneCandidates;
+}
+
+int phgGpuSpMVBytes(phgGpuSystem *s, int fp32, int64_t *bytes) {
+    if (s == nullptr || bytes == nullptr) return fail(PHG_GPU_ERR_ARG, "invalid arguments");
+    if (!s->assembled) return fail(PHG_GPU_ERR_STATE, "no assembled system");
+    CHECK_RC(set_device(s));
+    CHECK_RC(tune_spmv(s));
+    const int64_t n = s->n, npos = sell_positions(n), nsl = npos / 32;
+    const int64_t vec = (fp32 ? 8 : 16) * n, sl = 4 * (nsl + 1);   // x read once + y written; slice offsets
+    if (fp32) {
+        CHECK_RC(tune_spmv32(s));
+        if (s->kind32 == 2) *bytes = 6 * s->q16_total + 16 * npos + sl + vec;
+        else if (s->kind32 == 1) *bytes = 8 * s->sell2_total + 6 * npos + sl + vec;
+        else *bytes = 8 * s->sell_total + 6 * npos + sl + vec;
+    } else if (s->plan.kind == SPMV_SELL) {
+        *bytes = 12 * s->sell_total + 6 * npos + sl + vec;
+    } else {
+        *bytes = 12 * s->nnz + 4 * (n + 1) + vec;
+    }
+    return PHG_GPU_OK;
 }
 
 int phgGpuGetLaunchCount(phgGpuSystem *s, int64_t *count) {
