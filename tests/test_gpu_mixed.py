@@ -113,15 +113,16 @@ LAYOUTS32 = [("sell", 4), ("sell", 8), ("sell", 16), ("pair", 2), ("pair", 4), (
              ("q16", 2)]
 
 
-@pytest.mark.parametrize("case", ["p2_m16", "far_coupled"])
+@pytest.mark.parametrize("case", ["p2_m16", "p3_m6", "far_coupled"])
 def test_every_fp32_layout_in_mixed_pcg(gpu, oracle, case):
     """The mixed solver with each FP32 product layout forced: the FP64
     residual (recomputed by the oracle) meets the stopping rule and the
     iteration counts agree within a few iterations (the layouts differ only
     in the FP32 summation order).  "far_coupled" is a matrix given through
-    phgGpuSetMatrix whose rows couple columns far apart."""
-    if case == "p2_m16":
-        s = system(gpu, 2, 16)
+    phgGpuSetMatrix whose rows couple columns far apart; P3 rows (up to 175
+    entries) take several rounds of the warp that builds the q16 layout."""
+    if case in ("p2_m16", "p3_m6"):
+        s = system(gpu, 2, 16) if case == "p2_m16" else system(gpu, 3, 6)
         ptr, cols, vals = s.get_matrix()
         rhs = s.get_rhs()
     else:
