@@ -166,17 +166,27 @@ geometry_kernel(int64_t nelem, int64_t nvert, const double *__restrict__ verts, 
     }
 }
 
+// Quadrature weights, passed by value: every lane reads the same weight at
+// the same time, so they are read from the kernel's parameter (constant)
+// bank instead of through the load/store pipe the kernel is bound by.
+struct ElemWeights {
+    double wk[kElemMaxQK];
+    double wr[kElemMaxQR];
+};
+
 // Element matrices and vectors: one warp per element.
 template <int P>
 __global__ void __launch_bounds__(ElemDims<P>::WARPS * 32)
 element_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, const int32_t *__restrict__ e2l,
                const double *__restrict__ kappa, const double mass, const double *__restrict__ f,
-               const double *__restrict__ wk, const double *__restrict__ gk,
-               const double *__restrict__ wr, const double *__restrict__ br,
+               const ElemWeights Wt, const double *__restrict__ gk, const double *__restrict__ br,
                double *__restrict__ Ke, double *__restrict__ Re, int *status) {
     using D = ElemDims<P>;
     constexpr int N = D::N, QK = D::QK, QR = D::QR, W = D::WARPS;
     __shared__ double s_geo[W][kGeo + 1];       // J (16), volume, kappa
+    // basis gradients at the stiffness points, component-major with the basis
+    // index fastest (grad[(c * QK + q) * N + k]): lanes that read gradients
+    // of different bases hit different banks
     __shared__ double s_grad[W][N * QK * 3];
     __shared__ double s_K[W][N * N];
     __shared__ double s_f[W][N];
@@ -201,24 +211,25 @@ element_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, cons
         __syncwarp();
         const double vol = J[16], kap = J[17];
 
-        // basis gradients at the stiffness points: grad[(k*QK + q)*3 + c]
+        // basis gradients at the stiffness points
+        constexpr int CS = QK * N;   // component stride of grad
         for (int idx = lane; idx < N * QK; idx += 32) {
-            const int k = idx / QK, q = idx % QK;
-            double *o = grad + 3 * idx;
+            const int k = idx % N, q = idx / N;
+            double *o = grad + q * N + k;
             if (P == 1) {
-                o[0] = J[4 * k]; o[1] = J[4 * k + 1]; o[2] = J[4 * k + 2];
+                o[0] = J[4 * k]; o[CS] = J[4 * k + 1]; o[2 * CS] = J[4 * k + 2];
             } else if (k < 4) {
                 const double d = gk[(q * N + k) * 4 + k];
                 o[0] = rn_mul(d, J[4 * k]);
-                o[1] = rn_mul(d, J[4 * k + 1]);
-                o[2] = rn_mul(d, J[4 * k + 2]);
+                o[CS] = rn_mul(d, J[4 * k + 1]);
+                o[2 * CS] = rn_mul(d, J[4 * k + 2]);
             } else {
                 const double *G = gk + (q * N + k) * 4;
                 const double g0 = G[0], g1 = G[1], g2 = G[2], g3 = G[3];
 #pragma unroll
                 for (int c = 0; c < 3; c++)
-                    o[c] = rn_add(rn_add(rn_add(rn_mul(g0, J[c]), rn_mul(g1, J[4 + c])), rn_mul(g2, J[8 + c])),
-                                  rn_mul(g3, J[12 + c]));
+                    o[c * CS] = rn_add(rn_add(rn_add(rn_mul(g0, J[c]), rn_mul(g1, J[4 + c])), rn_mul(g2, J[8 + c])),
+                                       rn_mul(g3, J[12 + c]));
             }
         }
         for (int q = lane; q < QR; q += 32) {
@@ -235,11 +246,11 @@ element_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, cons
             double d = 0.;
 #pragma unroll 4
             for (int q = 0; q < QK; q++) {
-                const double *g1 = grad + 3 * (b * QK + q);
-                const double *g2 = grad + 3 * (a * QK + q);
-                const double d0 = rn_add(0., rn_add(rn_add(rn_mul(g1[0], g2[0]), rn_mul(g1[1], g2[1])),
-                                                    rn_mul(g1[2], g2[2])));
-                const double t = rn_mul(d0, wk[q]);
+                const double *g1 = grad + q * N + b;
+                const double *g2 = grad + q * N + a;
+                const double d0 = rn_add(0., rn_add(rn_add(rn_mul(g1[0], g2[0]), rn_mul(g1[CS], g2[CS])),
+                                                    rn_mul(g1[2 * CS], g2[2 * CS])));
+                const double t = rn_mul(d0, Wt.wk[q]);
                 d = rn_add(d, kappa != nullptr ? rn_mul(t, kap) : t);
             }
             double v = rn_mul(d, vol);
@@ -247,7 +258,7 @@ element_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, cons
                 double dm = 0.;
                 for (int q = 0; q < QR; q++) {
                     const double d0 = rn_add(0., rn_mul(br[q * N + b], br[q * N + a]));
-                    dm = rn_add(dm, rn_mul(d0, wr[q]));
+                    dm = rn_add(dm, rn_mul(d0, Wt.wr[q]));
                 }
                 v = rn_add(v, rn_mul(mass, rn_mul(dm, vol)));
             }
@@ -256,7 +267,7 @@ element_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, cons
         }
         if (lane < N) {
             double d = 0.0;
-            for (int q = 0; q < QR; q++) d = rn_add(d, rn_mul(rn_mul(br[q * N + lane], wr[q]), fq[q]));
+            for (int q = 0; q < QR; q++) d = rn_add(d, rn_mul(rn_mul(br[q * N + lane], Wt.wr[q]), fq[q]));
             Re[(size_t)e * N + lane] = rn_mul(d, vol);
         }
         __syncwarp();
@@ -393,7 +404,7 @@ __device__ __forceinline__ double bdry_rhs(const double *g, int32_t k, int mult)
 }
 
 template <int N>
-__global__ void __launch_bounds__(WalkCfg<N>::WARPS * 32, 4)
+__global__ void __launch_bounds__(WalkCfg<N>::WARPS * 32, 8)
 row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t *__restrict__ inc,
                 const int32_t *__restrict__ e2l, const uint8_t *__restrict__ bdry,
                 const double *__restrict__ Ke, const double *__restrict__ Re, const double *__restrict__ g,
@@ -643,7 +654,10 @@ static void elem_launch(const ElemArgs &A, cudaStream_t s) {
     geometry_kernel<<<grid_for(A.nelem, 128, 148 * 64), 128, 0, s>>>(A.nelem, A.nvert, A.verts, A.elems, A.geo,
                                                                     A.status);
     const int blocks = grid_for(A.nelem, W, 148 * 64);
-    element_kernel<P><<<blocks, W * 32, 0, s>>>(A.nelem, A.ndof, A.geo, A.e2l, A.kappa, A.mass, A.f, A.wk, A.gk, A.wr,
+    ElemWeights Wt{};
+    for (int q = 0; q < ElemDims<P>::QK; q++) Wt.wk[q] = A.wk_host[q];
+    for (int q = 0; q < ElemDims<P>::QR; q++) Wt.wr[q] = A.wr_host[q];
+    element_kernel<P><<<blocks, W * 32, 0, s>>>(A.nelem, A.ndof, A.geo, A.e2l, A.kappa, A.mass, A.f, Wt, A.gk,
                                                 A.br, A.Ke, A.Re, A.status);
 }
 

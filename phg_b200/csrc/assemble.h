@@ -5,13 +5,19 @@
 
 namespace phgb {
 
+// Largest quadrature rules of the element kernel (P3: order 4 with 14
+// points for the stiffness, order 6 with 24 for the mass and RHS).
+constexpr int kElemMaxQK = 14;
+constexpr int kElemMaxQR = 24;
+
 struct ElemArgs {
     int64_t nelem, nvert, ndof;
     const double *verts;
     const int32_t *elems, *e2l;
     const double *kappa, *f;                 // may be null
     double mass;                             // mass coefficient c (0: stiffness only)
-    const double *wk, *gk, *wr, *br;         // element tables
+    const double *gk, *br;                   // element tables (device)
+    const double *wk_host, *wr_host;         // quadrature weights (host; passed by value)
     double *geo;                             // scratch: nelem * geometry_doubles
     double *Ke, *Re;
     int *status;

@@ -152,7 +152,8 @@ struct phgGpuSystem_ {
 
     // element tables
     int tab_order = 0;
-    DevBuf<double> wk, gk, wr, br;
+    DevBuf<double> gk, br;                 // basis derivatives / values at the points (device)
+    std::vector<double> wk, wr;            // quadrature weights (passed to the kernel by value)
 
     // assembly buffers
     DevBuf<double> Ke, Re, kappa, f, g, geo;
@@ -307,14 +308,14 @@ int stage(phgGpuSystem *s, const T *src, size_t n, DevBuf<T> &buf, const T **out
 int upload_tables(phgGpuSystem *s, int p) {
     if (s->tab_order == p) return PHG_GPU_OK;
     const ElementTables t = make_tables(p);
-    CHECK_RC(s->wk.ensure(t.wk.size()));
+    if ((int)t.wk.size() > kElemMaxQK || (int)t.wr.size() > kElemMaxQR)
+        return fail(PHG_GPU_ERR_LIMIT, "quadrature rule larger than the element kernel's");
     CHECK_RC(s->gk.ensure(t.gk.size()));
-    CHECK_RC(s->wr.ensure(t.wr.size()));
     CHECK_RC(s->br.ensure(t.br.size()));
-    CK(cudaMemcpy(s->wk.p, t.wk.data(), t.wk.size() * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(s->gk.p, t.gk.data(), t.gk.size() * sizeof(double), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(s->wr.p, t.wr.data(), t.wr.size() * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(s->br.p, t.br.data(), t.br.size() * sizeof(double), cudaMemcpyHostToDevice));
+    s->wk = t.wk;
+    s->wr = t.wr;
     s->tab_order = p;
     return PHG_GPU_OK;
 }
@@ -683,7 +684,7 @@ int phgGpuDestroy(phgGpuSystem *s) {
     for (auto *b : bf) b->release();
     s->bint.release();
     s->btick.release();
-    DevBuf<double> *dbufs[] = {&s->verts, &s->wk, &s->gk, &s->wr, &s->br, &s->Ke, &s->Re, &s->kappa, &s->f,
+    DevBuf<double> *dbufs[] = {&s->verts, &s->gk, &s->br, &s->Ke, &s->Re, &s->kappa, &s->f,
                                &s->g, &s->geo, &s->va, &s->bva, &s->rhs, &s->diag, &s->x, &s->r, &s->p, &s->Ap,
                                &s->partials, &s->hist, &s->sums};
     for (auto *b : dbufs) b->release();
@@ -789,7 +790,7 @@ static int element_pass(phgGpuSystem *s, const double *kappa, double mass, const
     ea.nelem = s->nelem; ea.nvert = s->nvert; ea.ndof = ndof;
     ea.verts = s->verts.p; ea.elems = s->elems.p; ea.e2l = s->e2l.p;
     ea.kappa = dk; ea.f = df; ea.mass = mass;
-    ea.wk = s->wk.p; ea.gk = s->gk.p; ea.wr = s->wr.p; ea.br = s->br.p;
+    ea.gk = s->gk.p; ea.br = s->br.p; ea.wk_host = s->wk.data(); ea.wr_host = s->wr.data();
     ea.Ke = s->Ke.p; ea.Re = s->Re.p; ea.geo = s->geo.p; ea.status = s->status.p;
     CK(launch_element_kernel(s->order, ea, s->stream));
     s->launches += 2;
