@@ -180,6 +180,7 @@ __global__ void __launch_bounds__(ElemDims<P>::WARPS * 32)
 element_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, const int32_t *__restrict__ e2l,
                const double *__restrict__ kappa, const double mass, const double *__restrict__ f,
                const ElemWeights Wt, const double *__restrict__ gk, const double *__restrict__ br,
+               const double *__restrict__ brt,
                double *__restrict__ Ke, double *__restrict__ Re, int *status) {
     using D = ElemDims<P>;
     constexpr int N = D::N, QK = D::QK, QR = D::QR, W = D::WARPS;
@@ -219,13 +220,13 @@ element_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, cons
             if (P == 1) {
                 o[0] = J[4 * k]; o[CS] = J[4 * k + 1]; o[2 * CS] = J[4 * k + 2];
             } else if (k < 4) {
-                const double d = gk[(q * N + k) * 4 + k];
+                const double d = gk[(k * QK + q) * N + k];
                 o[0] = rn_mul(d, J[4 * k]);
                 o[CS] = rn_mul(d, J[4 * k + 1]);
                 o[2 * CS] = rn_mul(d, J[4 * k + 2]);
             } else {
-                const double *G = gk + (q * N + k) * 4;
-                const double g0 = G[0], g1 = G[1], g2 = G[2], g3 = G[3];
+                const double *G = gk + q * N + k;
+                const double g0 = G[0], g1 = G[CS], g2 = G[2 * CS], g3 = G[3 * CS];
 #pragma unroll
                 for (int c = 0; c < 3; c++)
                     o[c * CS] = rn_add(rn_add(rn_add(rn_mul(g0, J[c]), rn_mul(g1, J[4 + c])), rn_mul(g2, J[8 + c])),
@@ -234,7 +235,7 @@ element_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, cons
         }
         for (int q = lane; q < QR; q += 32) {
             double v = 0.0;
-            for (int k = 0; k < N; k++) v = rn_add(v, rn_mul(br[q * N + k], fl[k]));
+            for (int k = 0; k < N; k++) v = rn_add(v, rn_mul(brt[k * QR + q], fl[k]));
             fq[q] = v;
         }
         __syncwarp();
@@ -658,7 +659,7 @@ static void elem_launch(const ElemArgs &A, cudaStream_t s) {
     for (int q = 0; q < ElemDims<P>::QK; q++) Wt.wk[q] = A.wk_host[q];
     for (int q = 0; q < ElemDims<P>::QR; q++) Wt.wr[q] = A.wr_host[q];
     element_kernel<P><<<blocks, W * 32, 0, s>>>(A.nelem, A.ndof, A.geo, A.e2l, A.kappa, A.mass, A.f, Wt, A.gk,
-                                                A.br, A.Ke, A.Re, A.status);
+                                                A.br, A.brt, A.Ke, A.Re, A.status);
 }
 
 cudaError_t launch_element_kernel(int p, const ElemArgs &A, cudaStream_t s) {

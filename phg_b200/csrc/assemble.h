@@ -16,7 +16,10 @@ struct ElemArgs {
     const int32_t *elems, *e2l;
     const double *kappa, *f;                 // may be null
     double mass;                             // mass coefficient c (0: stiffness only)
-    const double *gk, *br;                   // element tables (device)
+    // element tables (device): gk = d phi_k / d lambda_c at stiffness point q
+    // as gk[(c * QK + q) * N + k]; br = phi_k at rhs point q as br[q * N + k],
+    // brt the same transposed (brt[k * QR + q])
+    const double *gk, *br, *brt;
     const double *wk_host, *wr_host;         // quadrature weights (host; passed by value)
     double *geo;                             // scratch: nelem * geometry_doubles
     double *Ke, *Re;

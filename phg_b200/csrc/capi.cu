@@ -152,7 +152,7 @@ struct phgGpuSystem_ {
 
     // element tables
     int tab_order = 0;
-    DevBuf<double> gk, br;                 // basis derivatives / values at the points (device)
+    DevBuf<double> gk, br, brt;            // basis derivatives / values at the points (device)
     std::vector<double> wk, wr;            // quadrature weights (passed to the kernel by value)
 
     // assembly buffers
@@ -310,10 +310,21 @@ int upload_tables(phgGpuSystem *s, int p) {
     const ElementTables t = make_tables(p);
     if ((int)t.wk.size() > kElemMaxQK || (int)t.wr.size() > kElemMaxQR)
         return fail(PHG_GPU_ERR_LIMIT, "quadrature rule larger than the element kernel's");
-    CHECK_RC(s->gk.ensure(t.gk.size()));
+    // the kernel reads gk component-major with the basis index fastest, and
+    // br both point-major (the RHS sums) and basis-major (f_h at the points)
+    const int N = t.N, QK = t.nq_k, QR = t.nq_r;
+    std::vector<double> gkc(t.gk.size()), brt(t.br.size());
+    for (int q = 0; q < QK; q++)
+        for (int k = 0; k < N; k++)
+            for (int c = 0; c < 4; c++) gkc[((size_t)c * QK + q) * N + k] = t.gk[((size_t)q * N + k) * 4 + c];
+    for (int q = 0; q < QR; q++)
+        for (int k = 0; k < N; k++) brt[(size_t)k * QR + q] = t.br[(size_t)q * N + k];
+    CHECK_RC(s->gk.ensure(gkc.size()));
     CHECK_RC(s->br.ensure(t.br.size()));
-    CK(cudaMemcpy(s->gk.p, t.gk.data(), t.gk.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CHECK_RC(s->brt.ensure(brt.size()));
+    CK(cudaMemcpy(s->gk.p, gkc.data(), gkc.size() * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(s->br.p, t.br.data(), t.br.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s->brt.p, brt.data(), brt.size() * sizeof(double), cudaMemcpyHostToDevice));
     s->wk = t.wk;
     s->wr = t.wr;
     s->tab_order = p;
@@ -684,7 +695,7 @@ int phgGpuDestroy(phgGpuSystem *s) {
     for (auto *b : bf) b->release();
     s->bint.release();
     s->btick.release();
-    DevBuf<double> *dbufs[] = {&s->verts, &s->gk, &s->br, &s->Ke, &s->Re, &s->kappa, &s->f,
+    DevBuf<double> *dbufs[] = {&s->verts, &s->gk, &s->br, &s->brt, &s->Ke, &s->Re, &s->kappa, &s->f,
                                &s->g, &s->geo, &s->va, &s->bva, &s->rhs, &s->diag, &s->x, &s->r, &s->p, &s->Ap,
                                &s->partials, &s->hist, &s->sums};
     for (auto *b : dbufs) b->release();
@@ -790,7 +801,7 @@ static int element_pass(phgGpuSystem *s, const double *kappa, double mass, const
     ea.nelem = s->nelem; ea.nvert = s->nvert; ea.ndof = ndof;
     ea.verts = s->verts.p; ea.elems = s->elems.p; ea.e2l = s->e2l.p;
     ea.kappa = dk; ea.f = df; ea.mass = mass;
-    ea.gk = s->gk.p; ea.br = s->br.p; ea.wk_host = s->wk.data(); ea.wr_host = s->wr.data();
+    ea.gk = s->gk.p; ea.br = s->br.p; ea.brt = s->brt.p; ea.wk_host = s->wk.data(); ea.wr_host = s->wr.data();
     ea.Ke = s->Ke.p; ea.Re = s->Re.p; ea.geo = s->geo.p; ea.status = s->status.p;
     CK(launch_element_kernel(s->order, ea, s->stream));
     s->launches += 2;
