@@ -219,7 +219,9 @@ int phgGpuSolverPCGMixed(phgGpuSystem *sys, double rtol, double btol,
  * shape it times CSR with 4/8/16/32 lanes per row and SELL-C-sigma (32-row
  * slices, rows sorted by length in 256-row windows) with 2/4/8-fold
  * unrolling, and keeps the fastest.  kind: 0 = CSR (param = lanes per row),
- * 1 = SELL (param = unroll); times_ms (optional, 17 doubles) gets the
+ * 1 = SELL (param = unroll), 2 = q16 (param = 1; the 16-bit-column layout
+ * with FP64 values, a candidate only when every row fits two 65536-column
+ * windows); times_ms (optional, 18 doubles) gets the
  * measured time of each candidate in that order, then the times of the FP32
  * products of the mixed solver (SELL unrolled 4/8/16, pair-SELL -- two
  * consecutive entries per lane -- unrolled 2/4/8, q16 -- four entries per
@@ -251,8 +253,9 @@ int phgGpuTimeSpMV(phgGpuSystem *sys, int fp32, int reps, double *ms_per_launch)
 int phgGpuSpMVBytes(phgGpuSystem *sys, int fp32, int64_t *bytes);
 
 /* Overrides the autotuner for the current matrix shape: kind 0 = CSR with
- * param = 4/8/16/32 lanes per row, kind 1 = SELL with param = 2/4/8
- * (no counterpart in the reference). */
+ * param = 4/8/16/32 lanes per row, kind 1 = SELL with param = 2/4/8, kind 2
+ * = q16 with param = 1 (PHG_GPU_ERR_ARG when a row spans more than two
+ * 65536-column windows) (no counterpart in the reference). */
 int phgGpuSetSpMVPlan(phgGpuSystem *sys, int kind, int param);
 
 /* Number of kernels this system has launched so far (the nodes of captured

@@ -117,7 +117,9 @@ def _np(a, dtype):
     return np.ascontiguousarray(a, dtype=dtype)
 
 
-# FP32 product layouts of the mixed solver, by their C-ABI codes
+# FP64 product layouts (solvers, mat_vec) and FP32 product layouts of the
+# mixed solver, by their C-ABI codes
+LAYOUTS64 = ("csr", "sell", "q16")
 LAYOUTS32 = ("sell", "pair", "q16")
 
 
@@ -231,7 +233,7 @@ class Solver:
         return x, nits, res.value, nupd.value
 
     SPMV_LAYOUTS = (("csr", 4), ("csr", 8), ("csr", 16), ("csr", 32),
-                    ("sell", 2), ("sell", 4), ("sell", 8))
+                    ("sell", 2), ("sell", 4), ("sell", 8), ("q16", 1))
 
     def time_spmv(self, fp32=False, reps=50):
         """Average ms of one SpMV launch (chosen layout; FP32 values if fp32)."""
@@ -247,7 +249,7 @@ class Solver:
         return b.value
 
     def set_spmv_plan(self, layout, param):
-        _check(lib().phgGpuSetSpMVPlan(self._h, 0 if layout == "csr" else 1, int(param)))
+        _check(lib().phgGpuSetSpMVPlan(self._h, LAYOUTS64.index(layout), int(param)))
 
     def set_spmv_plan32(self, layout, unroll):
         """Forces the mixed solver's FP32 product: layout "sell", "pair" or
@@ -289,7 +291,7 @@ class Solver:
         kind, param = C.c_int(), C.c_int()
         times = np.zeros(24)
         nc = _check(lib().phgGpuGetSpMVPlan(self._h, C.byref(kind), C.byref(param), _ptr(times)))
-        names = ["csr4", "csr8", "csr16", "csr32", "sell_u2", "sell_u4", "sell_u8"][:nc]
+        names = ["csr4", "csr8", "csr16", "csr32", "sell_u2", "sell_u4", "sell_u8", "q16"][:nc]
         info = dict(zip(names, times[:nc].tolist()))
         names32 = ("fp32_sell_u4", "fp32_sell_u8", "fp32_sell_u16", "fp32_pair_u2", "fp32_pair_u4",
                    "fp32_pair_u8", "fp32_q16_u1", "fp32_q16_u2")
@@ -298,7 +300,7 @@ class Solver:
         k = nc + len(names32)
         info["fp32_unroll"] = int(times[k])
         info["fp32_layout"] = LAYOUTS32[int(times[k + 1])]
-        return ("csr" if kind.value == 0 else "sell"), param.value, info
+        return LAYOUTS64[kind.value], param.value, info
 
     def launch_count(self):
         c = _I64()

@@ -118,11 +118,13 @@ __global__ void diag_kernel(int64_t n, const int32_t *rp, const int32_t *ci, con
 constexpr int kGraphChunk = 16;
 
 // SpMV autotuner candidates: CSR with 4/8/16/32 lanes per row, SELL-C-sigma
-// with the inner loop unrolled 2/4/8 times.
-constexpr int kTuneCandidates = 7;
+// with the inner loop unrolled 2/4/8 times, q16 (FP64 values; only for
+// matrices whose rows fit two 65536-column windows).
+constexpr int kTuneCandidates = 8;
 constexpr int kTune32 = 8;   // FP32 candidates of the mixed solver
-const int kTuneKind[kTuneCandidates] = {SPMV_CSR, SPMV_CSR, SPMV_CSR, SPMV_CSR, SPMV_SELL, SPMV_SELL, SPMV_SELL};
-const int kTuneParam[kTuneCandidates] = {4, 8, 16, 32, 2, 4, 8};
+const int kTuneKind[kTuneCandidates] = {SPMV_CSR,  SPMV_CSR,  SPMV_CSR,  SPMV_CSR,
+                                        SPMV_SELL, SPMV_SELL, SPMV_SELL, SPMV_Q16};
+const int kTuneParam[kTuneCandidates] = {4, 8, 16, 32, 2, 4, 8, 1};
 
 }  // namespace
 
@@ -561,14 +563,35 @@ int tune_spmv32(phgGpuSystem *s) {
     return PHG_GPU_OK;
 }
 
+// The layout arrays an FP64 plan's kernels read, for a graph's key: a graph
+// is captured again when a reallocation moved any of them.
+void plan_key(phgGpuSystem *s, phgGpuSystem_::GraphKey &key) {
+    if (s->plan.kind == SPMV_CSR) {
+        key.va = s->va.p;
+        const void *e[8] = {s->rp.p, s->ci.p, nullptr, nullptr, nullptr, nullptr, nullptr, s->partials.p};
+        memcpy(key.extra, e, sizeof(e));
+    } else if (s->plan.kind == SPMV_SELL) {
+        key.va = s->sell_vals.p;
+        const void *e[8] = {s->sell_cols.p, s->sell_perm.p, s->sell_len.p, s->sell_sptr.p,
+                            nullptr, nullptr, nullptr, s->partials.p};
+        memcpy(key.extra, e, sizeof(e));
+    } else {
+        key.va = s->q16_v64.p;
+        const void *e[8] = {s->q16_cols.p, s->q16_perm.p, s->q16_len.p, s->q16_split.p,
+                            s->q16_b0.p, s->q16_b1.p, s->q16_sptr.p, s->partials.p};
+        memcpy(key.extra, e, sizeof(e));
+    }
+}
+
 SpmvPlan make_plan(phgGpuSystem *s, int kind, int param) {
     SpmvPlan P;
     P.kind = kind;
     P.lpr = kind == SPMV_CSR ? param : 8;
-    P.unroll = kind == SPMV_SELL ? param : 4;
+    P.unroll = kind == SPMV_CSR ? 4 : param;
     P.csr = CsrView{s->n, s->rp.p, s->ci.p, s->va.p};
     P.sell = SellView{s->n, sell_positions(s->n) / 32, s->sell_perm.p, s->sell_len.p, s->sell_sptr.p,
                       s->sell_cols.p, s->sell_vals.p, s->sell_vals32.p};
+    P.q16 = q16_view(s);
     return P;
 }
 
@@ -579,10 +602,20 @@ SpmvPlan make_plan(phgGpuSystem *s, int kind, int param) {
 int tune_spmv(phgGpuSystem *s, bool build_layout = true) {
     if (s->tuned && s->tuned_n == s->n && s->tuned_nnz == s->nnz) {
         if (build_layout && s->plan.kind == SPMV_SELL) CHECK_RC(ensure_sell(s));
-        s->plan = make_plan(s, s->plan.kind, s->plan.kind == SPMV_CSR ? s->plan.lpr : s->plan.unroll);
-        return PHG_GPU_OK;
+        // a q16 plan is checked against every new matrix (a matrix of the
+        // same shape may not fit it); it is then timed again without q16
+        bool keep = true;
+        if (s->plan.kind == SPMV_Q16) {
+            CHECK_RC(ensure_q16(s));
+            keep = s->q16_fits;
+        }
+        if (keep) {
+            s->plan = make_plan(s, s->plan.kind, s->plan.kind == SPMV_CSR ? s->plan.lpr : s->plan.unroll);
+            return PHG_GPU_OK;
+        }
     }
     CHECK_RC(ensure_sell(s));
+    CHECK_RC(ensure_q16(s));
     CHECK_RC(solver_buffers(s));
     cudaEvent_t a, b;
     CK(cudaEventCreate(&a));
@@ -590,6 +623,8 @@ int tune_spmv(phgGpuSystem *s, bool build_layout = true) {
     int best = 0;
     const int reps = 5;
     for (int c = 0; c < kTuneCandidates; c++) {
+        s->tune_ms[c] = 0.0;
+        if (kTuneKind[c] == SPMV_Q16 && !s->q16_fits) continue;
         const SpmvPlan P = make_plan(s, kTuneKind[c], kTuneParam[c]);
         for (int i = 0; i < 2; i++) CK(launch_spmv_plan(P, s->rhs.p, s->Ap.p, s->stream));
         CK(cudaEventRecord(a, s->stream));
@@ -600,7 +635,7 @@ int tune_spmv(phgGpuSystem *s, bool build_layout = true) {
         CK(cudaEventElapsedTime(&ms, a, b));
         s->tune_ms[c] = ms / reps;
         s->launches += 2 + reps;
-        if (s->tune_ms[c] < s->tune_ms[best]) best = c;
+        if (s->tune_ms[c] < s->tune_ms[best]) best = c;   // candidate 0 (CSR) is always timed
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
@@ -1016,6 +1051,7 @@ int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol,
     CK(cudaMemsetAsync(s->ticket.p, 0, sizeof(unsigned) * kRedTickets, s->stream));
     CHECK_RC(tune_spmv32(s));   // builds the chosen FP32 layout for this matrix
     const int unroll = s->unroll32;
+    if (s->plan.kind == SPMV_Q16) CHECK_RC(ensure_q16(s));   // the FP64 plan's layout (checked by tune_spmv)
     const bool q16 = s->kind32 == 2;
     // FP64 products (residuals): the q16 layout's FP64 values, or the FP64
     // plan (whose SELL arrays the kinds 0 and 1 have built)
@@ -1182,6 +1218,12 @@ int phgGpuSetSpMVPlan(phgGpuSystem *s, int kind, int param) {
     if (c == kTuneCandidates) return fail(PHG_GPU_ERR_ARG, "no SpMV layout (%d, %d)", kind, param);
     CHECK_RC(set_device(s));
     if (kind == SPMV_SELL) CHECK_RC(ensure_sell(s));
+    if (kind == SPMV_Q16) {
+        CHECK_RC(ensure_q16(s));
+        if (!s->q16_fits)
+            return fail(PHG_GPU_ERR_ARG, "the q16 layout does not fit this matrix: a row spans more than two "
+                        "65536-column windows");
+    }
     s->plan = make_plan(s, kind, param);
     s->tuned = true;
     s->tuned_n = s->n;
@@ -1236,6 +1278,8 @@ int phgGpuSpMVBytes(phgGpuSystem *s, int fp32, int64_t *bytes) {
         else *bytes = 8 * s->sell_total + 6 * npos + sl + vec;
     } else if (s->plan.kind == SPMV_SELL) {
         *bytes = 12 * s->sell_total + 6 * npos + sl + vec;
+    } else if (s->plan.kind == SPMV_Q16) {
+        *bytes = 10 * s->q16_total + 16 * npos + sl + vec;
     } else {
         *bytes = 12 * s->nnz + 4 * (n + 1) + vec;
     }
@@ -1306,7 +1350,7 @@ int pcg_core(phgGpuSystem *s, const double *drhs, double rtol, double btol, doub
     phgGpuSystem_::GraphKey key{};
     key.x = B.x; key.r = B.r; key.p = B.p; key.Ap = B.Ap; key.D = B.D; key.hist = dhist;
     key.n = n; key.lpr = s->plan.kind * 100 + s->plan.lpr * 10 + s->plan.unroll; key.s = s->stream;
-    key.va = s->plan.kind == SPMV_CSR ? (const void *)s->va.p : (const void *)s->sell_vals.p;
+    plan_key(s, key);
     if (s->graph == nullptr || !(s->gkey == key)) {
         if (s->graph != nullptr) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; }
         cudaGraph_t gr;
@@ -1391,7 +1435,7 @@ int bicg_core(phgGpuSystem *s, double rtol, double btol, double atol, int maxit,
     phgGpuSystem_::GraphKey key{};
     key.x = B.x; key.r = B.rg; key.p = B.rh; key.D = B.D; key.hist = dhist;
     key.n = n; key.lpr = s->plan.kind * 100 + s->plan.lpr * 10 + s->plan.unroll; key.s = s->stream;
-    key.va = s->plan.kind == SPMV_CSR ? (const void *)s->va.p : (const void *)s->sell_vals.p;
+    plan_key(s, key);
     if (s->graph_bicg == nullptr || !(s->gkey_bicg == key)) {
         if (s->graph_bicg != nullptr) { cudaGraphExecDestroy(s->graph_bicg); s->graph_bicg = nullptr; }
         cudaGraph_t gr;
@@ -1513,7 +1557,7 @@ int phgGpuSolverGMRES(phgGpuSystem *s, int restart, double rtol, double btol, do
     phgGpuSystem_::GraphKey key{};
     key.x = B.x; key.r = B.z; key.p = B.V; key.D = B.D; key.Ap = B.st;
     key.n = n * 100 + restart; key.lpr = s->plan.kind * 100 + s->plan.lpr * 10 + s->plan.unroll; key.s = s->stream;
-    key.va = s->plan.kind == SPMV_CSR ? (const void *)s->va.p : (const void *)s->sell_vals.p;
+    plan_key(s, key);
     if (s->graph_gmres == nullptr || !(s->gkey_gmres == key)) {
         if (s->graph_gmres != nullptr) { cudaGraphExecDestroy(s->graph_gmres); s->graph_gmres = nullptr; }
         cudaGraph_t gr;

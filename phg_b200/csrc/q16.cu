@@ -8,6 +8,7 @@
 // bytes of offsets per step.
 #include "common.cuh"
 #include "pcg_final.cuh"
+#include "q16.cuh"
 #include "q16.h"
 #include "reduce.cuh"
 
@@ -108,11 +109,6 @@ q16_fill_kernel(int64_t npos, const int32_t *__restrict__ rp, const int32_t *__r
     }
 }
 
-// Column of entry j of a lane's row.
-__device__ __forceinline__ int32_t q16_col(int j, int sp, int32_t b0, int32_t b1, unsigned off) {
-    return (j < sp ? b0 : b1) + (int32_t)off;
-}
-
 // FP32 product; with DOT also p.Ap (x = p) and alpha (pcg_pap_final).
 template <bool DOT, int U>
 __global__ void __launch_bounds__(kVecThreads, kResidentBlocks)
@@ -161,40 +157,28 @@ q16_spmv32_kernel(const Q16View Q, const float *__restrict__ x, float *__restric
     if (grid_sum2(dot, dummy, partials, st->ticket)) pcg_pap_final(dot, st);
 }
 
-// FP64 row sums of the layout's FP64 values against an FP32 (YT = float) or
-// FP64 vector: acc = sum_j a_ij x_j for the lane's row.
-template <typename XT>
-__device__ __forceinline__ double q16_row64(const Q16View &Q, int64_t s, int lane, int l, int sp, int32_t b0,
-                                            int32_t b1, const XT *__restrict__ x) {
-    const int wq = (__shfl_sync(0xffffffffu, l, 0) + 3) >> 2;
-    const uint2 *cp = reinterpret_cast<const uint2 *>(Q.cols + Q.sptr[s]) + lane;
-    const double2 *vp = reinterpret_cast<const double2 *>(Q.vals64 + Q.sptr[s]) + 2 * lane;
-    double acc = 0.0;
-    for (int jq = 0; jq < wq; jq++) {
-        const bool ok = 4 * jq < l;
-        const uint2 c = ok ? __ldcs(cp + 32 * jq) : make_uint2(0u, 0u);
-        const double2 v0 = ok ? __ldcs(vp + 64 * jq) : make_double2(0.0, 0.0);
-        const double2 v1 = ok ? __ldcs(vp + 64 * jq + 1) : make_double2(0.0, 0.0);
-        const int j = 4 * jq;
-        if (j < l) acc += v0.x * (double)__ldg(&x[q16_col(j, sp, b0, b1, c.x & 0xffffu)]);
-        if (j + 1 < l) acc += v0.y * (double)__ldg(&x[q16_col(j + 1, sp, b0, b1, c.x >> 16)]);
-        if (j + 2 < l) acc += v1.x * (double)__ldg(&x[q16_col(j + 2, sp, b0, b1, c.y & 0xffffu)]);
-        if (j + 3 < l) acc += v1.y * (double)__ldg(&x[q16_col(j + 3, sp, b0, b1, c.y >> 16)]);
-    }
-    return acc;
-}
-
+// FP64 product; with DOT also p.Ap (x = p) and alpha, for the FP64 PCG.
+template <bool DOT>
 __global__ void __launch_bounds__(kVecThreads, kResidentBlocks)
-q16_spmv64_kernel(const Q16View Q, const double *__restrict__ x, double *__restrict__ y) {
+q16_spmv64_kernel(const Q16View Q, const double *__restrict__ x, double *__restrict__ y, double *partials,
+                  PcgState *st) {
+    if (DOT && st->done) return;
+    if (DOT) grid_sum_init();
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t)blockIdx.x * kVecThreads + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * kVecThreads) >> 5;
+    double dot = 0.0, dummy = 0.0;
     for (int64_t s = warp; s < Q.nslices; s += nwarps) {
         const int64_t pos = s * 32 + lane;
         const int32_t row = Q.perm[pos];
         const double acc = q16_row64(Q, s, lane, Q.len[pos], Q.split[pos], Q.base0[pos], Q.base1[pos], x);
-        if (row >= 0) y[row] = acc;
+        if (row >= 0) {
+            y[row] = acc;
+            if (DOT) dot += x[row] * acc;
+        }
     }
+    if (!DOT) return;
+    if (grid_sum2(dot, dummy, partials, st->ticket)) pcg_pap_final(dot, st);
 }
 
 // Reliable update of the mixed solver on this layout (FP64 values): x += y,
@@ -267,7 +251,13 @@ cudaError_t launch_q16_spmv32_dot(const Q16View &Q, int unroll, const float *x, 
 }
 
 cudaError_t launch_q16_spmv64(const Q16View &Q, const double *x, double *y, cudaStream_t s) {
-    q16_spmv64_kernel<<<vec_blocks(Q.nslices * 32), kVecThreads, 0, s>>>(Q, x, y);
+    q16_spmv64_kernel<false><<<vec_blocks(Q.nslices * 32), kVecThreads, 0, s>>>(Q, x, y, nullptr, nullptr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_q16_spmv64_dot(const Q16View &Q, const double *x, double *y, double *partials, PcgState *st,
+                                  cudaStream_t s) {
+    q16_spmv64_kernel<true><<<vec_blocks(Q.nslices * 32), kVecThreads, 0, s>>>(Q, x, y, partials, st);
     return cudaGetLastError();
 }
 

@@ -4,27 +4,6 @@
 
 namespace phgb {
 
-// Same slices as SELL-C-sigma (C = 32, sigma = 256), stored widest first.
-// Each lane holds four consecutive entries of its row per step (one 16-byte
-// load of FP32 values, one 8-byte load of four 16-bit column offsets), so an
-// entry costs 6 bytes in the FP32 product instead of 8.  A row's entries are
-// split into two column windows of 65536: entries [0, split) are offsets
-// from base0 (the row's smallest column), the rest from base1 (the smallest
-// column outside the first window).  Rows of Lagrange P1-P3 matrices numbered
-// vertices first, then edges and faces, fit; a matrix with a row that does
-// not fit does not get this layout.
-struct Q16View {
-    int64_t nslices;
-    const int32_t *sptr;       // stored slice offsets in entries (nslices + 1), multiples of 128
-    const int32_t *perm;       // row of each stored position, -1 for padding
-    const uint16_t *len;       // its length
-    const uint16_t *split;     // entries of the first window
-    const int32_t *base0, *base1;
-    const uint16_t *cols;      // column offsets
-    const float *vals32;       // FP32 values (mixed solver's product)
-    const double *vals64;      // FP64 values (reliable updates, residuals)
-};
-
 // Writable pointers of the layout, for its construction.
 struct Q16Out {
     const int32_t *sptr;
@@ -50,6 +29,10 @@ cudaError_t launch_q16_fill(int64_t nslices, const int32_t *rp, const int32_t *c
 // FP32 product y = A x (unroll 1 or 2 steps), FP64 product y = A x.
 cudaError_t launch_q16_spmv32(const Q16View &Q, int unroll, const float *x, float *y, cudaStream_t s);
 cudaError_t launch_q16_spmv64(const Q16View &Q, const double *x, double *y, cudaStream_t s);
+
+// The FP64 product computing p.Ap and alpha (x = p), for the FP64 PCG.
+cudaError_t launch_q16_spmv64_dot(const Q16View &Q, const double *x, double *y, double *partials, PcgState *st,
+                                  cudaStream_t s);
 
 // The same FP32 product computing p.Ap and alpha (x = p); the mixed
 // solver's reliable update on this layout.

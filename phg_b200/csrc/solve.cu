@@ -405,6 +405,7 @@ static void plan_spmv(const SpmvPlan &P, const VT *vals, const VT *x, VT *y, dou
 }
 
 cudaError_t launch_spmv_plan(const SpmvPlan &P, const double *x, double *y, cudaStream_t s) {
+    if (P.kind == SPMV_Q16) return launch_q16_spmv64(P.q16, x, y, s);
     plan_spmv<false, double>(P, P.kind == SPMV_CSR ? P.csr.va : P.sell.vals, x, y, nullptr, nullptr, s);
     return cudaGetLastError();
 }
@@ -412,7 +413,12 @@ cudaError_t launch_spmv_plan(const SpmvPlan &P, const double *x, double *y, cuda
 cudaError_t launch_pcg_iteration_plan(const PcgBuffers &B, const SpmvPlan &P, cudaStream_t s) {
     const int vb = vvec_blocks(B.A.n, 2);
     pcg_dir_kernel<double><<<vb, kVecThreads, 0, s>>>(B.A.n, B.r, B.D, B.p, B.st);
-    plan_spmv<true, double>(P, P.kind == SPMV_CSR ? P.csr.va : P.sell.vals, B.p, B.Ap, B.partials, B.st, s);
+    if (P.kind == SPMV_Q16) {
+        const cudaError_t e = launch_q16_spmv64_dot(P.q16, B.p, B.Ap, B.partials, B.st, s);
+        if (e != cudaSuccess) return e;
+    } else {
+        plan_spmv<true, double>(P, P.kind == SPMV_CSR ? P.csr.va : P.sell.vals, B.p, B.Ap, B.partials, B.st, s);
+    }
     pcg_update_kernel<double, double><<<vb, kVecThreads, 0, s>>>(B.A.n, B.x, B.r, B.p, B.Ap, B.D, B.partials,
                                                                 B.st, B.hist);
     return cudaGetLastError();

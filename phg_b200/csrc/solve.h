@@ -45,7 +45,9 @@ struct PcgBuffers {
 
 // SpMV layouts: CSR with `lpr` lanes per row, or SELL-C-sigma (C = 32,
 // sigma = 256) with the inner loop unrolled `unroll` times.
-enum { SPMV_CSR = 0, SPMV_SELL = 1 };
+// SPMV_Q16: the 16-bit-column layout with FP64 values (FP64 products read
+// 10 bytes per stored entry instead of 12).
+enum { SPMV_CSR = 0, SPMV_SELL = 1, SPMV_Q16 = 2 };
 
 struct SellView {
     int64_t n, nslices;
@@ -66,10 +68,32 @@ struct Sell2View {
     const uint16_t *len2;     // its length
 };
 
+// The 16-bit-column layout ("q16", q16.cu): the same slices as SELL-C-sigma (C = 32, sigma = 256), stored widest first.
+// Each lane holds four consecutive entries of its row per step (one 16-byte
+// load of FP32 values, one 8-byte load of four 16-bit column offsets), so an
+// entry costs 6 bytes in the FP32 product instead of 8.  A row's entries are
+// split into two column windows of 65536: entries [0, split) are offsets
+// from base0 (the row's smallest column), the rest from base1 (the smallest
+// column outside the first window).  Rows of Lagrange P1-P3 matrices numbered
+// vertices first, then edges and faces, fit; a matrix with a row that does
+// not fit does not get this layout.
+struct Q16View {
+    int64_t nslices;
+    const int32_t *sptr;       // stored slice offsets in entries (nslices + 1), multiples of 128
+    const int32_t *perm;       // row of each stored position, -1 for padding
+    const uint16_t *len;       // its length
+    const uint16_t *split;     // entries of the first window
+    const int32_t *base0, *base1;
+    const uint16_t *cols;      // column offsets
+    const float *vals32;       // FP32 values (mixed solver's product)
+    const double *vals64;      // FP64 values (reliable updates, residuals)
+};
+
 struct SpmvPlan {
     int kind = SPMV_CSR, lpr = 8, unroll = 4;
     CsrView csr{};
     SellView sell{};
+    Q16View q16{};
 };
 
 // State of the mixed-precision PCG (FP32 Krylov vectors, FP64 x and

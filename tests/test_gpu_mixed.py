@@ -22,7 +22,7 @@ def system(pb, p, m, kappa_seed=None):
 
 
 @pytest.mark.parametrize("layout,param", [("csr", 4), ("csr", 8), ("csr", 16), ("csr", 32),
-                                          ("sell", 2), ("sell", 4), ("sell", 8)])
+                                          ("sell", 2), ("sell", 4), ("sell", 8), ("q16", 1)])
 def test_every_spmv_layout_matches_oracle(gpu, oracle, layout, param):
     for name in ("p2_m6_sine", "p3_m3_kappa", "p1_m5_kappa"):
         G = load_golden(name)
@@ -175,3 +175,30 @@ def test_q16_layout_follows_the_matrix(gpu, oracle):
     x, nits, res, _ = s.solve_pcg_mixed(rtol=1e-8)
     assert np.linalg.norm(rhs - oracle.spmv(ptr, cols, vals * 2.0, x)) <= 1e-8 * np.linalg.norm(rhs) * (1 + 1e-9)
     s.close()
+
+
+@pytest.mark.parametrize("layout,param", [("csr", 8), ("sell", 4), ("q16", 1)])
+def test_krylov_solvers_on_each_fp64_layout(gpu, oracle, layout, param):
+    """PCG, BiCGstab and GMRES_r (their products with epilogues) on each FP64
+    layout forced for a P2 system with variable kappa: the FP64 residual,
+    recomputed by the oracle, meets the stopping rule, and the iteration
+    counts agree with the CSR layout's within a few iterations (the layouts
+    differ only in the summation order)."""
+    s = system(gpu, 2, 12, kappa_seed=4)
+    ptr, cols, vals = s.get_matrix()
+    rhs = s.get_rhs()
+    nb = np.linalg.norm(rhs)
+    its = {}
+    for lay, par in (("csr", 8), (layout, param)):
+        s.set_spmv_plan(lay, par)
+        x, n_pcg, _ = s.solve_pcg(rtol=1e-9, btol=0.0, atol=0.0)
+        assert np.linalg.norm(rhs - oracle.spmv(ptr, cols, vals, x)) <= 1e-9 * nb * 1.01, lay
+        x, n_bicg, _ = s.solve_bicgstab(rtol=1e-9, btol=0.0, atol=0.0)
+        assert np.linalg.norm(rhs - oracle.spmv(ptr, cols, vals, x)) <= 1e-8 * nb, lay
+        x, n_gm, _ = s.solve_gmres(restart=30, rtol=1e-9, btol=0.0, atol=0.0)
+        assert np.linalg.norm(rhs - oracle.spmv(ptr, cols, vals, x)) <= 1e-8 * nb, lay
+        its[lay] = (n_pcg, n_bicg, n_gm)
+        assert s.spmv_plan()[0] == lay
+    s.close()
+    for a, b in zip(its["csr"], its[layout]):
+        assert abs(a - b) <= max(3, a // 20), its
