@@ -24,12 +24,12 @@ __global__ void q16_sizes_kernel(int64_t nslices, const uint16_t *__restrict__ l
         size[k] = 128 * ((len[(int64_t)order[k] * 32] + 3) / 4);
 }
 
-// One warp per stored position: the warp reads the row's CSR entries 32 at a
-// time (coalesced) in three rounds: the smallest column (base0); the size of
-// the first window and the smallest and largest column outside it; the
-// entries, first-window entries first, each window in CSR order (ranks from
-// ballots).  Positions past the row's length up to the slice's width
-// (rounded up to 4) are zero.
+// One thread per stored position (the 32 positions of a slice are a warp's
+// lanes).  Three passes over the row's CSR entries: the smallest column
+// (base0); the size of the first window and the smallest and largest column
+// outside it; the entries, first-window entries first, each window in CSR
+// order.  Positions past the row's length up to the slice's width (rounded
+// up to 4) are zero.
 __global__ void __launch_bounds__(kVecThreads, kResidentBlocks)
 q16_fill_kernel(int64_t npos, const int32_t *__restrict__ rp, const int32_t *__restrict__ ci,
                 const double *__restrict__ va, const int32_t *__restrict__ sell_perm,
@@ -37,75 +37,59 @@ q16_fill_kernel(int64_t npos, const int32_t *__restrict__ rp, const int32_t *__r
                 const int32_t *__restrict__ sptr, int32_t *__restrict__ perm, uint16_t *__restrict__ len,
                 uint16_t *__restrict__ split, int32_t *__restrict__ base0, int32_t *__restrict__ base1,
                 uint16_t *__restrict__ cols, float *__restrict__ vals32, double *__restrict__ vals64, int *nofit) {
-    const int lane = threadIdx.x & 31;
-    const unsigned lt = (1u << lane) - 1u;
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t pos = warp; pos < npos; pos += nwarps) {
+    for (int64_t pos = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pos < npos;
+         pos += (int64_t)gridDim.x * blockDim.x) {
         const int64_t k = pos >> 5;
-        const int pl = (int)(pos & 31);   // the row's lane in its slice
+        const int lane = (int)(pos & 31);
         const int64_t src0 = (int64_t)order[k] * 32;
-        const int32_t row = sell_perm[src0 + pl];
-        const int l = sell_len[src0 + pl];
+        const int32_t row = sell_perm[src0 + lane];
+        const int l = sell_len[src0 + lane];
         const int wq = (sell_len[src0] + 3) & ~3;   // SELL slices are sorted: position 0 is the widest
-        const int64_t b = (int64_t)sptr[k] + 4 * pl;
+        const int64_t b = (int64_t)sptr[k] + 4 * lane;
         int32_t b0 = 0, b1 = 0;
-        int sp = 0;
-        const int lr = row >= 0 ? l : 0;
-        if (lr > 0) {
+        int sp = 0, j = 0;
+        if (row >= 0 && l > 0) {
             const int64_t r0 = rp[row];
-            int32_t mn = INT_MAX;
-            for (int t = lane; t < lr; t += 32) mn = min(mn, ci[r0 + t]);
-            b0 = __reduce_min_sync(0xffffffffu, mn);
-            int32_t lo = INT_MAX, hi = -1;
-            for (int t0 = 0; t0 < lr; t0 += 32) {
-                const int t = t0 + lane;
-                const int32_t c = t < lr ? ci[r0 + t] : b0;
-                const bool w0 = c - b0 < 65536;
-                sp += __popc(__ballot_sync(0xffffffffu, t < lr && w0));
-                if (t < lr && !w0) {
-                    lo = min(lo, c);
+            b0 = INT_MAX;
+            for (int t = 0; t < l; t++) b0 = min(b0, ci[r0 + t]);
+            b1 = INT_MAX;
+            int32_t hi = -1;
+            for (int t = 0; t < l; t++) {
+                const int32_t c = ci[r0 + t];
+                if (c - b0 < 65536) {
+                    sp++;
+                } else {
+                    b1 = min(b1, c);
                     hi = max(hi, c);
                 }
             }
-            lo = __reduce_min_sync(0xffffffffu, lo);
-            hi = __reduce_max_sync(0xffffffffu, hi);
-            b1 = hi < 0 ? b0 : lo;
+            if (hi < 0) b1 = b0;
             const bool fits = hi < 0 || hi - b1 < 65536;
-            if (!fits && lane == 0) atomicExch(nofit, 1);
+            if (!fits) atomicExch(nofit, 1);
             int j0 = 0, j1 = sp;
-            for (int t0 = 0; t0 < lr; t0 += 32) {
-                const int t = t0 + lane;
-                const bool valid = t < lr;
-                const int32_t c = valid ? ci[r0 + t] : b0;
+            for (int t = 0; t < l; t++) {
+                const int32_t c = ci[r0 + t];
                 const bool w0 = c - b0 < 65536;
-                const unsigned m0 = __ballot_sync(0xffffffffu, valid && w0);
-                const unsigned m1 = __ballot_sync(0xffffffffu, valid && !w0);
-                if (valid) {
-                    const int jj = w0 ? j0 + __popc(m0 & lt) : j1 + __popc(m1 & lt);
-                    const int64_t idx = b + (int64_t)(jj >> 2) * 128 + (jj & 3);
-                    cols[idx] = fits ? (uint16_t)(c - (w0 ? b0 : b1)) : (uint16_t)0;
-                    const double v = va[r0 + t];
-                    vals64[idx] = v;
-                    vals32[idx] = (float)v;
-                }
-                j0 += __popc(m0);
-                j1 += __popc(m1);
+                const int jj = w0 ? j0++ : j1++;
+                const int64_t idx = b + (int64_t)(jj >> 2) * 128 + (jj & 3);
+                cols[idx] = fits ? (uint16_t)(c - (w0 ? b0 : b1)) : (uint16_t)0;
+                const double v = va[r0 + t];
+                vals64[idx] = v;
+                vals32[idx] = (float)v;
             }
+            j = l;
         }
-        for (int j = lr + lane; j < wq; j += 32) {
+        for (; j < wq; j++) {
             const int64_t idx = b + (int64_t)(j >> 2) * 128 + (j & 3);
             cols[idx] = 0;
             vals64[idx] = 0.0;
             vals32[idx] = 0.0f;
         }
-        if (lane == 0) {
-            perm[pos] = row;
-            len[pos] = (uint16_t)l;
-            split[pos] = (uint16_t)sp;
-            base0[pos] = b0;
-            base1[pos] = b1;
-        }
+        perm[pos] = row;
+        len[pos] = (uint16_t)l;
+        split[pos] = (uint16_t)sp;
+        base0[pos] = b0;
+        base1[pos] = b1;
     }
 }
 
@@ -225,7 +209,7 @@ cudaError_t launch_q16_fill(int64_t nslices, const int32_t *rp, const int32_t *c
                             const int32_t *sell_perm, const uint16_t *sell_len, const int32_t *order,
                             const Q16Out &O, int *nofit, cudaStream_t s) {
     const int64_t npos = nslices * 32;
-    q16_fill_kernel<<<vec_blocks(npos * 32), kVecThreads, 0, s>>>(npos, rp, ci, va, sell_perm, sell_len, order, O.sptr,
+    q16_fill_kernel<<<vec_blocks(npos), kVecThreads, 0, s>>>(npos, rp, ci, va, sell_perm, sell_len, order, O.sptr,
                                                              O.perm, O.len, O.split, O.base0, O.base1, O.cols,
                                                              O.vals32, O.vals64, nofit);
     return cudaGetLastError();
