@@ -307,7 +307,9 @@ def impl_ours(args):
     with torch.cuda.stream(stream):
         step(pinned, x_host, True)
     e2e_ms, _, _ = timed(pinned, x_host, max(1, args.steps), True)
-    h2d = sum(t.numel() * t.element_size() for t in pinned.values())
+    # inputs of the step, plus the initial guess the solver reads from x
+    # (the solution comes back through the same host array)
+    h2d = sum(t.numel() * t.element_size() for t in pinned.values()) + x_host.numel() * x_host.element_size()
     d2h = x_host.numel() * x_host.element_size()
 
     # accuracy: mixed vs FP64 solution, both vs the exact sine solution
