@@ -222,6 +222,7 @@ struct phgGpuSystem_ {
     DevBuf<int> q16_nofit;
     int *h_nofit = nullptr;
     int64_t sell2_total = 0, q16_total = 0;   // stored entries (padding included)
+    int64_t pair_entries = 0, q16_entries = 0; // the same, known from the slice widths
     double tune_ms[kTuneCandidates] = {};
 
     // mixed-precision solver
@@ -411,6 +412,13 @@ int ensure_slice_order(phgGpuSystem *s) {
     for (int64_t i = 0; i < nsl; i++) start[65535 - w[i] + 1]++;
     for (int b = 1; b <= 65536; b++) start[b] += start[b - 1];
     for (int64_t i = 0; i < nsl; i++) order[start[65535 - w[i]]++] = (int32_t)i;
+    // stored entries of the pair and q16 layouts, exactly, in 64 bits
+    s->pair_entries = 0;
+    s->q16_entries = 0;
+    for (int64_t i = 0; i < nsl; i++) {
+        s->pair_entries += 64 * (((int64_t)w[i] + 1) / 2);
+        s->q16_entries += 128 * (((int64_t)w[i] + 3) / 4);
+    }
     CK(cudaMemcpyAsync(s->sell2_order.p, order.data(), sizeof(int32_t) * nsl, cudaMemcpyHostToDevice, s->stream));
     CK(cudaStreamSynchronize(s->stream));
     s->order_valid = true;
@@ -431,7 +439,8 @@ int ensure_sell2(phgGpuSystem *s) {
     int32_t total = 0;
     CK(cudaMemcpyAsync(&total, s->sell2_sptr.p + nsl, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
-    if (total < 0) return fail(PHG_GPU_ERR_LIMIT, "pair SELL layout larger than 2^31 entries");
+    if (s->pair_entries >= (int64_t)INT32_MAX || (int64_t)total != s->pair_entries)
+        return fail(PHG_GPU_ERR_LIMIT, "pair SELL layout larger than 2^31 entries");
     CHECK_RC(s->sell2_cols.ensure((size_t)total));
     CHECK_RC(s->sell2_vals.ensure((size_t)total));
     CHECK_RC(s->sell2_perm.ensure((size_t)nsl * 32));
@@ -450,6 +459,20 @@ int ensure_q16(phgGpuSystem *s) {
     if (s->q16_valid) return PHG_GPU_OK;
     CHECK_RC(ensure_slice_order(s));
     const int64_t nsl = sell_positions(s->n) / 32, npos = nsl * 32;
+    {   // the layout is an optimisation: without room for it (32-bit offsets,
+        // or 90% of the free device memory) it is simply not offered
+        auto grow = [](int64_t need, size_t cap, int64_t bytes) { return need > (int64_t)cap ? (need - (int64_t)cap) * bytes : 0; };
+        const int64_t e = s->q16_entries;
+        const int64_t extra = grow(e, s->q16_cols.cap, 2) + grow(e, s->q16_v32.cap, 4) + grow(e, s->q16_v64.cap, 8) +
+                              grow(npos, s->q16_perm.cap, 16);
+        size_t free_b = 0, total_b = 0;
+        CK(cudaMemGetInfo(&free_b, &total_b));
+        if (e >= (int64_t)INT32_MAX || extra > (int64_t)(0.9 * (double)free_b)) {
+            s->q16_valid = true;
+            s->q16_fits = false;
+            return PHG_GPU_OK;
+        }
+    }
     CHECK_RC(s->q16_ssz.ensure((size_t)nsl));
     CHECK_RC(s->q16_sptr.ensure((size_t)nsl + 1));
     CHECK_RC(s->scan_ws.ensure((size_t)scan_workspace_elems(nsl)));
@@ -460,7 +483,7 @@ int ensure_q16(phgGpuSystem *s) {
     int32_t total = 0;
     CK(cudaMemcpyAsync(&total, s->q16_sptr.p + nsl, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
-    if (total < 0) return fail(PHG_GPU_ERR_LIMIT, "q16 layout larger than 2^31 entries");
+    if ((int64_t)total != s->q16_entries) return fail(PHG_GPU_ERR_CUDA, "q16 layout: slice sizes disagree");
     CHECK_RC(s->q16_cols.ensure((size_t)total));
     CHECK_RC(s->q16_v32.ensure((size_t)total));
     CHECK_RC(s->q16_v64.ensure((size_t)total));
