@@ -583,34 +583,6 @@ cudaError_t launch_mixed_init(int64_t n, const double *rtrue, float *r32, float 
     return cudaGetLastError();
 }
 
-cudaError_t launch_spmv32(const SellView &S, int unroll, const float *x, float *y, cudaStream_t s) {
-    const int sb = vec_blocks(S.nslices * 32);
-    switch (unroll) {
-    case 2: sell_spmv_kernel<float, false, 2><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals32, x, y, nullptr, nullptr); break;
-    case 8: sell_spmv_kernel<float, false, 8><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals32, x, y, nullptr, nullptr); break;
-    case 16: sell_spmv_kernel<float, false, 16><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals32, x, y, nullptr, nullptr); break;
-    default: sell_spmv_kernel<float, false, 4><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals32, x, y, nullptr, nullptr); break;
-    }
-    return cudaGetLastError();
-}
-
-cudaError_t launch_mixed_iteration(const MixedBuffers &B, const SellView &S, int unroll, cudaStream_t s) {
-    const int vb = vvec_blocks(B.n, 4);
-    PcgState *st = &B.ms->pcg;
-    pcg_dir_kernel<float><<<vb, kVecThreads, 0, s>>>(B.n, B.r32, B.D32, B.p32, st);
-    const int sb = vec_blocks(S.nslices * 32);
-    switch (unroll) {
-    case 2: sell_spmv_kernel<float, true, 2><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals32, B.p32, B.Ap32, B.partials, st); break;
-    case 8: sell_spmv_kernel<float, true, 8><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals32, B.p32, B.Ap32, B.partials, st); break;
-    case 16: sell_spmv_kernel<float, true, 16><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals32, B.p32, B.Ap32, B.partials, st); break;
-    default: sell_spmv_kernel<float, true, 4><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals32, B.p32, B.Ap32, B.partials, st); break;
-    }
-    mixed_update_kernel<<<vb, kVecThreads, 0, s>>>(B.n, B.y32, B.r32, B.p32, B.Ap32, B.D32, B.partials, B.ms);
-    mixed_reliable_kernel<4><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals, B.x, B.y32,
-                                                         B.rtrue, B.r32, B.D32, B.partials, B.ms, B.hist);
-    return cudaGetLastError();
-}
-
 // ---------------------------------------------------------------------------
 // FP32 values in "pair" SELL: the same slices as SELL-C-sigma, but each lane
 // keeps two consecutive entries of its row side by side, so a warp moves

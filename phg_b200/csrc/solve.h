@@ -125,8 +125,6 @@ cudaError_t launch_spmv32k(const SellView &S, const Sell2View &S2, int kind, int
                            cudaStream_t s);
 cudaError_t launch_mixed_iteration2(const MixedBuffers &B, const SellView &S, const Sell2View &S2, int kind, int u,
                                     cudaStream_t s);
-cudaError_t launch_spmv32(const SellView &S, int unroll, const float *x, float *y, cudaStream_t s);
-cudaError_t launch_mixed_iteration(const MixedBuffers &B, const SellView &S, int unroll, cudaStream_t s);
 int64_t sell_positions(int64_t n);   // perm/len entries = slices * 32
 cudaError_t launch_sell_sort(int64_t n, const int32_t *rp, int32_t *perm, uint16_t *len, int32_t *slice_size,
                              cudaStream_t s);
