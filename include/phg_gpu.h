@@ -38,13 +38,20 @@ extern "C" {
 #define PHG_GPU_ERR_CUDA	(-2)	/* CUDA runtime error */
 #define PHG_GPU_ERR_STATE	(-3)	/* call out of order */
 #define PHG_GPU_ERR_LIMIT	(-4)	/* size beyond a documented limit */
-#define PHG_GPU_ERR_BREAKDOWN	(-5)	/* PCG breakdown: matrix not SPD */
+#define PHG_GPU_ERR_BREAKDOWN	(-5)	/* breakdown the reference cannot continue
+					   from (BiCGstab, the adjoint solve) */
 #define PHG_GPU_ERR_NAN		(-6)	/* non-finite value in the iteration */
 
 typedef struct phgGpuSystem_ phgGpuSystem;
 
 /* Text of the calling thread's last error ("" if none). */
 const char *phgGpuLastError(void);
+/* Text of the warning the calling thread's last solver call raised ("" if
+ * none; every solver call clears it).  A PCG breakdown -- r.z or p.Ap of 0,
+ * where the reference prints "Warning! the matrix may not be SPD" and returns
+ * its iteration count (src/solver-phg.c:547-571) -- returns the iteration
+ * count with x as it is and sets this text. */
+const char *phgGpuLastWarning(void);
 /* Library version, major * 10000 + minor * 100 + patch. */
 int phgGpuVersion(void);
 
@@ -113,6 +120,13 @@ int phgGpuElementMatrices(phgGpuSystem *sys, const double *kappa,
 int phgGpuSetMatrix(phgGpuSystem *sys, int64_t n, const int64_t *ptr,
 		    const int32_t *cols, const double *vals, const double *rhs);
 
+/* Replaces the right-hand side the solvers use (n values, boundary
+ * elimination already applied) and keeps the matrix: a new phgSolverVecSolve
+ * on the same matrix (src/solver.c:1131-1150) or a change of
+ * solver->rhs->data before phgSolverSolve.  Non-finite values:
+ * PHG_GPU_ERR_NAN. */
+int phgGpuSetRHS(phgGpuSystem *sys, const double *rhs);
+
 /* Sizes of the assembled system: rows, matrix entries, saved boundary
  * column entries. */
 int phgGpuGetSizes(phgGpuSystem *sys, int64_t *n, int64_t *nnz,
@@ -140,7 +154,9 @@ int phgGpuMatVec(phgGpuSystem *sys, const double *x, double *y);
  * x: initial guess in, solution out (n).  Returns the iteration count
  * (>= 0) or a negative error code; *residual gets the final ||r||_2.
  * hist (optional, maxit + 1 doubles) receives ||r|| after each
- * iteration, hist[0] = ||r0||. */
+ * iteration, hist[0] = ||r0||.  On a breakdown (the matrix may not be SPD)
+ * the iteration stops and the count is returned, as in the reference, with
+ * the warning in phgGpuLastWarning(). */
 int phgGpuSolverPCG(phgGpuSystem *sys, double rtol, double btol,
 		    double atol, int maxit, double *x, double *residual,
 		    double *hist);
@@ -209,7 +225,8 @@ int phgGpuAdjointGradient(phgGpuSystem *sys, const double *u,
  * residual; on return *residual is ||b - A x||_2 computed in FP64.  Extends
  * the reference (its FLOAT is fixed at build time, configure.in:627-671).
  * Returns the number of FP32 iterations or a negative error code;
- * *nupdates gets the number of reliable updates. */
+ * *nupdates gets the number of reliable updates.  A breakdown stops the
+ * iteration as in phgGpuSolverPCG (count returned, phgGpuLastWarning()). */
 int phgGpuSolverPCGMixed(phgGpuSystem *sys, double rtol, double btol,
 			 double atol, int maxit, double *x, double *residual,
 			 int *nupdates);
@@ -274,11 +291,13 @@ int phgGpuGetLaunchCount(phgGpuSystem *sys, int64_t *count);
  * n + 1), cols, vals, rhs and x (initial guess in, solution out) must be
  * device memory of the current device; work runs on `stream`
  * (cudaStream_t, NULL = default stream) and the call returns when it is
- * done.  The first call on a device looks up the array's device address;
- * make that first call before any stream capture.  All calls share the one
- * array, so calls that overlap on the GPU (other host threads, other
+ * done.  Every call looks up the array's address in the current device's
+ * context (so a context created again after cudaDeviceReset is served
+ * correctly); the first call on a device also loads the library's device
+ * code, so make that first call before any stream capture.  All calls share
+ * the one array, so calls that overlap on the GPU (other host threads, other
  * streams) race: serialise them.  Returns the iteration count or a negative
- * error code. */
+ * error code; a breakdown is reported as in phgGpuSolverPCG. */
 #define PHG_GPU_NOALLOC_MAX_ROWS 262144
 int phgGpuSolverPCGNoAlloc(int64_t n, const int64_t *ptr, const int32_t *cols,
 			   const double *vals, const double *rhs, double *x,

@@ -7,8 +7,8 @@ ctypes and offers the same operations with numpy arrays (host memory) or
 torch CUDA tensors (device memory).  There is no CPU fallback: if the
 library is missing or no GPU is present, calls raise.
 """
-from .core import (PhgGpuError, Solver, lib, load_library, LIB_PATH)  # noqa: F401
+from .core import (PhgGpuError, Solver, last_warning, lib, load_library, LIB_PATH)  # noqa: F401
 from .mesh import kuhn_cube, lagrange_dofs, sine_source, write_medit  # noqa: F401
 
-__all__ = ["PhgGpuError", "Solver", "lib", "load_library", "LIB_PATH",
+__all__ = ["PhgGpuError", "Solver", "last_warning", "lib", "load_library", "LIB_PATH",
            "kuhn_cube", "lagrange_dofs", "sine_source", "write_medit"]

@@ -22,6 +22,7 @@ _P = C.c_void_p
 _I64 = C.c_int64
 SIGNATURES = {
     "phgGpuLastError": (C.c_char_p, []),
+    "phgGpuLastWarning": (C.c_char_p, []),
     "phgGpuVersion": (C.c_int, []),
     "phgGpuCreate": (C.c_int, [C.c_int, _P, C.POINTER(_P)]),
     "phgGpuDestroy": (C.c_int, [_P]),
@@ -31,6 +32,7 @@ SIGNATURES = {
     "phgGpuBuildLinearSystem": (C.c_int, [_P, _P, _P, _P]),
     "phgGpuBuildLinearSystemMass": (C.c_int, [_P, _P, C.c_double, _P, _P]),
     "phgGpuSetMatrix": (C.c_int, [_P, _I64, _P, _P, _P, _P]),
+    "phgGpuSetRHS": (C.c_int, [_P, _P]),
     "phgGpuGetSizes": (C.c_int, [_P, C.POINTER(_I64), C.POINTER(_I64), C.POINTER(_I64)]),
     "phgGpuGetMatrix": (C.c_int, [_P, _P, _P, _P]),
     "phgGpuGetBdryColumns": (C.c_int, [_P, _P, _P, _P]),
@@ -94,6 +96,13 @@ def _check(rc):
     if rc < 0:
         raise PhgGpuError(rc, lib().phgGpuLastError().decode())
     return rc
+
+
+def last_warning():
+    """Warning text of the calling thread's last solver call ("" if none):
+    e.g. a PCG breakdown, which the reference reports as "the matrix may not
+    be SPD" and survives (solver-phg.c:547-571)."""
+    return lib().phgGpuLastWarning().decode()
 
 
 def _ptr(a):
@@ -184,6 +193,12 @@ class Solver:
         ptr, cols = _np(ptr, np.int64), _np(cols, np.int32)
         vals, rhs = _np(vals, np.float64), _np(rhs, np.float64)
         _check(lib().phgGpuSetMatrix(self._h, len(ptr) - 1, _ptr(ptr), _ptr(cols), _ptr(vals), _ptr(rhs)))
+
+    def set_rhs(self, rhs):
+        """Replaces the right-hand side of the assembled system (after
+        boundary elimination), keeping the matrix."""
+        rhs = _np(rhs, np.float64)
+        _check(lib().phgGpuSetRHS(self._h, _ptr(rhs)))
 
     def sizes(self):
         n, nnz, bnnz = _I64(), _I64(), _I64()

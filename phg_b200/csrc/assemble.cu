@@ -157,6 +157,10 @@ geometry_kernel(int64_t nelem, int64_t nvert, const double *__restrict__ verts, 
             }
         }
         if (!ok) atomicExch(status, PHGB_DEV_BAD_INDEX);
+        bool fin = true;
+#pragma unroll
+        for (int t = 0; t < 12; t++) fin = fin && isfinite(x[t]);
+        if (!fin) atomicExch(status, PHGB_DEV_NONFINITE);
         double J[16], vol;
         jacobian_vol(x, J, vol);
         double *o = geo + (size_t)e * kGeo;
@@ -198,7 +202,11 @@ element_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, cons
 
     for (int64_t e = (int64_t)blockIdx.x * W + w; e < nelem; e += (int64_t)gridDim.x * W) {
         if (lane < 17) J[lane] = geo[(size_t)e * kGeo + lane];
-        if (lane == 17) J[17] = kappa != nullptr ? kappa[e] : 0.0;
+        if (lane == 17) {
+            const double kv = kappa != nullptr ? kappa[e] : 0.0;
+            if (!isfinite(kv)) atomicExch(status, PHGB_DEV_NONFINITE);
+            J[17] = kv;
+        }
         // f_h at the element's nodes
         if (lane < N) {
             double fv = 0.0;
@@ -206,6 +214,7 @@ element_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, cons
                 const int32_t d = e2l[(size_t)e * N + lane];
                 if (d < 0 || d >= ndof) atomicExch(status, PHGB_DEV_BAD_INDEX);
                 else fv = f[d];
+                if (!isfinite(fv)) atomicExch(status, PHGB_DEV_NONFINITE);
             }
             fl[lane] = fv;
         }
@@ -443,6 +452,7 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
         const int64_t rbase = (int64_t)i0 * N, rcap = (int64_t)(i1 - i0) * N;
         if (active && isb && gl == 0) {
             const int mult = i1 - i0;
+            if (g != nullptr && !isfinite(g[d])) atomicExch(status, PHGB_DEV_NONFINITE);
             double m = 0.0;
             for (int i = 0; i < mult; i++) m = rn_add(m, 1.0);
             if (mult > 0) {

@@ -26,6 +26,7 @@ using namespace phgb;
 namespace {
 
 thread_local std::string g_last_error;
+thread_local std::string g_last_warning;
 
 int fail(int code, const char *fmt, ...) {
     char buf[512];
@@ -35,6 +36,18 @@ int fail(int code, const char *fmt, ...) {
     va_end(ap);
     g_last_error = buf;
     return code;
+}
+
+// A condition the reference reports with a warning and survives (a PCG
+// breakdown: solver-phg.c:547-571 prints "the matrix may not be SPD" and
+// returns the iteration count).
+void warn(const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_warning = buf;
 }
 
 #define CK(call)                                                                              \
@@ -105,6 +118,12 @@ __global__ void narrow_kernel(int64_t n, const int64_t *in, int32_t *out) {
         out[i] = (int32_t)in[i];
 }
 
+// Flags a NaN or infinite value of v in *status.
+__global__ void nonfinite_kernel(int64_t n, const double *v, int *status) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (!isfinite(v[i])) atomicExch(status, PHGB_DEV_NONFINITE);
+}
+
 // phgMatSetupDiagonal (matvec.c:500-549): first entry of row i in column i.
 __global__ void diag_kernel(int64_t n, const int32_t *rp, const int32_t *ci, const double *va, double *d) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -131,6 +150,7 @@ const int kTuneParam[kTuneCandidates] = {4, 8, 16, 32, 2, 4, 8, 1};
 namespace phgb {
 // Lets other translation units of the library report through phgGpuLastError().
 void set_last_error(const char *msg) { g_last_error = msg; }
+void set_last_warning(const char *msg) { g_last_warning = msg; }
 }  // namespace phgb
 
 struct phgGpuSystem_ {
@@ -275,6 +295,8 @@ int check_status(phgGpuSystem *s, const char *where) {
     CK(cudaMemsetAsync(s->status.p, 0, sizeof(int), s->stream));
     switch (st) {
     case PHGB_DEV_BAD_INDEX: return fail(PHG_GPU_ERR_ARG, "%s: vertex or DOF index out of range", where);
+    case PHGB_DEV_NONFINITE:
+        return fail(PHG_GPU_ERR_NAN, "%s: a coordinate, kappa, f or g value is NaN or infinite", where);
     case PHGB_DEV_ROW_OVERFLOW:
         return fail(PHG_GPU_ERR_LIMIT, "%s: a matrix row has more than %d entries", where,
                     row_walk_max_row(s->order));
@@ -676,6 +698,8 @@ extern "C" {
 
 const char *phgGpuLastError(void) { return g_last_error.c_str(); }
 
+const char *phgGpuLastWarning(void) { return g_last_warning.c_str(); }
+
 int phgGpuVersion(void) { return 100; }
 
 int phgGpuCreate(int device, void *stream, phgGpuSystem **out) {
@@ -980,6 +1004,17 @@ int phgGpuSetMatrix(phgGpuSystem *s, int64_t n, const int64_t *ptr, const int32_
     return PHG_GPU_OK;
 }
 
+int phgGpuSetRHS(phgGpuSystem *s, const double *rhs) {
+    if (s == nullptr || rhs == nullptr) return fail(PHG_GPU_ERR_ARG, "phgGpuSetRHS: invalid arguments");
+    if (!s->assembled) return fail(PHG_GPU_ERR_STATE, "phgGpuSetRHS: no assembled system");
+    CHECK_RC(set_device(s));
+    CHECK_RC(copy_in(s, s->rhs.p, rhs, (size_t)s->n));
+    nonfinite_kernel<<<vec_blocks(s->n), 256, 0, s->stream>>>(s->n, s->rhs.p, s->status.p);
+    CK(cudaGetLastError());
+    s->launches += 1;
+    return check_status(s, "phgGpuSetRHS");
+}
+
 int phgGpuGetSizes(phgGpuSystem *s, int64_t *n, int64_t *nnz, int64_t *nnz_bdry) {
     if (s == nullptr) return fail(PHG_GPU_ERR_ARG, "null system");
     if (!s->assembled) return fail(PHG_GPU_ERR_STATE, "no assembled system");
@@ -1055,6 +1090,7 @@ int phgGpuMatVec(phgGpuSystem *s, const double *x, double *y) {
 
 int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol, int maxit, double *x,
                          double *residual, int *nupdates) {
+    g_last_warning.clear();
     if (s == nullptr || x == nullptr) return fail(PHG_GPU_ERR_ARG, "invalid arguments");
     if (!s->assembled) return fail(PHG_GPU_ERR_STATE, "no assembled system");
     if (maxit < 0) return fail(PHG_GPU_ERR_ARG, "maxit < 0");
@@ -1177,9 +1213,20 @@ int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol,
         nupd += hm.nupdates;
         fold_kernel<<<vec_blocks(n), 256, 0, s->stream>>>(n, s->x.p, s->y32.p, s->mst.p);
         s->launches += 1;
-        if (hm.pcg.status == PCG_BREAKDOWN)
-            return fail(PHG_GPU_ERR_BREAKDOWN, "mixed PCG breakdown: the matrix may not be SPD");
         if (hm.pcg.status == PCG_NONFINITE) return fail(PHG_GPU_ERR_NAN, "mixed PCG: non-finite residual");
+        if (hm.pcg.status == PCG_BREAKDOWN) {
+            // as the FP64 PCG: warn, keep the iterate, report the FP64 residual
+            warn("mixed PCG stopped after %d iterations: the matrix may not be SPD", nits_total);
+            CK(product64(s->x.p, s->Ap.p));
+            CK(launch_residual(n, s->rhs.p, s->Ap.p, s->r.p, s->stream));
+            CK(launch_init_sums(n, 1, s->x.p, s->r.p, s->diag.p, s->partials.p, s->ticket.p, s->sums.p,
+                                s->stream));
+            s->launches += 3;
+            CK(cudaMemcpyAsync(s->h_sums, s->sums.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+            CK(cudaStreamSynchronize(s->stream));
+            res_true = sqrt(s->h_sums[0]);
+            break;
+        }
         // explicit FP64 residual of the accumulated solution
         CK(product64(s->x.p, s->Ap.p));
         CK(launch_residual(n, s->rhs.p, s->Ap.p, s->r.p, s->stream));
@@ -1394,7 +1441,7 @@ int pcg_core(phgGpuSystem *s, const double *drhs, double rtol, double btol, doub
     const int nits = s->h_st->nits;
     if (residual) *residual = s->h_st->residual;
     if (s->h_st->status == PCG_BREAKDOWN)
-        return fail(PHG_GPU_ERR_BREAKDOWN, "PCG breakdown after %d iterations: the matrix may not be SPD", nits);
+        warn("PCG stopped after %d iterations: the matrix may not be SPD", nits);
     if (s->h_st->status == PCG_NONFINITE)
         return fail(PHG_GPU_ERR_NAN, "PCG: non-finite residual after %d iterations", nits);
     return nits;
@@ -1507,6 +1554,7 @@ extern "C" {
 
 int phgGpuSolverPCG(phgGpuSystem *s, double rtol, double btol, double atol, int maxit, double *x,
                     double *residual, double *hist) {
+    g_last_warning.clear();
     if (s == nullptr || x == nullptr) return fail(PHG_GPU_ERR_ARG, "invalid arguments");
     if (!s->assembled) return fail(PHG_GPU_ERR_STATE, "no assembled system");
     if (maxit < 0) return fail(PHG_GPU_ERR_ARG, "maxit < 0");
@@ -1529,6 +1577,7 @@ int phgGpuSolverPCG(phgGpuSystem *s, double rtol, double btol, double atol, int 
 
 int phgGpuSolverGMRES(phgGpuSystem *s, int restart, double rtol, double btol, double atol, int maxit, double *x,
                       double *residual) {
+    g_last_warning.clear();
     if (s == nullptr || x == nullptr) return fail(PHG_GPU_ERR_ARG, "invalid arguments");
     if (!s->assembled) return fail(PHG_GPU_ERR_STATE, "no assembled system");
     if (maxit < 0) return fail(PHG_GPU_ERR_ARG, "maxit < 0");
@@ -1610,6 +1659,7 @@ int phgGpuSolverGMRES(phgGpuSystem *s, int restart, double rtol, double btol, do
 
 int phgGpuSolverBiCGstab(phgGpuSystem *s, double rtol, double btol, double atol, int maxit, double *x,
                          double *residual, double *hist) {
+    g_last_warning.clear();
     if (s == nullptr || x == nullptr) return fail(PHG_GPU_ERR_ARG, "invalid arguments");
     if (!s->assembled) return fail(PHG_GPU_ERR_STATE, "no assembled system");
     if (maxit < 0) return fail(PHG_GPU_ERR_ARG, "maxit < 0");
@@ -1632,6 +1682,7 @@ int phgGpuSolverBiCGstab(phgGpuSystem *s, double rtol, double btol, double atol,
 
 int phgGpuAdjointGradient(phgGpuSystem *s, const double *u, const double *u_obs, double rtol, int maxit,
                           double *grad, double *J, int *nits_out) {
+    g_last_warning.clear();
     if (s == nullptr || u == nullptr || u_obs == nullptr || grad == nullptr)
         return fail(PHG_GPU_ERR_ARG, "invalid arguments");
     if (!s->assembled || !s->have_bdry_cols)
@@ -1660,6 +1711,8 @@ int phgGpuAdjointGradient(phgGpuSystem *s, const double *u, const double *u_obs,
     double res = 0.0;
     const int nits = pcg_core(s, s->adj_rhs.p, rtol, 0.0, 0.0, maxit, nullptr, &res);
     if (nits < 0) return nits;
+    if (s->h_st->status == PCG_BREAKDOWN)
+        return fail(PHG_GPU_ERR_BREAKDOWN, "phgGpuAdjointGradient: adjoint PCG breakdown (matrix not SPD)");
     CK(cudaMemcpyAsync(s->adj_lambda.p, s->x.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s->stream));
     const bool gdev = is_device_ptr(grad);
     double *dg = gdev ? grad : s->adj_grad.p;
@@ -1675,6 +1728,7 @@ int phgGpuAdjointGradient(phgGpuSystem *s, const double *u, const double *u_obs,
 
 int phgGpuSolverBlockPCG(phgGpuSystem *s, int nrhs, const double *B, double *X, double rtol, int maxit,
                          int mixed, int *nits_out, double *res_out) {
+    g_last_warning.clear();
     if (s == nullptr || B == nullptr || X == nullptr || nrhs <= 0) return fail(PHG_GPU_ERR_ARG, "invalid arguments");
     if (nrhs > 64) return fail(PHG_GPU_ERR_LIMIT, "phgGpuSolverBlockPCG: at most 64 right-hand sides per call");
     if (!s->assembled) return fail(PHG_GPU_ERR_STATE, "no assembled system");

@@ -16,19 +16,18 @@
 #include "solve.h"
 
 namespace phgb {
-void set_last_error(const char *msg);   // capi.cu
+void set_last_error(const char *msg);     // capi.cu
+void set_last_warning(const char *msg);   // capi.cu
 }
 
 #include <float.h>
 #include <math.h>
 #include <stdio.h>
 
-#include <mutex>
 
 namespace {
 
 constexpr int64_t kMaxRows = PHG_GPU_NOALLOC_MAX_ROWS;
-constexpr int kMaxBlocks = 148 * 8;   // largest grid vec_blocks() returns
 constexpr size_t kAlign = 256;
 
 constexpr size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
@@ -41,19 +40,16 @@ constexpr size_t kOffP = kOffR + kVec;
 constexpr size_t kOffAp = kOffP + kVec;
 constexpr size_t kOffRp = kOffAp + kVec;
 constexpr size_t kOffPartials = kOffRp + align_up(sizeof(int32_t) * (kMaxRows + 1));
-constexpr size_t kOffSums = kOffPartials + align_up(sizeof(double) * (2 * kMaxBlocks + 64));
+// grid-sum workspace for the largest grid any grid sum may use (reduce.cuh)
+constexpr size_t kOffSums = kOffPartials + align_up(sizeof(double) * phgb::red_partials_doubles(phgb::kRedMaxBlocks));
 constexpr size_t kOffState = kOffSums + align_up(sizeof(double) * 2);
 constexpr size_t kOffTicket = kOffState + align_up(sizeof(phgb::PcgState));
 constexpr size_t kStaticScratchBytes = kOffTicket + align_up(sizeof(unsigned) * phgb::kRedTickets);
 
 // The scratch memory.  In host code this name is only a stand-in for the
 // symbol, not a device address; the device address comes from
-// cudaGetSymbolAddress, once per device, below.
+// cudaGetSymbolAddress with the device current, on every call, below.
 static __device__ __align__(256) unsigned char g_pcg_scratch[kStaticScratchBytes];
-
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-unsigned char *g_scratch_addr[kMaxDevices] = {};
 
 // records the message for phgGpuLastError() (kept in capi.cu)
 int fail(int code, const char *msg) {
@@ -61,21 +57,19 @@ int fail(int code, const char *msg) {
     return code;
 }
 
-// Device address of the scratch array on `dev`, looked up once per device
-// with that device current.
-int scratch_address(int dev, unsigned char **out) {
-    if (dev < 0 || dev >= kMaxDevices) return fail(PHG_GPU_ERR_LIMIT, "device index too large");
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (g_scratch_addr[dev] == nullptr) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_pcg_scratch);
-        if (e != cudaSuccess || p == nullptr) {
-            cudaGetLastError();
-            return fail(PHG_GPU_ERR_CUDA, "cudaGetSymbolAddress failed for the PCG scratch array");
-        }
-        g_scratch_addr[dev] = (unsigned char *)p;
+// Device address of the scratch array in the current device's context.  It
+// is looked up on every call (a host-side table lookup once the library's
+// device code is loaded), so a context that was reset and created again gets
+// the array's new address.  The first lookup on a device loads the device
+// code; that first call must not happen during a stream capture.
+int scratch_address(unsigned char **out) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_pcg_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+        cudaGetLastError();
+        return fail(PHG_GPU_ERR_CUDA, "cudaGetSymbolAddress failed for the PCG scratch array");
     }
-    *out = g_scratch_addr[dev];
+    *out = (unsigned char *)p;
     return PHG_GPU_OK;
 }
 
@@ -117,6 +111,7 @@ constexpr int kChunk = 16;
 int solve(int64_t n, const int64_t *ptr, const int32_t *cols, const double *vals, const double *rhs, double *x,
           double rtol, double btol, double atol, int maxit, cudaStream_t s, double *residual) {
     using namespace phgb;
+    set_last_warning("");
     if (n <= 0 || ptr == nullptr || cols == nullptr || vals == nullptr || rhs == nullptr || x == nullptr || maxit < 0)
         return fail(PHG_GPU_ERR_ARG, "phgGpuSolverPCGNoAlloc: invalid arguments");
     if (n > kMaxRows) {
@@ -133,7 +128,7 @@ int solve(int64_t n, const int64_t *ptr, const int32_t *cols, const double *vals
             return fail(PHG_GPU_ERR_ARG, "phgGpuSolverPCGNoAlloc: arguments must be device memory "
                                          "of the current device");
     unsigned char *base = nullptr;
-    int rc = scratch_address(dev, &base);
+    int rc = scratch_address(&base);
     if (rc != PHG_GPU_OK) return rc;
     double *D = (double *)(base + kOffDiag), *r = (double *)(base + kOffR);
     double *p = (double *)(base + kOffP), *Ap = (double *)(base + kOffAp);
@@ -141,7 +136,6 @@ int solve(int64_t n, const int64_t *ptr, const int32_t *cols, const double *vals
     double *partials = (double *)(base + kOffPartials), *sums = (double *)(base + kOffSums);
     PcgState *st = (PcgState *)(base + kOffState);
     unsigned *ticket = (unsigned *)(base + kOffTicket);
-    if (2 * vec_blocks(n * 32) > 2 * kMaxBlocks) return fail(PHG_GPU_ERR_LIMIT, "grid larger than scratch");
 
     int64_t nnz = 0, first = 0;
     CKS(cudaMemcpyAsync(&nnz, ptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
@@ -199,8 +193,11 @@ int solve(int64_t n, const int64_t *ptr, const int32_t *cols, const double *vals
         CKS(cudaStreamSynchronize(s));
     }
     if (residual) *residual = hs.residual;
-    if (hs.status == PCG_BREAKDOWN) return fail(PHG_GPU_ERR_BREAKDOWN, "PCG breakdown: the matrix may not be SPD");
     if (hs.status == PCG_NONFINITE) return fail(PHG_GPU_ERR_NAN, "PCG: non-finite residual");
+    // a breakdown ends the iteration as in the reference (solver-phg.c:547-571):
+    // x as it is, the iteration count returned, a warning recorded
+    if (hs.status == PCG_BREAKDOWN)
+        phgb::set_last_warning("phgGpuSolverPCGNoAlloc: PCG stopped, the matrix may not be SPD");
     return hs.nits;
 }
 

@@ -214,7 +214,7 @@ static_assert(148 * 8 <= kRedMaxBlocks, "grids of reducing kernels must fit the 
 
 int vec_blocks(int64_t n) {
     int64_t b = ceil_div(n, kVecThreads);
-    if (b > 148 * 8) b = 148 * 8;
+    if (b > kVecMaxBlocks) b = kVecMaxBlocks;
     if (b < 1) b = 1;
     return (int)b;
 }

@@ -20,6 +20,14 @@ enum { PCG_RUNNING = 0, PCG_BREAKDOWN = 1, PCG_NONFINITE = 2 };
 constexpr int kRedGroup = 64;
 constexpr int kRedMaxBlocks = 2048;   // at most 32 groups: one load per lane
 constexpr int kRedTickets = 1 + kRedMaxBlocks / kRedGroup;
+// Doubles of grid-sum workspace (reduce.cuh) a grid of `blocks` blocks uses.
+constexpr int64_t red_partials_doubles(int64_t blocks) {
+    return 2 * (blocks + (blocks + kRedGroup - 1) / kRedGroup);
+}
+// Largest grid vec_blocks() returns; every grid-sum launch stays within
+// kRedMaxBlocks.
+constexpr int kVecMaxBlocks = 148 * kResidentBlocks;
+static_assert(kVecMaxBlocks <= kRedMaxBlocks, "grid sums take at most kRedMaxBlocks blocks");
 
 struct PcgState {
     double rz_cur, rz_prev, pAp, alpha, residual, tol;

@@ -193,15 +193,73 @@ def test_nonzero_initial_guess(gpu, oracle):
     s.close()
 
 
-def test_breakdown_reported(gpu):
-    """p.Ap == 0 stops PCG as the reference does (solver-phg.c:561-571) and
-    comes back as PHG_GPU_ERR_BREAKDOWN."""
+def test_breakdown_reported(gpu, oracle):
+    """p.Ap == 0 stops PCG as the reference does (solver-phg.c:561-571): the
+    iteration count comes back with x as it is, and the warning the
+    reference prints ("the matrix may not be SPD") is readable."""
+    ptr, cols, vals = np.array([0, 1, 2]), np.array([0, 1], np.int32), np.array([1.0, -1.0])
+    b = np.array([1.0, 1.0])
     s = gpu.Solver(0)
-    s.set_matrix(np.array([0, 1, 2]), np.array([0, 1], np.int32), np.array([1.0, -1.0]),
-                 np.array([1.0, 1.0]))
+    s.set_matrix(ptr, cols, vals, b)
+    x, nits, res = s.solve_pcg(rtol=1e-10)
+    xo, no, ro, _ = oracle.pcg(ptr, cols, vals, vals, b, rtol=1e-10)
+    assert nits == no == 1
+    assert np.array_equal(x, xo) and res == ro
+    assert "not be SPD" in gpu.last_warning()
+    # the next solver call clears the warning
+    s.set_matrix(ptr, cols, np.array([1.0, 2.0]), b)
+    x, nits, _ = s.solve_pcg(rtol=1e-10)
+    assert gpu.last_warning() == "" and nits >= 1
+    s.close()
+
+
+def test_nonfinite_input_reported(gpu):
+    """A NaN or infinite kappa, f, g or coordinate is PHG_GPU_ERR_NAN at
+    build time (the system stays usable); so is a non-finite right-hand
+    side handed to phgGpuSetRHS."""
+    G = load_golden("p2_m3_sine")
+    s = gpu.Solver(0)
+    s.set_mesh(G["verts"], G["elems"])
+    s.set_dof_map(2, G["e2l"], G["bdry"])
+    nel, nd = len(G["elems"]), len(G["bdry"])
+    cases = []
+    k = np.ones(nel); k[5] = np.nan; cases.append(dict(kappa=k, f=G["f"]))
+    k = np.ones(nel); k[0] = np.inf; cases.append(dict(kappa=k, f=G["f"]))
+    f = G["f"].copy(); f[7] = np.nan; cases.append(dict(f=f))
+    g = np.zeros(nd); g[np.flatnonzero(G["bdry"])[3]] = -np.inf; cases.append(dict(f=G["f"], g=g))
+    for kw in cases:
+        with pytest.raises(gpu.PhgGpuError) as ei:
+            s.build_linear_system(**kw)
+        assert ei.value.code == -6, kw.keys()
+    v = G["verts"].copy(); v[2, 1] = np.nan
+    s.set_mesh(v, G["elems"])
     with pytest.raises(gpu.PhgGpuError) as ei:
-        s.solve_pcg(rtol=1e-10)
-    assert ei.value.code == -5
+        s.build_linear_system(f=G["f"])
+    assert ei.value.code == -6
+    s.set_mesh(G["verts"], G["elems"])
+    s.build_linear_system(f=G["f"])
+    assert np.array_equal(s.get_rhs(), G["rhs"])
+    r = G["rhs"].copy(); r[1] = np.nan
+    with pytest.raises(gpu.PhgGpuError) as ei:
+        s.set_rhs(r)
+    assert ei.value.code == -6
+    s.close()
+
+
+def test_set_rhs_new_solve(gpu, oracle):
+    """phgGpuSetRHS keeps the matrix and solves a new right-hand side, as a
+    second phgSolverVecSolve on the same matrix does."""
+    G = load_golden("p2_m5_kappa")
+    s = build(gpu, 2, G["verts"], G["elems"], G["e2l"], G["bdry"], G["f"], G["g"], G["kappa"])
+    b2 = np.random.default_rng(3).standard_normal(len(G["rhs"]))
+    b2[G["bdry"] != 0] = 0.0
+    s.set_rhs(b2)
+    assert np.array_equal(s.get_rhs(), b2)
+    x, nits, _ = s.solve_pcg(rtol=1e-10, btol=0.0, atol=0.0)
+    xo, no, _, _ = oracle.pcg(G["rows_ptr"], G["rows_cols"], G["rows_vals"], G["diag"], b2,
+                              rtol=1e-10, btol=0.0, atol=0.0)
+    assert abs(nits - no) <= 2
+    assert np.linalg.norm(x - xo) <= 1e-7 * np.linalg.norm(xo)
     s.close()
 
 
