@@ -160,22 +160,47 @@ def write_mesh(m, path):
     write_medit(path, v, e)
 
 
-def run_reference(args, m, reps, sample_maxit):
-    """Runs the reference's OpenMP build on the workload; returns the JSON
-    lines of its repetitions (rep 0 runs to tolerance, later reps stop
-    after `sample_maxit` PCG iterations)."""
+def run_reference(args, m, reps, sample_maxit, threads=None, maxit=100000):
+    """Runs the reference's OpenMP build on the workload (element loop on all
+    threads as examples/poisson.c does, PHG's OpenMP SpMV and BLAS-1);
+    returns the JSON lines of its repetitions (rep 0 runs to tolerance or
+    `maxit`, later reps stop after `sample_maxit` PCG iterations)."""
     if not os.path.exists(REF_DUMP_OMP):
         raise RuntimeError("reference build missing (oracle/_ref/phg_dump_omp)")
     with tempfile.TemporaryDirectory() as d:
         mesh = os.path.join(d, "cube.mesh")
         write_mesh(m, mesh)
-        env = dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count()), OMP_PROC_BIND="false")
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads or os.cpu_count()), OMP_PROC_BIND="false")
         cmd = [REF_DUMP_OMP, "-mesh_file", mesh, "-dof_type", "P2", "-solver", "pcg",
                "-pcg_pc_type", "jacobi", "-solver_rtol", "1e-8", "-solver_btol", "0",
-               "-solver_atol", "0", "-solver_maxit", "100000", "-map_reorder", "no",
+               "-solver_atol", "0", "-solver_maxit", str(maxit), "-map_reorder", "no",
                "-repeat", str(reps), "-sample_maxit", str(sample_maxit)]
         out = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=3600, check=True)
     return [json.loads(l) for l in out.stdout.splitlines() if l.startswith("{")]
+
+
+def stage_split(rec, nits_full):
+    """Stage times (ms) of one reference repetition; a capped solve is
+    scaled to the full iteration count."""
+    return {"t_build_ms": round(1e3 * rec["t_build"], 1), "t_assemble_ms": round(1e3 * rec["t_assemble"], 1),
+            "t_solve_ms": round(1e3 * rec["t_solve"] * nits_full / max(rec["nits"], 1), 1),
+            "nits": int(nits_full), "threads": int(rec["threads"])}
+
+
+# iterations of the one-thread sample of the reference (its solve time is
+# scaled to the full count)
+ONE_THREAD_SAMPLE_ITS = 20
+
+
+def one_thread_reference(args, m, nits_full):
+    """The reference on one thread: element loop and phgSolverAssemble in
+    full, PCG for ONE_THREAD_SAMPLE_ITS iterations scaled to nits_full."""
+    r = run_reference(args, m, 1, 0, threads=1, maxit=ONE_THREAD_SAMPLE_ITS)[0]
+    st = stage_split(r, nits_full)
+    st["value_ms"] = round(st["t_build_ms"] + st["t_assemble_ms"] + st["t_solve_ms"], 1)
+    st["sample"] = ("1 thread: element loop + phgSolverAssemble in full, %d PCG iterations scaled to %d"
+                    % (r["nits"], nits_full))
+    return st
 
 
 def reference_step_ms(rec, nits_full):
@@ -198,6 +223,8 @@ def impl_reference(args):
     vals = [reference_step_ms(r, r["nits"]) for r in timed]
     v = statistics.mean(vals)
     threads = recs[0]["threads"]
+    mean_rec = {k: statistics.mean(r[k] for r in timed) for k in ("t_build", "t_assemble", "t_solve")}
+    mean_rec.update(nits=nits_full, threads=threads)
     line = {
         "impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "ms",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -207,7 +234,8 @@ def impl_reference(args):
                          "sample": "reference OpenMP build (oracle/_ref/phg_dump_omp), the full "
                                    "workload each step: element loop + phgSolverAssemble + FP64 "
                                    "PCG to 1e-8 (%d iterations); mesh import outside the timing"
-                                   % nits_full},
+                                   % nits_full,
+                         "stages": stage_split(mean_rec, nits_full)},
         "e2e": {"value": round(v, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "reference_nits": nits_full,
         "reference_full_solve_ms": round(1e3 * (recs[0]["t_build"] + recs[0]["t_assemble"] +
@@ -353,8 +381,8 @@ def impl_ours(args):
         "metric": METRIC, "value": round(ms, 3), "unit": "ms", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64",
-        "data": "synthetic", "config": dict(workload(m), parallelism="replicas x%d" % world,
-                                            path="mixed: FP32 inner PCG, FP64 reliable updates"),
+        "data": "synthetic", "config": workload(m),
+        "parallelism": "replicas x%d" % world, "path": "mixed: FP32 inner PCG, FP64 reliable updates",
         "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "kernel": "FP32 SpMV (%s layout, unroll %d)" % (tune.get("fp32_layout"), tune.get("fp32_unroll", 0)),
@@ -383,22 +411,48 @@ def impl_ours(args):
         "n": int(n), "nnz": int(nnz),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        try:
-            recs = run_reference(args, m, 1, 0)
-            r0 = recs[0]
-            line["cpu_baseline"] = {
-                "value": round(reference_step_ms(r0, r0["nits"]), 1), "unit": "ms",
-                "cores": r0["threads"], "kind": "reference",
-                "sample": "the full workload once: reference OpenMP build (oracle/_ref/phg_dump_omp), "
-                          "element loop + phgSolverAssemble + FP64 PCG (%d its)" % r0["nits"]}
-        except Exception as ex:  # report, never fail the GPU measurement
-            line["cpu_baseline"] = {"value": None, "unit": "ms", "cores": os.cpu_count(),
-                                    "kind": "reference", "sample": "failed: %s" % ex}
+        line["cpu_baseline"] = cpu_baseline_leg(args, m)
+        # the checker: the FP64 oracle PCG (the reference's recurrence restated
+        # on the CPU) on this matrix, which the parity tests show is the
+        # oracle's own bit for bit; the mixed solution's distance to it
+        line["pcg"].update(oracle_check(s, xm))
     s.close()
     if rank == 0:
         print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
+
+
+def cpu_baseline_leg(args, m):
+    """The reference's OpenMP build on all host threads (the full workload
+    once) and the one-thread sample, with the stage split."""
+    try:
+        r0 = run_reference(args, m, 1, 0)[0]
+        out = {"value": round(reference_step_ms(r0, r0["nits"]), 1), "unit": "ms",
+               "cores": r0["threads"], "kind": "reference",
+               "sample": "the full workload once: reference OpenMP build (oracle/_ref/phg_dump_omp), "
+                         "element loop (OpenMP, as examples/poisson.c) + phgSolverAssemble + FP64 PCG "
+                         "(%d its)" % r0["nits"],
+               "stages": stage_split(r0, r0["nits"])}
+        out["one_thread"] = one_thread_reference(args, m, r0["nits"])
+        return out
+    except Exception as ex:  # report, never fail the GPU measurement
+        return {"value": None, "unit": "ms", "cores": os.cpu_count(), "kind": "reference",
+                "sample": "failed: %s" % ex}
+
+
+def oracle_check(s, xm):
+    """Relative L2 distance of the mixed solution to the FP64 oracle PCG
+    solution of the same system (test infrastructure, run as the checker)."""
+    try:
+        from oracle import pho
+        ptr, cols, vals = s.get_matrix()
+        xo, no, _, _ = pho.pcg(ptr, cols, vals, s.get_diagonal(), s.get_rhs(), rtol=1e-8, btol=0.0,
+                               atol=0.0)
+        return {"rel_l2_vs_oracle": float(np.linalg.norm(xm - xo) / np.linalg.norm(xo)),
+                "oracle_nits": int(no)}
+    except Exception as ex:  # report, never fail the GPU measurement
+        return {"rel_l2_vs_oracle": None, "oracle_check": "failed: %s" % ex}
 
 
 def main():

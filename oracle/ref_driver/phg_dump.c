@@ -177,7 +177,13 @@ main(int argc, char *argv[])
 
 	t0 = phgGetTime(NULL);
 	i = 0;
-	ForAllElements(g, e) {
+	/* the OpenMP build runs the element loop on all threads, as
+	 * examples/poisson.c:116-119 does (serial when dumping fixtures, so
+	 * the element order of the dumps is the grid's) */
+#if USE_OMP
+#pragma omp parallel for private(e) if (!(dump && last))
+#endif
+	ForAllElementsBegin(g, e) {
 	    int a, b, N = DofNBas(u_h, e);
 	    FLOAT A[N][N], B[N], buffer[N], *row;
 	    INT I[N];
@@ -221,9 +227,9 @@ main(int argc, char *argv[])
 		for (a = 0; a < NVert; a++)
 		    elems[e->index * NVert + a] = e->verts[a];
 		order[i] = e->index;
+		i++;
 	    }
-	    i++;
-	}
+	} ForAllElementsEnd
 	t_build = phgGetTime(NULL) - t0;
 
 	if (dump && last) {
