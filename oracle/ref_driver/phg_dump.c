@@ -38,6 +38,21 @@ static INT sample_maxit = 0;		/* > 0: cap PCG iterations after rep 0 */
 static FLOAT mass_coef = 0.;		/* != 0: add mass_coef * mass matrix */
 static const char *rhs_case_names[] = {"sine", "linear", NULL};
 
+#if PHG_GPU_PLUGIN
+/* the GPU OEM solvers (phg_b200/shim/phg_gpu_solver.c), chosen with
+ * -gpu_solver and passed to phgSolverCreate instead of SOLVER_DEFAULT */
+extern OEM_SOLVER phgSolverGpuPCG_, phgSolverGpuPCGMixed_,
+		  phgSolverGpuBiCGstab_, phgSolverGpuGMRES_;
+static INT gpu_solver = 0;
+static const char *gpu_solver_names[] =
+	{"none", "pcg", "pcg_mixed", "bicgstab", "gmres", NULL};
+static OEM_SOLVER *gpu_solvers[] = {NULL, &phgSolverGpuPCG_,
+	&phgSolverGpuPCGMixed_, &phgSolverGpuBiCGstab_, &phgSolverGpuGMRES_};
+#define OEM_CHOICE	gpu_solvers[gpu_solver]
+#else
+#define OEM_CHOICE	SOLVER_DEFAULT
+#endif
+
 static void
 func_f(FLOAT x, FLOAT y, FLOAT z, FLOAT *value)
 {
@@ -132,6 +147,11 @@ main(int argc, char *argv[])
 		"PCG iteration cap for repetitions after the first (timing samples)",
 		&sample_maxit);
 
+#if PHG_GPU_PLUGIN
+    phgOptionsRegisterKeyword("-gpu_solver", "GPU OEM solver (none: PHG's own)",
+		gpu_solver_names, &gpu_solver);
+#endif
+
     phgInit(&argc, &argv);
     if (mesh_file == NULL)
 	phgError(1, "-mesh_file is required\n");
@@ -161,7 +181,7 @@ main(int argc, char *argv[])
     for (rep = 0; rep < repeat; rep++) {
 	BOOLEAN last = (rep == repeat - 1);
 	phgDofSetDataByValue(u_h, 0.0);
-	solver = phgSolverCreate(SOLVER_DEFAULT, u_h, NULL);
+	solver = phgSolverCreate(OEM_CHOICE, u_h, NULL);
 	if (rep > 0 && sample_maxit > 0) {
 	    solver->maxit = sample_maxit;
 	    solver->warn_maxit = FALSE;
@@ -257,6 +277,8 @@ main(int argc, char *argv[])
 	    FILE *fp;
 	    char path[4096];
 	    write_bin("x.f64", u_h->data, sizeof(FLOAT), ndof);
+	    if (solver->mat->diag == NULL)	/* a solver without Jacobi setup */
+		phgMatSetupDiagonal(solver->mat);
 	    write_bin("diag.f64", solver->mat->diag, sizeof(FLOAT), ndof);
 	    write_bin("verts.f64", g->verts, sizeof(FLOAT), 3 * g->nvert);
 	    write_bin("elems.i32", elems, sizeof(INT), NVert * g->nelem);

@@ -11,6 +11,7 @@
 #include "block.h"
 #include "bicgstab.h"
 #include "gmres.h"
+#include "mixed.h"
 
 #include <math.h>
 #include <float.h>
@@ -99,13 +100,6 @@ bool is_device_ptr(const void *ptr) {
         return false;
     }
     return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-}
-
-// x += y unless the correction y was already folded in (y_reset set).
-__global__ void fold_kernel(int64_t n, double *x, const float *y, const MixedState *ms) {
-    if (ms->y_reset) return;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        x[i] += (double)y[i];
 }
 
 __global__ void widen_kernel(int64_t n, const int32_t *in, int64_t *out) {
@@ -261,8 +255,9 @@ struct phgGpuSystem_ {
     double btile_ms[4] = {};
     cudaGraphExec_t graph_block = nullptr;
     GraphKey gkey_block{};
-    DevBuf<MixedState> mst;
-    MixedState *h_mst = nullptr;
+    DevBuf<float> u32, s32;             // mixed solver: u = D^-1 r, s = A p
+    DevBuf<GearState> gst;
+    GearState *h_gst_mixed = nullptr;
     cudaGraphExec_t graph_mixed = nullptr;
     GraphKey gkey_mixed{};
     // BiCGstab: its seven working vectors in one buffer, its state
@@ -362,7 +357,8 @@ int solver_buffers(phgGpuSystem *s) {
     CHECK_RC(s->r.ensure(n));
     CHECK_RC(s->p.ensure(n));
     CHECK_RC(s->Ap.ensure(n));
-    CHECK_RC(s->partials.ensure(2 * (size_t)vec_blocks((int64_t)n * 32) + 64));
+    // grid sums of two or three values over at most kRedMaxBlocks blocks
+    CHECK_RC(s->partials.ensure((size_t)red_partials3_doubles(kRedMaxBlocks) + 64));
     CHECK_RC(s->sums.ensure(2));
     CHECK_RC(s->st.ensure(1));
     CHECK_RC(s->ticket.ensure(kRedTickets));
@@ -747,7 +743,7 @@ int phgGpuDestroy(phgGpuSystem *s) {
     if (s->stream != nullptr) cudaStreamSynchronize(s->stream);
     if (s->graph != nullptr) cudaGraphExecDestroy(s->graph);
     if (s->graph_mixed != nullptr) cudaGraphExecDestroy(s->graph_mixed);
-    if (s->h_mst) cudaFreeHost(s->h_mst);
+    if (s->h_gst_mixed) cudaFreeHost(s->h_gst_mixed);
     if (s->graph_bicg != nullptr) cudaGraphExecDestroy(s->graph_bicg);
     if (s->h_bst) cudaFreeHost(s->h_bst);
     if (s->graph_gmres != nullptr) cudaGraphExecDestroy(s->graph_gmres);
@@ -762,7 +758,7 @@ int phgGpuDestroy(phgGpuSystem *s) {
     s->sell2_order.release(); s->sell2_perm.release(); s->sell2_width.release(); s->sell2_len.release();
     for (auto *b : fbufs) b->release();
     s->sell_perm.release(); s->sell_ssz.release(); s->sell_sptr.release(); s->sell_cols.release();
-    s->sell_len.release(); s->sell_vals.release(); s->mst.release();
+    s->sell_len.release(); s->sell_vals.release(); s->gst.release(); s->u32.release(); s->s32.release();
     DevBuf<int32_t> *qi[] = {&s->q16_ssz, &s->q16_sptr, &s->q16_perm, &s->q16_b0, &s->q16_b1};
     for (auto *b : qi) b->release();
     DevBuf<uint16_t> *qu[] = {&s->q16_len, &s->q16_split, &s->q16_cols};
@@ -1104,12 +1100,13 @@ int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol,
     CHECK_RC(s->Ap32.ensure(un));
     CHECK_RC(s->y32.ensure(un));
     CHECK_RC(s->D32.ensure(un));
-    CHECK_RC(s->mst.ensure(1));
-    if (s->h_mst == nullptr) CK(cudaMallocHost((void **)&s->h_mst, sizeof(MixedState)));
+    CHECK_RC(s->u32.ensure(un));
+    CHECK_RC(s->s32.ensure(un));
+    CHECK_RC(s->gst.ensure(1));
+    if (s->h_gst_mixed == nullptr) CK(cudaMallocHost((void **)&s->h_gst_mixed, sizeof(GearState)));
     CHECK_RC(copy_in(s, s->x.p, x, un));
     CK(cudaMemsetAsync(s->ticket.p, 0, sizeof(unsigned) * kRedTickets, s->stream));
     CHECK_RC(tune_spmv32(s));   // builds the chosen FP32 layout for this matrix
-    const int unroll = s->unroll32;
     if (s->plan.kind == SPMV_Q16) CHECK_RC(ensure_q16(s));   // the FP64 plan's layout (checked by tune_spmv)
     const bool q16 = s->kind32 == 2;
     // FP64 products (residuals): the q16 layout's FP64 values, or the FP64
@@ -1138,8 +1135,29 @@ int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol,
     double tol = -1.0;
     int nits_total = 0, nupd = 0;
     double res_true = 0.0;
-    MixedBuffers B{n, s->x.p, s->r.p, s->r32.p, s->p32.p, s->Ap32.p, s->y32.p, s->D32.p, s->partials.p, s->mst.p,
-                   nullptr};
+    const GearBuffers B{n, s->x.p, s->r.p, s->r32.p, s->u32.p, s->Ap32.p, s->p32.p, s->s32.p, s->y32.p, s->D32.p,
+                        s->partials.p, s->gst.p};
+    const GearLayouts L{s->kind32, s->unroll32, sell_view(s), sell2_view(s), Q};
+    // the solve's graph, captured again when a buffer or the layout changed
+    phgGpuSystem_::GraphKey key{};
+    key.x = s->x.p; key.r = s->r32.p; key.p = s->p32.p; key.Ap = s->Ap32.p; key.D = s->D32.p;
+    key.n = n; key.lpr = s->unroll32 + 100 * s->kind32;
+    key.s = s->stream;
+    if (q16) {
+        key.va = Q.vals32; key.hist = Q.vals64;
+        const void *e[8] = {Q.cols, Q.perm, Q.len, Q.split, Q.base0, Q.base1, Q.sptr, s->partials.p};
+        memcpy(key.extra, e, sizeof(e));
+    } else {
+        key.va = s->sell2_vals.p; key.hist = s->sell_cols.p;
+        const void *e[8] = {s->sell2_cols.p, s->sell2_perm.p, s->u32.p, s->sell2_sptr.p,
+                            s->sell_vals.p, s->sell_vals32.p, s->s32.p, s->partials.p};
+        memcpy(key.extra, e, sizeof(e));
+    }
+    if (s->graph_mixed == nullptr || !(s->gkey_mixed == key)) {
+        if (s->graph_mixed != nullptr) { cudaGraphExecDestroy(s->graph_mixed); s->graph_mixed = nullptr; }
+        CK(build_gear_graph(B, L, kGraphChunk, s->stream, &s->graph_mixed, nullptr));
+        s->gkey_mixed = key;
+    }
     // the explicit FP64 residual b - A x is checked at the end; a recurrence
     // that drifted above the tolerance restarts from it (at most twice)
     for (int restart = 0; restart < 3; restart++) {
@@ -1150,83 +1168,40 @@ int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol,
         } else {
             CK(cudaMemcpyAsync(s->r.p, s->rhs.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, s->stream));
         }
-        CK(launch_mixed_init(n, s->r.p, s->r32.p, s->y32.p, s->diag.p, s->D32.p, s->partials.p, s->ticket.p,
-                             s->sums.p, s->stream));
+        CK(launch_gear_init(B, s->diag.p, s->ticket.p, s->sums.p, s->stream));
         s->launches += 1;
         CK(cudaMemcpyAsync(s->h_sums, s->sums.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
         CK(cudaStreamSynchronize(s->stream));
-        const double r0 = sqrt(s->h_sums[0]), rz0 = s->h_sums[1];
-        if (!isfinite(rz0)) return fail(PHG_GPU_ERR_NAN, "phgGpuSolverPCGMixed: zero or non-finite diagonal");
+        const double r0 = sqrt(s->h_sums[0]), ru0 = s->h_sums[1];
+        if (!isfinite(ru0)) return fail(PHG_GPU_ERR_NAN, "phgGpuSolverPCGMixed: zero or non-finite diagonal");
         if (tol < 0.0) {   // get_tol (solver-phg.c:104-115) on the initial residual
             tol = r0 * rtol;
             if (tol < rb * btol) tol = rb * btol;
             if (tol < atol) tol = atol;
         }
-        MixedState m{};
-        m.pcg.rz_cur = rz0;
-        m.pcg.residual = r0;
-        m.pcg.tol = tol;
-        m.pcg.maxit = maxit - nits_total;
-        m.pcg.done = !(r0 > tol && nits_total < maxit);
-        m.maxr = r0;
-        m.delta = 0.1;
-        m.y_reset = 1;
-        *s->h_mst = m;
-        CK(cudaMemcpyAsync(s->mst.p, s->h_mst, sizeof(MixedState), cudaMemcpyHostToDevice, s->stream));
-
-        phgGpuSystem_::GraphKey key{};
-        key.x = s->x.p; key.r = s->r32.p; key.p = s->p32.p; key.Ap = s->Ap32.p; key.D = s->D32.p;
-        key.n = n; key.lpr = unroll + 100 * s->kind32;
-        key.s = s->stream;
-        if (q16) {
-            key.va = Q.vals32; key.hist = Q.vals64;
-            const void *e[8] = {Q.cols, Q.perm, Q.len, Q.split, Q.base0, Q.base1, Q.sptr, s->partials.p};
-            memcpy(key.extra, e, sizeof(e));
-        } else {
-            key.va = s->sell2_vals.p; key.hist = s->sell_cols.p;
-            const void *e[8] = {s->sell2_cols.p, s->sell2_perm.p, s->sell2_len.p, s->sell2_sptr.p,
-                                s->sell_vals.p, s->sell_vals32.p, s->sell_sptr.p, s->partials.p};
-            memcpy(key.extra, e, sizeof(e));
-        }
-        if (s->graph_mixed == nullptr || !(s->gkey_mixed == key)) {
-            if (s->graph_mixed != nullptr) { cudaGraphExecDestroy(s->graph_mixed); s->graph_mixed = nullptr; }
-            cudaGraph_t gr;
-            CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-            for (int i = 0; i < kGraphChunk; i++) {
-                if (q16) launch_mixed_iteration_q16(B, Q, unroll, s->stream);
-                else launch_mixed_iteration2(B, sell_view(s), sell2_view(s), s->kind32, unroll, s->stream);
-            }
-            CK(cudaStreamEndCapture(s->stream, &gr));
-            cudaError_t e = cudaGraphInstantiate(&s->graph_mixed, gr, 0);
-            cudaGraphDestroy(gr);
-            CK(e);
-            s->gkey_mixed = key;
-        }
-        while (!s->h_mst->pcg.done) {
-            CK(cudaGraphLaunch(s->graph_mixed, s->stream));
-            s->launches += 4 * kGraphChunk;
-            CK(cudaMemcpyAsync(s->h_mst, s->mst.p, sizeof(MixedState), cudaMemcpyDeviceToHost, s->stream));
-            CK(cudaStreamSynchronize(s->stream));
-        }
-        const MixedState &hm = *s->h_mst;
-        nits_total += hm.pcg.nits;
-        nupd += hm.nupdates;
-        fold_kernel<<<vec_blocks(n), 256, 0, s->stream>>>(n, s->x.p, s->y32.p, s->mst.p);
-        s->launches += 1;
-        if (hm.pcg.status == PCG_NONFINITE) return fail(PHG_GPU_ERR_NAN, "mixed PCG: non-finite residual");
-        if (hm.pcg.status == PCG_BREAKDOWN) {
-            // as the FP64 PCG: warn, keep the iterate, report the FP64 residual
-            warn("mixed PCG stopped after %d iterations: the matrix may not be SPD", nits_total);
-            CK(product64(s->x.p, s->Ap.p));
-            CK(launch_residual(n, s->rhs.p, s->Ap.p, s->r.p, s->stream));
-            CK(launch_init_sums(n, 1, s->x.p, s->r.p, s->diag.p, s->partials.p, s->ticket.p, s->sums.p,
-                                s->stream));
-            s->launches += 3;
-            CK(cudaMemcpyAsync(s->h_sums, s->sums.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
-            CK(cudaStreamSynchronize(s->stream));
-            res_true = sqrt(s->h_sums[0]);
-            break;
-        }
+        GearState g{};
+        g.tol = tol;
+        g.maxit = maxit - nits_total;
+        g.maxr = r0;
+        g.delta = 0.1;
+        g.residual = r0;
+        g.first = 1;
+        g.y_reset = 1;
+        g.done = !(r0 > tol && nits_total < maxit);
+        g.max_passes = g.maxit / kGraphChunk + 3;
+        *s->h_gst_mixed = g;
+        CK(cudaMemcpyAsync(s->gst.p, s->h_gst_mixed, sizeof(GearState), cudaMemcpyHostToDevice, s->stream));
+        if (!g.done) CK(cudaGraphLaunch(s->graph_mixed, s->stream));
+        CK(cudaMemcpyAsync(s->h_gst_mixed, s->gst.p, sizeof(GearState), cudaMemcpyDeviceToHost, s->stream));
+        CK(launch_gear_fold(B, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        const GearState &hg = *s->h_gst_mixed;
+        s->launches += 2 * (int64_t)hg.nits + 2 * (int64_t)hg.nupdates + hg.passes + 1;
+        nits_total += hg.nits;
+        nupd += hg.nupdates;
+        if (hg.status == PCG_NONFINITE) return fail(PHG_GPU_ERR_NAN, "mixed PCG: non-finite residual");
+        if (hg.status == GEAR_PASS_LIMIT)
+            return fail(PHG_GPU_ERR_STATE, "mixed PCG: the iteration loop exceeded its pass bound");
         // explicit FP64 residual of the accumulated solution
         CK(product64(s->x.p, s->Ap.p));
         CK(launch_residual(n, s->rhs.p, s->Ap.p, s->r.p, s->stream));
@@ -1235,6 +1210,11 @@ int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol,
         CK(cudaMemcpyAsync(s->h_sums, s->sums.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
         CK(cudaStreamSynchronize(s->stream));
         res_true = sqrt(s->h_sums[0]);
+        if (hg.status == PCG_BREAKDOWN) {
+            // as the FP64 PCG: warn, keep the iterate, report its FP64 residual
+            warn("mixed PCG stopped after %d iterations: the matrix may not be SPD", nits_total);
+            break;
+        }
         if (!(res_true > tol) || nits_total >= maxit) break;
         x_nonzero = true;
     }

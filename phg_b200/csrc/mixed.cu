@@ -1,0 +1,383 @@
+// Mixed-precision Jacobi-PCG with one grid-wide reduction per iteration.
+//
+// The recurrence is the single-reduction form of preconditioned CG
+// (Chronopoulos and Gear): with u = D^-1 r, w = A u and s = A p kept by
+// recurrence,
+//   gamma = r.u, delta = w.u
+//   beta  = gamma / gamma_prev,  alpha = gamma / (delta - beta gamma / alpha_prev)
+//   p = u + beta p,  s = w + beta s,  y += alpha p,  r -= alpha s,  u = D^-1 r
+// In exact arithmetic it produces the iterates of solver_pcg
+// (solver-phg.c:485-604); its three dot products (gamma, delta and ||r||^2)
+// are summed in the epilogue of the one matrix-vector product of the
+// iteration, so an iteration is two kernels:
+//   K1  w = A u (FP32 values and vectors), then gamma, delta, ||r||^2 in FP64
+//       (one grid sum); the last block decides the step's alpha and beta,
+//       or that a reliable update is due
+//   K2  the vector update above, no reduction
+// A reliable update (the FP32 residual has fallen tenfold since the last one,
+// or the iteration looks converged) runs inside a conditional graph node:
+//   R1  x += y (FP64), rtrue -= A y with the FP64 matrix values, r = (float)
+//       rtrue, u = D^-1 r, ||rtrue||^2 -> the stopping test on the FP64
+//       residual (the reference's rule, get_tol solver-phg.c:104)
+//   R2  K1 again on the new u
+// The iterations run in a conditional WHILE loop of `chunk` iterations per
+// pass, so a solve is one graph launch and the host waits once.
+#include "common.cuh"
+#include "mixed.h"
+#include "reduce.cuh"
+#include "rows.cuh"
+
+#include <math.h>
+
+namespace phgb {
+
+// ---------------------------------------------------------------------------
+// The scalar decisions, taken by the one thread that finishes a grid sum.
+
+__device__ __forceinline__ void gear_breakdown(GearState *st) {
+    st->done = 1;
+    st->status = PCG_BREAKDOWN;
+    st->nits += 1;   // the reference counts the step it breaks down in (solver-phg.c:537)
+}
+
+// gamma = r.u, delta = w.u, rr = r.r of the current vectors.  AFTER_RU: the
+// product that follows a reliable update (the stopping test was just done on
+// the FP64 residual).  Returns whether a reliable update is due.
+template <bool AFTER_RU>
+__device__ __forceinline__ bool gear_final(GearState *st, double gamma, double delta, double rr) {
+    const double res = sqrt(rr);
+    if (!(isfinite(res) && isfinite(gamma) && isfinite(delta))) {
+        st->done = 1;
+        st->status = PCG_NONFINITE;
+        st->residual = res;
+        return false;
+    }
+    if (!AFTER_RU) {
+        st->y_reset = 0;   // the previous update kernel has consumed it
+        st->residual = res;
+        const bool conv = !(res > st->tol) || st->nits >= st->maxit;
+        if (conv || res < st->delta * st->maxr) {
+            st->final_check = conv ? 1 : 0;
+            return true;
+        }
+    }
+    double alpha, beta;
+    if (st->first) {
+        if (delta == 0.0) { gear_breakdown(st); return false; }
+        beta = 0.0;
+        alpha = gamma / delta;
+    } else {
+        if (st->gamma_prev == 0.0) { gear_breakdown(st); return false; }
+        beta = gamma / st->gamma_prev;
+        const double den = delta - beta * gamma / st->alpha_prev;
+        if (den == 0.0) { gear_breakdown(st); return false; }
+        alpha = gamma / den;
+    }
+    st->alpha = alpha;
+    st->beta = beta;
+    st->gamma_prev = gamma;
+    st->alpha_prev = alpha;
+    st->first = 0;
+    st->nits += 1;
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// K1 / R2: w = A u with the three dot products.  Grid-stride over slices,
+// at most 8 blocks of 256 threads per SM.
+template <class L, bool AFTER_RU>
+__global__ void __launch_bounds__(kVecThreads, kResidentBlocks)
+gear_spmv_kernel(const L lay, const GearBuffers B, cudaGraphConditionalHandle hif) {
+    GearState *st = B.st;
+    if (st->done) return;
+    grid_sum3_init();
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * kVecThreads + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * kVecThreads) >> 5;
+    double v[3] = {0.0, 0.0, 0.0};
+    const int64_t nsl = lay.nslices();
+    for (int64_t s = warp; s < nsl; s += nwarps) {
+        const int64_t pos = s * 32 + lane;
+        const int32_t row = lay.row(pos);
+        const float acc = lay.sum(s, lane, pos, B.u);
+        if (row >= 0) {
+            B.w[row] = acc;
+            const double ri = (double)B.r[row], ui = (double)B.u[row];
+            v[0] += ri * ui;
+            v[1] += (double)acc * ui;
+            v[2] += ri * ri;
+        }
+    }
+    if (grid_sum3(v, B.partials, st->ticket)) {
+        const bool ru = gear_final<AFTER_RU>(st, v[0], v[1], v[2]);
+        if (!AFTER_RU) cudaGraphSetConditional(hif, ru ? 1u : 0u);
+    }
+}
+
+// R1: the reliable update with the FP64 matrix values.
+template <class L64>
+__global__ void __launch_bounds__(kVecThreads, 6)
+gear_reliable_kernel(const L64 lay, const GearBuffers B) {
+    GearState *st = B.st;
+    if (st->done) return;
+    grid_sum_init();
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * kVecThreads + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * kVecThreads) >> 5;
+    double rr = 0.0, dummy = 0.0;
+    const int64_t nsl = lay.nslices();
+    for (int64_t s = warp; s < nsl; s += nwarps) {
+        const int64_t pos = s * 32 + lane;
+        const int32_t row = lay.row(pos);
+        const double acc = lay.sum(s, lane, pos, B.y);
+        if (row >= 0) {
+            B.x[row] += (double)B.y[row];
+            const double rt = B.rtrue[row] - acc;
+            B.rtrue[row] = rt;
+            const float rf = (float)rt;
+            B.r[row] = rf;
+            B.u[row] = rf / B.D[row];
+            rr += rt * rt;
+        }
+    }
+    if (grid_sum2(rr, dummy, B.partials, st->ticket)) {
+        const double res = sqrt(rr);
+        st->residual = res;
+        st->maxr = res;
+        st->y_reset = 1;
+        st->nupdates += 1;
+        st->final_check = 0;
+        if (!isfinite(res)) {
+            st->done = 1;
+            st->status = PCG_NONFINITE;
+        } else if (!(res > st->tol) || st->nits >= st->maxit) {
+            st->done = 1;   // the FP64 residual meets the tolerance, or maxit
+        }
+    }
+}
+
+// K2: the vector update, 16-byte vectors of four rows, no reduction.
+__global__ void __launch_bounds__(kVecThreads)
+gear_update_kernel(const GearBuffers B) {
+    const GearState *st = B.st;
+    if (st->done) return;
+    const float a = (float)st->alpha, b = (float)st->beta;
+    const bool reset = st->y_reset != 0;
+    const int64_t n = B.n;
+    const int nfull = aligned16(B.r, B.u, B.w, B.p, B.s, B.y, B.D) ? (int)(n / 4) : 0;   // n < 2^31
+    const int stride = gridDim.x * blockDim.x;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nfull; c += stride) {
+        const int i = 4 * c;
+        VArr<float> u = vload(B.u + i), p = vload(B.p + i), w = vload_ro(B.w + i), s = vload(B.s + i);
+        VArr<float> y = reset ? VArr<float>{{0.0f, 0.0f, 0.0f, 0.0f}} : vload(B.y + i);
+        VArr<float> r = vload(B.r + i);
+        const VArr<float> d = vload_ro(B.D + i);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            p.v[q] = u.v[q] + b * p.v[q];
+            s.v[q] = w.v[q] + b * s.v[q];
+            y.v[q] = y.v[q] + a * p.v[q];
+            r.v[q] = r.v[q] - a * s.v[q];
+            u.v[q] = r.v[q] / d.v[q];
+        }
+        vstore(B.p + i, p);
+        vstore(B.s + i, s);
+        vstore(B.y + i, y);
+        vstore(B.r + i, r);
+        vstore(B.u + i, u);
+    }
+    for (int64_t i = (int64_t)nfull * 4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const float p = B.u[i] + b * B.p[i], s = B.w[i] + b * B.s[i];
+        B.p[i] = p;
+        B.s[i] = s;
+        B.y[i] = (reset ? 0.0f : B.y[i]) + a * p;
+        const float r = B.r[i] - a * s;
+        B.r[i] = r;
+        B.u[i] = r / B.D[i];
+    }
+}
+
+// One pass of the graph loop is over: stop when done, or when the passes
+// exceed the bound the iteration limit gives (a safeguard: every pass takes
+// `chunk` steps until done).
+__global__ void gear_loop_kernel(GearState *st, cudaGraphConditionalHandle hwhile) {
+    st->passes += 1;
+    if (!st->done && st->passes > st->max_passes) {
+        st->done = 1;
+        st->status = GEAR_PASS_LIMIT;
+    }
+    cudaGraphSetConditional(hwhile, st->done ? 0u : 1u);
+}
+
+__global__ void __launch_bounds__(kVecThreads)
+gear_init_kernel(const GearBuffers B, const double *__restrict__ D64, unsigned *ticket, double *out) {
+    grid_sum_init();
+    double rr = 0.0, ru = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < B.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double rt = B.rtrue[i];
+        const float rf = (float)rt, df = (float)D64[i];
+        const float uf = rf / df;
+        B.r[i] = rf;
+        B.u[i] = uf;
+        B.D[i] = df;
+        B.y[i] = 0.0f;
+        B.p[i] = 0.0f;
+        B.s[i] = 0.0f;
+        rr += rt * rt;
+        ru += (double)rf * (double)uf;
+    }
+    if (grid_sum2(rr, ru, B.partials, ticket)) { out[0] = rr; out[1] = ru; }
+}
+
+__global__ void gear_fold_kernel(const GearBuffers B) {
+    if (B.st->y_reset) return;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < B.n; i += (int64_t)gridDim.x * blockDim.x)
+        B.x[i] += (double)B.y[i];
+}
+
+// ---------------------------------------------------------------------------
+// Host side.
+
+static int update_blocks(int64_t n) {
+    int64_t b = ceil_div(ceil_div(n, 4), kVecThreads);
+    if (b > 148 * 4) b = 148 * 4;
+    return b < 1 ? 1 : (int)b;
+}
+
+cudaError_t launch_gear_init(const GearBuffers &B, const double *D64, unsigned *ticket, double *out,
+                             cudaStream_t s) {
+    gear_init_kernel<<<vec_blocks(B.n), kVecThreads, 0, s>>>(B, D64, ticket, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gear_fold(const GearBuffers &B, cudaStream_t s) {
+    gear_fold_kernel<<<vec_blocks(B.n), kVecThreads, 0, s>>>(B);
+    return cudaGetLastError();
+}
+
+// Captures the launches `f` makes on `st` into `g` after `dep` (none if
+// null); *last gets the node the capture ended with.
+template <typename F>
+static cudaError_t capture_into(cudaStream_t st, cudaGraph_t g, cudaGraphNode_t dep, F &&f, cudaGraphNode_t *last) {
+    cudaError_t e = cudaStreamBeginCaptureToGraph(st, g, dep != nullptr ? &dep : nullptr, nullptr, dep != nullptr ? 1 : 0,
+                                                  cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    f();
+    cudaError_t le = cudaGetLastError();
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    cudaError_t ie = cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &nd);
+    cudaGraphNode_t ln = (ie == cudaSuccess && nd == 1) ? deps[0] : nullptr;
+    cudaGraph_t out = nullptr;
+    e = cudaStreamEndCapture(st, &out);
+    if (le != cudaSuccess) return le;
+    if (ie != cudaSuccess) return ie;
+    if (e != cudaSuccess) return e;
+    if (ln == nullptr) return cudaErrorStreamCaptureUnjoined;
+    *last = ln;
+    return cudaSuccess;
+}
+
+// Adds a conditional node of `type` on handle h after dep; *body gets its graph.
+static cudaError_t add_conditional(cudaGraph_t g, cudaGraphNode_t dep, cudaGraphConditionalHandle h,
+                                   cudaGraphConditionalNodeType type, cudaGraphNode_t *node, cudaGraph_t *body) {
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = type;
+    np.conditional.size = 1;
+    cudaError_t e = cudaGraphAddNode(node, g, dep != nullptr ? &dep : nullptr, dep != nullptr ? 1 : 0, &np);
+    if (e != cudaSuccess) return e;
+    *body = np.conditional.phGraph_out[0];
+    return cudaSuccess;
+}
+
+// The iteration's kernels for FP32 layout L32 and FP64 layout L64.
+template <class L32, class L64>
+static cudaError_t build_body(const GearBuffers &B, const L32 &l32, const L64 &l64, int chunk, cudaStream_t stream,
+                              cudaGraph_t body, cudaGraphConditionalHandle hwhile) {
+    const int sb = vec_blocks(l32.nslices_host * 32);
+    const int rb = sb < 148 * 6 ? sb : 148 * 6;   // the reliable kernel holds 6 blocks per SM
+    const int ub = update_blocks(B.n);
+    cudaGraphNode_t prev = nullptr;
+    for (int i = 0; i < chunk; i++) {
+        cudaGraphConditionalHandle hif;
+        cudaError_t e = cudaGraphConditionalHandleCreate(&hif, body, 0, 0);
+        if (e != cudaSuccess) return e;
+        cudaGraphNode_t k1, ifn, k2;
+        e = capture_into(stream, body, prev, [&] {
+            gear_spmv_kernel<typename L32::Dev, false><<<sb, kVecThreads, 0, stream>>>(l32.dev, B, hif);
+        }, &k1);
+        if (e != cudaSuccess) return e;
+        cudaGraph_t ifbody;
+        e = add_conditional(body, k1, hif, cudaGraphCondTypeIf, &ifn, &ifbody);
+        if (e != cudaSuccess) return e;
+        cudaGraphNode_t r2;
+        e = capture_into(stream, ifbody, nullptr, [&] {
+            gear_reliable_kernel<L64><<<rb, kVecThreads, 0, stream>>>(l64, B);
+            gear_spmv_kernel<typename L32::Dev, true><<<sb, kVecThreads, 0, stream>>>(l32.dev, B, hif);
+        }, &r2);
+        if (e != cudaSuccess) return e;
+        e = capture_into(stream, body, ifn, [&] {
+            gear_update_kernel<<<ub, kVecThreads, 0, stream>>>(B);
+        }, &k2);
+        if (e != cudaSuccess) return e;
+        prev = k2;
+    }
+    cudaGraphNode_t lk;
+    return capture_into(stream, body, prev, [&] { gear_loop_kernel<<<1, 1, 0, stream>>>(B.st, hwhile); }, &lk);
+}
+
+// A device layout functor with the slice count known on the host.
+template <class D>
+struct HostLayout {
+    using Dev = D;
+    D dev;
+    int64_t nslices_host;
+};
+
+cudaError_t build_gear_graph(const GearBuffers &B, const GearLayouts &L, int chunk, cudaStream_t stream,
+                             cudaGraphExec_t *exec, int *kernels_per_iteration) {
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaGraphCreate(&g, 0);
+    if (e != cudaSuccess) return e;
+    cudaGraphConditionalHandle hw;
+    cudaGraphNode_t wnode;
+    cudaGraph_t body = nullptr;
+    e = cudaGraphConditionalHandleCreate(&hw, g, 1, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) e = add_conditional(g, nullptr, hw, cudaGraphCondTypeWhile, &wnode, &body);
+    if (e == cudaSuccess) {
+        const int64_t nsl = L.S.nslices;
+        const SellRows<double, double, 4> sell64{nsl, L.S.perm, L.S.len, L.S.sptr, L.S.cols, L.S.vals};
+        if (L.kind == 2) {
+            const Q16Rows64 q64{L.Q};
+            if (L.unroll == 2)
+                e = build_body(B, HostLayout<Q16Rows32<2>>{{L.Q}, L.Q.nslices}, q64, chunk, stream, body, hw);
+            else
+                e = build_body(B, HostLayout<Q16Rows32<1>>{{L.Q}, L.Q.nslices}, q64, chunk, stream, body, hw);
+        } else if (L.kind == 1) {
+            switch (L.unroll) {
+            case 2: e = build_body(B, HostLayout<PairRows32<2>>{{nsl, L.S2}, nsl}, sell64, chunk, stream, body, hw); break;
+            case 8: e = build_body(B, HostLayout<PairRows32<8>>{{nsl, L.S2}, nsl}, sell64, chunk, stream, body, hw); break;
+            default: e = build_body(B, HostLayout<PairRows32<4>>{{nsl, L.S2}, nsl}, sell64, chunk, stream, body, hw); break;
+            }
+        } else {
+            using S32_4 = SellRows<float, float, 4>;
+            using S32_8 = SellRows<float, float, 8>;
+            using S32_16 = SellRows<float, float, 16>;
+            switch (L.unroll) {
+            case 8: e = build_body(B, HostLayout<S32_8>{{nsl, L.S.perm, L.S.len, L.S.sptr, L.S.cols, L.S.vals32}, nsl}, sell64, chunk, stream, body, hw); break;
+            case 16: e = build_body(B, HostLayout<S32_16>{{nsl, L.S.perm, L.S.len, L.S.sptr, L.S.cols, L.S.vals32}, nsl}, sell64, chunk, stream, body, hw); break;
+            default: e = build_body(B, HostLayout<S32_4>{{nsl, L.S.perm, L.S.len, L.S.sptr, L.S.cols, L.S.vals32}, nsl}, sell64, chunk, stream, body, hw); break;
+            }
+        }
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    if (kernels_per_iteration != nullptr) *kernels_per_iteration = 2;
+    return e;
+}
+
+}  // namespace phgb

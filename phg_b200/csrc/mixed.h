@@ -1,0 +1,58 @@
+// Mixed-precision Jacobi-PCG with one grid reduction per iteration
+// (mixed.cu): FP32 matrix, Krylov vectors and products, FP64 dot products,
+// FP64 reliable updates, the whole solve in one CUDA graph launch.
+#pragma once
+#include "solve.h"
+
+namespace phgb {
+
+// Device-resident scalars of one solve.
+struct GearState {
+    double alpha, beta;             // scalars of the step the update kernel takes next
+    double gamma_prev, alpha_prev;  // r.u and alpha of the previous step
+    double tol, maxr, delta, residual;
+    int nits, maxit, done, status, first, y_reset, final_check, nupdates, passes, max_passes;
+    unsigned ticket[kRedTickets];
+};
+
+enum { GEAR_PASS_LIMIT = 3 };       // status: the graph loop ran out of passes
+
+// Working vectors: x and rtrue FP64; r, u = r / D, w = A u, p, s = A p and
+// the correction y FP32.
+struct GearBuffers {
+    int64_t n;
+    double *x, *rtrue;
+    float *r, *u, *w, *p, *s, *y, *D;
+    double *partials;   // red_partials3_doubles(kRedMaxBlocks)
+    GearState *st;
+};
+
+// The FP32 product layout of the iteration (kind 0 SELL, 1 pair SELL, 2 q16,
+// with its unroll) and the FP64 values the reliable updates use (the q16
+// layout's for kind 2, the SELL copy's otherwise).
+struct GearLayouts {
+    int kind, unroll;
+    SellView S;
+    Sell2View S2;
+    Q16View Q;
+};
+
+// Grid-sum workspace of three sums (reduce.cuh) for `blocks` blocks.
+constexpr int64_t red_partials3_doubles(int64_t blocks) {
+    return 3 * (blocks + (blocks + kRedGroup - 1) / kRedGroup);
+}
+
+// r = (float) rtrue, u = r / D, D32 = (float) D64, y = p = s = 0, and
+// (||rtrue||^2, r.u) into out[0..1].
+cudaError_t launch_gear_init(const GearBuffers &B, const double *D64, unsigned *ticket, double *out,
+                             cudaStream_t s);
+// Builds the executable graph of a whole solve: a loop (conditional WHILE
+// node) over `chunk` iterations, each the FP32 product with its dot products,
+// a conditional reliable update, and the vector update; the loop ends when the
+// state says done.  Graph construction uses `stream` for capture.
+cudaError_t build_gear_graph(const GearBuffers &B, const GearLayouts &L, int chunk, cudaStream_t stream,
+                             cudaGraphExec_t *exec, int *kernels_per_iteration);
+// x += y unless the correction was already folded in.
+cudaError_t launch_gear_fold(const GearBuffers &B, cudaStream_t s);
+
+}  // namespace phgb

@@ -165,40 +165,6 @@ q16_spmv64_kernel(const Q16View Q, const double *__restrict__ x, double *__restr
     if (grid_sum2(dot, dummy, partials, st->ticket)) pcg_pap_final(dot, st);
 }
 
-// Reliable update of the mixed solver on this layout (FP64 values): x += y,
-// r_true -= A y, r32 = (float) r_true, ||r_true||^2 and r32.(r32 / D).
-// Its FP64 row sums need more than 32 registers a thread: six resident
-// blocks per SM, and a grid of 148 x 6 blocks to match.
-constexpr int kReliableBlocks = 6;
-
-__global__ void __launch_bounds__(kVecThreads, kReliableBlocks)
-q16_reliable_kernel(const Q16View Q, double *__restrict__ x, const float *__restrict__ y, double *__restrict__ rtrue,
-                    float *__restrict__ r32, const float *__restrict__ D, double *partials, MixedState *ms,
-                    double *hist) {
-    PcgState *st = &ms->pcg;
-    if (st->done || !ms->ru_flag) return;
-    grid_sum_init();
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = ((int64_t)blockIdx.x * kVecThreads + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * kVecThreads) >> 5;
-    double rr = 0.0, rz = 0.0;
-    for (int64_t s = warp; s < Q.nslices; s += nwarps) {
-        const int64_t pos = s * 32 + lane;
-        const int32_t row = Q.perm[pos];
-        const double acc = q16_row64(Q, s, lane, Q.len[pos], Q.split[pos], Q.base0[pos], Q.base1[pos], y);
-        if (row >= 0) {
-            x[row] += (double)y[row];
-            const double rt = rtrue[row] - acc;
-            rtrue[row] = rt;
-            const float rf = (float)rt;
-            r32[row] = rf;
-            rr += rt * rt;
-            rz += (double)rf * (double)(rf / D[row]);
-        }
-    }
-    if (grid_sum2(rr, rz, partials, st->ticket)) mixed_reliable_final(rr, rz, ms, hist);
-}
-
 cudaError_t launch_q16_sizes(int64_t nslices, const uint16_t *sell_len, const int32_t *order, int32_t *size,
                              cudaStream_t s) {
     q16_sizes_kernel<<<vec_blocks(nslices), kVecThreads, 0, s>>>(nslices, sell_len, order, size);
@@ -224,16 +190,6 @@ cudaError_t launch_q16_spmv32(const Q16View &Q, int unroll, const float *x, floa
     return cudaGetLastError();
 }
 
-cudaError_t launch_q16_spmv32_dot(const Q16View &Q, int unroll, const float *x, float *y, double *partials,
-                                  PcgState *st, cudaStream_t s) {
-    const int sb = vec_blocks(Q.nslices * 32);
-    if (unroll == 2)
-        q16_spmv32_kernel<true, 2><<<sb, kVecThreads, 0, s>>>(Q, x, y, partials, st);
-    else
-        q16_spmv32_kernel<true, 1><<<sb, kVecThreads, 0, s>>>(Q, x, y, partials, st);
-    return cudaGetLastError();
-}
-
 cudaError_t launch_q16_spmv64(const Q16View &Q, const double *x, double *y, cudaStream_t s) {
     q16_spmv64_kernel<false><<<vec_blocks(Q.nslices * 32), kVecThreads, 0, s>>>(Q, x, y, nullptr, nullptr);
     return cudaGetLastError();
@@ -242,13 +198,6 @@ cudaError_t launch_q16_spmv64(const Q16View &Q, const double *x, double *y, cuda
 cudaError_t launch_q16_spmv64_dot(const Q16View &Q, const double *x, double *y, double *partials, PcgState *st,
                                   cudaStream_t s) {
     q16_spmv64_kernel<true><<<vec_blocks(Q.nslices * 32), kVecThreads, 0, s>>>(Q, x, y, partials, st);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_q16_reliable(const Q16View &Q, const MixedBuffers &B, cudaStream_t s) {
-    const int sb = std::min(vec_blocks(Q.nslices * 32), 148 * kReliableBlocks);
-    q16_reliable_kernel<<<sb, kVecThreads, 0, s>>>(Q, B.x, B.y32, B.rtrue, B.r32, B.D32, B.partials, B.ms,
-                                                   B.hist);
     return cudaGetLastError();
 }
 

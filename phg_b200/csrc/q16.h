@@ -34,15 +34,4 @@ cudaError_t launch_q16_spmv64(const Q16View &Q, const double *x, double *y, cuda
 cudaError_t launch_q16_spmv64_dot(const Q16View &Q, const double *x, double *y, double *partials, PcgState *st,
                                   cudaStream_t s);
 
-// The same FP32 product computing p.Ap and alpha (x = p); the mixed
-// solver's reliable update on this layout.
-cudaError_t launch_q16_spmv32_dot(const Q16View &Q, int unroll, const float *x, float *y, double *partials,
-                                  PcgState *st, cudaStream_t s);
-cudaError_t launch_q16_reliable(const Q16View &Q, const MixedBuffers &B, cudaStream_t s);
-
-// One mixed-precision PCG iteration on the q16 layout: the same recurrence as
-// launch_mixed_iteration2 (dir, FP32 product with p.Ap, update, reliable
-// update in FP64).
-cudaError_t launch_mixed_iteration_q16(const MixedBuffers &B, const Q16View &Q, int unroll, cudaStream_t s);
-
 }  // namespace phgb

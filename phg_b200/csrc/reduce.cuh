@@ -103,6 +103,79 @@ __device__ __forceinline__ bool grid_sum2(double &a, double &b, double *partials
     return lane == 0;
 }
 
+// The same for three sums, with the same stages and ordering.  Workspace:
+// 3 * (gridDim.x + ceil(gridDim.x / kRedGroup)) doubles in `partials`.
+struct RedShared3 {
+    double v[3][32];
+    unsigned cnt;
+};
+
+__device__ __forceinline__ RedShared3 &red_smem3() {
+    __shared__ RedShared3 r;
+    return r;
+}
+
+__device__ __forceinline__ void grid_sum3_init() {
+    if (threadIdx.x == 0) red_smem3().cnt = 0u;
+    __syncthreads();
+}
+
+__device__ __forceinline__ bool grid_sum3(double (&v)[3], double *partials, unsigned *tickets) {
+    RedShared3 &R = red_smem3();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 3; k++) v[k] = warp_sum(v[k]);
+    unsigned arrived = 0;
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) R.v[k][w] = v[k];
+        __threadfence_block();
+        arrived = atomicAdd(&R.cnt, 1u);
+    }
+    arrived = __shfl_sync(0xffffffffu, arrived, 0);
+    if (arrived != (unsigned)nw - 1) return false;
+    __threadfence_block();
+    double t[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) t[k] = warp_sum(lane < nw ? ((volatile double *)R.v[k])[lane] : 0.0);
+    // stage 1: block sums -> group sums
+    const unsigned nb = gridDim.x, g = blockIdx.x / kRedGroup, g0 = g * kRedGroup;
+    const unsigned gs = min((unsigned)kRedGroup, nb - g0), ng = (nb + kRedGroup - 1) / kRedGroup;
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) partials[3 * (size_t)blockIdx.x + k] = t[k];
+        arrived = ticket_add_acq_rel(&tickets[1 + g]);
+    }
+    arrived = __shfl_sync(0xffffffffu, arrived, 0);
+    if (arrived != gs - 1) return false;
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const double a = lane < gs ? __ldcg(&partials[3 * (size_t)(g0 + lane) + k]) : 0.0;
+        const double b = lane + 32 < gs ? __ldcg(&partials[3 * (size_t)(g0 + lane + 32) + k]) : 0.0;
+        t[k] = warp_sum(a + b);
+    }
+    if (lane == 0) {
+        tickets[1 + g] = 0u;
+#pragma unroll
+        for (int k = 0; k < 3; k++) partials[3 * (size_t)(nb + g) + k] = t[k];
+        arrived = ticket_add_acq_rel(&tickets[0]);
+    }
+    arrived = __shfl_sync(0xffffffffu, arrived, 0);
+    if (arrived != ng - 1) return false;
+    // stage 2: group sums -> totals
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+        t[k] = warp_sum(lane < ng ? __ldcg(&partials[3 * (size_t)(nb + lane) + k]) : 0.0);
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) v[k] = t[k];
+        tickets[0] = 0u;
+    }
+    return lane == 0;
+}
+
 // Loads/stores of V consecutive elements (16 bytes) at an index that is a
 // multiple of V.
 template <typename T> struct Vec16;

@@ -425,165 +425,6 @@ cudaError_t launch_pcg_iteration_plan(const PcgBuffers &B, const SpmvPlan &P, cu
 }
 
 // ---------------------------------------------------------------------------
-// Mixed precision: FP32 PCG with reliable updates inside FP64 refinement.
-//
-// The Krylov vectors (r, p, Ap and the correction y) and the SpMV are FP32;
-// every dot product accumulates in FP64.  The FP64 solution x and the FP64
-// residual r_true = b - A x are brought up to date by a "reliable update"
-// whenever the iterated FP32 residual has dropped by `delta` since the last
-// update (and before the iteration may stop): x += y, r_true -= A y in FP64,
-// and the FP32 residual is replaced by the rounded r_true.  The search
-// direction is kept, so the iteration does not restart and converges like the
-// FP64 recurrence.  The stopping rule is the reference's, applied to the FP64
-// residual.  Kernels per iteration: dir32, SpMV32 (+ p.Ap), update32, and the
-// reliable update (returns at once unless flagged).
-
-__global__ void __launch_bounds__(kVecThreads)
-mixed_update_kernel(int64_t n, float *__restrict__ y, float *__restrict__ r, const float *__restrict__ p,
-                    const float *__restrict__ Ap, const float *__restrict__ D, double *partials, MixedState *ms) {
-    PcgState *st = &ms->pcg;
-    if (st->done) return;
-    grid_sum_init();
-    const float a = (float)st->alpha;
-    const bool reset = ms->y_reset != 0;
-    double rr = 0.0, rz = 0.0;
-    constexpr int UN = 2;   // vectors per thread in flight
-    const int nfull = aligned16(y, r, p, Ap, D) ? (int)(n / 4) : 0;   // n < 2^31
-    const int stride = gridDim.x * blockDim.x;
-    for (int c0 = blockIdx.x * blockDim.x + threadIdx.x; c0 < nfull; c0 += UN * stride) {
-        VArr<float> pp[UN], aa[UN], dd[UN], yv[UN], rv[UN];
-#pragma unroll
-        for (int u = 0; u < UN; u++) {
-            const int c = c0 + u * stride;
-            if (c < nfull) {
-                const int i = c * 4;
-                pp[u] = vload_ro(p + i);
-                aa[u] = vload_ro(Ap + i);
-                dd[u] = vload_ro(D + i);
-                yv[u] = reset ? VArr<float>{{0.0f, 0.0f, 0.0f, 0.0f}} : vload(y + i);
-                rv[u] = vload(r + i);
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < UN; u++) {
-            const int c = c0 + u * stride;
-            if (c < nfull) {
-#pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    yv[u].v[q] = yv[u].v[q] + a * pp[u].v[q];
-                    const float ri = rv[u].v[q] - a * aa[u].v[q];
-                    rv[u].v[q] = ri;
-                    rr += (double)ri * (double)ri;
-                    rz += (double)ri * (double)(ri / dd[u].v[q]);
-                }
-                vstore(y + c * 4, yv[u]);
-                vstore(r + c * 4, rv[u]);
-            }
-        }
-    }
-    for (int64_t i = nfull * 4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        y[i] = (reset ? 0.0f : y[i]) + a * p[i];
-        const float ri = r[i] - a * Ap[i];
-        r[i] = ri;
-        rr += (double)ri * (double)ri;
-        rz += (double)ri * (double)(ri / D[i]);
-    }
-    if (grid_sum2(rr, rz, partials, st->ticket)) {
-        const int k = st->nits + 1;
-        const double res = sqrt(rr);
-        st->nits = k;
-        st->residual = res;
-        st->rz_prev = st->rz_cur;
-        st->rz_cur = rz;
-        ms->y_reset = 0;
-        if (!isfinite(res)) {
-            st->done = 1;
-            st->status = PCG_NONFINITE;
-        } else if (!(res > st->tol) || k >= st->maxit) {
-            ms->ru_flag = 1;
-            ms->final_check = 1;
-        } else if (res < ms->delta * ms->maxr) {
-            ms->ru_flag = 1;
-        }
-    }
-}
-
-// Reliable update on the SELL layout (FP64 values): x += y, r_true -= A y,
-// r32 = (float) r_true, ||r_true||^2 and r32.(r32/D).
-template <int U>
-__global__ void __launch_bounds__(kVecThreads, kResidentBlocks)
-mixed_reliable_kernel(int64_t nslices, const int32_t *__restrict__ perm, const uint16_t *__restrict__ len,
-                      const int32_t *__restrict__ sptr, const int32_t *__restrict__ cols,
-                      const double *__restrict__ vals, double *__restrict__ x, const float *__restrict__ y,
-                      double *__restrict__ rtrue, float *__restrict__ r32, const float *__restrict__ D,
-                      double *partials, MixedState *ms, double *hist) {
-    PcgState *st = &ms->pcg;
-    if (st->done || !ms->ru_flag) return;
-    grid_sum_init();
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = ((int64_t)blockIdx.x * kVecThreads + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * kVecThreads) >> 5;
-    double rr = 0.0, rz = 0.0;
-    for (int64_t s = warp; s < nslices; s += nwarps) {
-        const int64_t pos = s * 32 + lane;
-        const int32_t row = perm[pos];
-        const int l = len[pos];
-        const int w = __shfl_sync(0xffffffffu, l, 0);
-        const int64_t b = (int64_t)sptr[s] + lane;
-        double acc = 0.0;
-        for (int j = 0; j < w; j += U) {
-            int32_t c[U];
-            double v[U];
-#pragma unroll
-            for (int u = 0; u < U; u++) {
-                const bool ok = j + u < l;
-                c[u] = ok ? __ldcs(&cols[b + 32 * (j + u)]) : 0;
-                v[u] = ok ? __ldcs(&vals[b + 32 * (j + u)]) : 0.0;
-            }
-#pragma unroll
-            for (int u = 0; u < U; u++)
-                if (j + u < l) acc += v[u] * (double)__ldg(&y[c[u]]);
-        }
-        if (row >= 0) {
-            x[row] += (double)y[row];
-            const double rt = rtrue[row] - acc;
-            rtrue[row] = rt;
-            const float rf = (float)rt;
-            r32[row] = rf;
-            rr += rt * rt;
-            rz += (double)rf * (double)(rf / D[row]);
-        }
-    }
-    if (grid_sum2(rr, rz, partials, st->ticket)) mixed_reliable_final(rr, rz, ms, hist);
-}
-
-// r32 = (float) rtrue, y = 0, and (||rtrue||^2, r32.(r32/D)).
-__global__ void __launch_bounds__(kVecThreads)
-mixed_init_kernel(int64_t n, const double *__restrict__ rtrue, float *__restrict__ r32, float *__restrict__ y,
-                  const double *__restrict__ D64, float *__restrict__ D32, double *partials, unsigned *ticket,
-                  double *out) {
-    grid_sum_init();
-    double rr = 0.0, rz = 0.0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const double rt = rtrue[i];
-        const float rf = (float)rt, df = (float)D64[i];
-        r32[i] = rf;
-        y[i] = 0.0f;
-        D32[i] = df;
-        rr += rt * rt;
-        rz += (double)rf * (double)(rf / df);
-    }
-    if (grid_sum2(rr, rz, partials, ticket)) { out[0] = rr; out[1] = rz; }
-}
-
-cudaError_t launch_mixed_init(int64_t n, const double *rtrue, float *r32, float *y, const double *D64, float *D32,
-                              double *partials, unsigned *ticket, double *out, cudaStream_t s) {
-    mixed_init_kernel<<<vec_blocks(n), kVecThreads, 0, s>>>(n, rtrue, r32, y, D64, D32, partials, ticket, out);
-    return cudaGetLastError();
-}
-
-// ---------------------------------------------------------------------------
 // FP32 values in "pair" SELL: the same slices as SELL-C-sigma, but each lane
 // keeps two consecutive entries of its row side by side, so a warp moves
 // 256 bytes of values and 256 bytes of column indices per load instruction
@@ -719,31 +560,6 @@ cudaError_t launch_spmv32k(const SellView &S, const Sell2View &S2, int kind, int
                            cudaStream_t s) {
     spmv32_dispatch<false>(S, S2, kind, u, x, y, nullptr, nullptr, s);
     return cudaGetLastError();
-}
-
-cudaError_t launch_mixed_iteration2(const MixedBuffers &B, const SellView &S, const Sell2View &S2, int kind, int u,
-                                    cudaStream_t s) {
-    const int vb = vvec_blocks(B.n, 4);
-    PcgState *st = &B.ms->pcg;
-    pcg_dir_kernel<float><<<vb, kVecThreads, 0, s>>>(B.n, B.r32, B.D32, B.p32, st);
-    spmv32_dispatch<true>(S, S2, kind, u, B.p32, B.Ap32, B.partials, st, s);
-    mixed_update_kernel<<<vb, kVecThreads, 0, s>>>(B.n, B.y32, B.r32, B.p32, B.Ap32, B.D32, B.partials, B.ms);
-    const int sb = vec_blocks(S.nslices * 32);
-    mixed_reliable_kernel<4><<<sb, kVecThreads, 0, s>>>(S.nslices, S.perm, S.len, S.sptr, S.cols, S.vals, B.x, B.y32,
-                                                         B.rtrue, B.r32, B.D32, B.partials, B.ms, B.hist);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_mixed_iteration_q16(const MixedBuffers &B, const Q16View &Q, int unroll, cudaStream_t s) {
-    const int vb = vvec_blocks(B.n, 4);
-    PcgState *st = &B.ms->pcg;
-    pcg_dir_kernel<float><<<vb, kVecThreads, 0, s>>>(B.n, B.r32, B.D32, B.p32, st);
-    cudaError_t e = launch_q16_spmv32_dot(Q, unroll, B.p32, B.Ap32, B.partials, st, s);
-    if (e != cudaSuccess) return e;
-    mixed_update_kernel<<<vb, kVecThreads, 0, s>>>(B.n, B.y32, B.r32, B.p32, B.Ap32, B.D32, B.partials, B.ms);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    return launch_q16_reliable(Q, B, s);
 }
 
 }  // namespace phgb

@@ -104,26 +104,7 @@ struct SpmvPlan {
     Q16View q16{};
 };
 
-// State of the mixed-precision PCG (FP32 Krylov vectors, FP64 x and
-// residual); `pcg` comes first so the FP32 SpMV kernel can update it.
-struct MixedState {
-    PcgState pcg;
-    double maxr, delta;
-    int ru_flag, final_check, y_reset, nupdates;
-};
-
-struct MixedBuffers {
-    int64_t n;
-    double *x, *rtrue;
-    float *r32, *p32, *Ap32, *y32, *D32;
-    double *partials;
-    MixedState *ms;
-    double *hist;
-};
-
 int vec_blocks(int64_t n);
-cudaError_t launch_mixed_init(int64_t n, const double *rtrue, float *r32, float *y, const double *D64, float *D32,
-                              double *partials, unsigned *ticket, double *out, cudaStream_t s);
 cudaError_t launch_sell2_heads(const SellView &S, uint16_t *width, cudaStream_t s);
 cudaError_t launch_sell2_sizes(const SellView &S, const int32_t *order, int32_t *sizes, cudaStream_t s);
 cudaError_t launch_sell2_fill(const SellView &S, const int32_t *rp, const int32_t *ci, const double *va,
@@ -131,8 +112,6 @@ cudaError_t launch_sell2_fill(const SellView &S, const int32_t *rp, const int32_
                               int32_t *cols2, float *vals2, cudaStream_t s);
 cudaError_t launch_spmv32k(const SellView &S, const Sell2View &S2, int kind, int u, const float *x, float *y,
                            cudaStream_t s);
-cudaError_t launch_mixed_iteration2(const MixedBuffers &B, const SellView &S, const Sell2View &S2, int kind, int u,
-                                    cudaStream_t s);
 int64_t sell_positions(int64_t n);   // perm/len entries = slices * 32
 cudaError_t launch_sell_sort(int64_t n, const int32_t *rp, int32_t *perm, uint16_t *len, int32_t *slice_size,
                              cudaStream_t s);
