@@ -36,6 +36,8 @@ static INT rhs_case = 0;		/* 0: sine (g = 0), 1: linear u=x+y+z */
 static INT repeat = 1;			/* repeat the whole pipeline (timing) */
 static INT sample_maxit = 0;		/* > 0: cap PCG iterations after rep 0 */
 static FLOAT mass_coef = 0.;		/* != 0: add mass_coef * mass matrix */
+static INT refine = 0;			/* uniform bisection levels after import */
+static INT refine_corner = 0;		/* local refinement rounds at (0,0,0) */
 static const char *rhs_case_names[] = {"sine", "linear", NULL};
 
 #if PHG_GPU_PLUGIN
@@ -143,6 +145,11 @@ main(int argc, char *argv[])
     phgOptionsRegisterFloat("-mass_coef",
 		"Coefficient c of the mass term (-div kappa grad u + c u = f)",
 		&mass_coef);
+    phgOptionsRegisterInt("-refine", "Uniform refinement levels (phgRefineAllElements)",
+		&refine);
+    phgOptionsRegisterInt("-refine_corner",
+		"Rounds of local refinement of the elements near (0,0,0)",
+		&refine_corner);
     phgOptionsRegisterInt("-sample_maxit",
 		"PCG iteration cap for repetitions after the first (timing samples)",
 		&sample_maxit);
@@ -160,6 +167,24 @@ main(int argc, char *argv[])
     g = phgNewGrid(-1);
     if (!phgImport(g, mesh_file, FALSE))
 	phgError(1, "can't read file \"%s\".\n", mesh_file);
+    /* meshes PHG refines itself: uniform bisection, then local bisection of
+     * the elements whose centroid lies within 0.25 of the corner (0,0,0)
+     * (the marking pattern of examples/eigen.c:398-411) */
+    if (refine > 0)
+	phgRefineAllElements(g, refine);
+    for (i = 0; i < refine_corner; i++) {
+	ForAllElements(g, e) {
+	    FLOAT c[3] = {0., 0., 0.};
+	    int k;
+	    for (k = 0; k < NVert; k++) {
+		c[0] += g->verts[e->verts[k]][0] * 0.25;
+		c[1] += g->verts[e->verts[k]][1] * 0.25;
+		c[2] += g->verts[e->verts[k]][2] * 0.25;
+	    }
+	    e->mark = (c[0] * c[0] + c[1] * c[1] + c[2] * c[2] < 0.0625) ? 1 : 0;
+	}
+	phgRefineMarkedElements(g);
+    }
 
     u_h = phgDofNew(g, DOF_DEFAULT, 1, "u_h", DofNoAction);
     phgDofSetDataByValue(u_h, 0.0);

@@ -399,6 +399,20 @@ struct WalkCfg {
     static constexpr int HS = N == 4 ? 128 : N == 10 ? 256 : 512;
     static constexpr int MAXROW = HS / 2;
     static constexpr int WARPS = 4;
+    static constexpr bool LONG = false;   // overflowing rows go to the list
+};
+
+// The second pass over the rows the first one could not hold (high-valence
+// vertices of locally refined meshes): a warp per row, a table of 2048 slots
+// for up to 1024 entries.
+template <int N>
+struct LongWalkCfg {
+    static constexpr int G = 32;
+    static constexpr int R = 1;
+    static constexpr int HS = 2048;
+    static constexpr int MAXROW = 1024;
+    static constexpr int WARPS = 1;
+    static constexpr bool LONG = true;    // an overflowing row is an error
 };
 
 __device__ __forceinline__ unsigned hash32(int32_t c) { return (unsigned)c * 2654435761u; }
@@ -413,15 +427,15 @@ __device__ __forceinline__ double bdry_rhs(const double *g, int32_t k, int mult)
     return s;
 }
 
-template <int N>
-__global__ void __launch_bounds__(WalkCfg<N>::WARPS * 32, 8)
+template <int N, class C>
+__global__ void __launch_bounds__(C::WARPS * 32, C::LONG ? 1 : 8)
 row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t *__restrict__ inc,
                 const int32_t *__restrict__ e2l, const uint8_t *__restrict__ bdry,
                 const double *__restrict__ Ke, const double *__restrict__ Re, const double *__restrict__ g,
                 int32_t *__restrict__ cnt_keep, int32_t *__restrict__ cnt_bdry,
                 int32_t *__restrict__ sc_cols, double *__restrict__ sc_vals,
-                double *__restrict__ rhs, double *__restrict__ diag, int *status) {
-    using C = WalkCfg<N>;
+                double *__restrict__ rhs, double *__restrict__ diag, int *status,
+                int32_t *__restrict__ over_list, int *nover) {
     constexpr int G = C::G, R = C::R, HS = C::HS, MAXROW = C::MAXROW, W = C::WARPS;
     __shared__ int32_t s_key[W][R][HS];
     __shared__ int16_t s_pos[W][R][HS];
@@ -438,8 +452,10 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
     double *sval = s_val[w][grp];
 
     const int64_t nwarps = (int64_t)gridDim.x * W;
-    for (int64_t wb = ((int64_t)blockIdx.x * W + w) * R; wb < ndof; wb += nwarps * R) {
-        const int64_t d = wb + grp;
+    // the first pass walks every row, the second the listed ones
+    const int64_t nrows = C::LONG ? (int64_t)*nover : ndof;
+    for (int64_t wb = ((int64_t)blockIdx.x * W + w) * R; wb < nrows; wb += nwarps * R) {
+        const int64_t d = C::LONG ? (wb + grp < nrows ? (int64_t)over_list[wb + grp] : ndof) : wb + grp;
         const bool active = d < ndof;
         int32_t i0 = 0, i1 = 0;
         bool isb = false;
@@ -547,7 +563,10 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
         }
         const bool bad = overflow || L > MAXROW;
         const unsigned badm = __ballot_sync(0xffffffffu, bad) & gmask;
-        if (badm != 0 && gl == 0) atomicExch(status, PHGB_DEV_ROW_OVERFLOW);
+        if (badm != 0 && gl == 0) {
+            if (C::LONG) atomicExch(status, PHGB_DEV_ROW_OVERFLOW);
+            else over_list[atomicAdd(nover, 1)] = (int32_t)d;   // assembled by the second pass
+        }
 
         // emit kept columns (front) and saved boundary columns (back, reversed),
         // in first-touch order.  Lanes also evaluate, in parallel, the lift
@@ -713,9 +732,16 @@ template <int N>
 static cudaError_t walk(const WalkArgs &A, cudaStream_t s) {
     constexpr int W = WalkCfg<N>::WARPS, R = WalkCfg<N>::R;
     const int blocks = grid_for(ceil_div(A.ndof, R), W, 148 * 32);
-    row_walk_kernel<N><<<blocks, W * 32, 0, s>>>(A.ndof, A.inc_ptr, A.inc, A.e2l, A.bdry, A.Ke, A.Re, A.g,
-                                                 A.cnt_keep, A.cnt_bdry, A.sc_cols, A.sc_vals, A.rhs, A.diag,
-                                                 A.status);
+    cudaError_t e = cudaMemsetAsync(A.nover, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    row_walk_kernel<N, WalkCfg<N>><<<blocks, W * 32, 0, s>>>(
+        A.ndof, A.inc_ptr, A.inc, A.e2l, A.bdry, A.Ke, A.Re, A.g, A.cnt_keep, A.cnt_bdry, A.sc_cols, A.sc_vals,
+        A.rhs, A.diag, A.status, A.over_list, A.nover);
+    // the rows the first pass listed (none in most meshes: the blocks return
+    // after reading the count)
+    row_walk_kernel<N, LongWalkCfg<N>><<<148 * 4, 32, 0, s>>>(
+        A.ndof, A.inc_ptr, A.inc, A.e2l, A.bdry, A.Ke, A.Re, A.g, A.cnt_keep, A.cnt_bdry, A.sc_cols, A.sc_vals,
+        A.rhs, A.diag, A.status, A.over_list, A.nover);
     return cudaGetLastError();
 }
 
@@ -732,6 +758,8 @@ cudaError_t launch_compact(int N, const WalkArgs &A, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-int row_walk_max_row(int p) { return p == 1 ? WalkCfg<4>::MAXROW : p == 2 ? WalkCfg<10>::MAXROW : WalkCfg<20>::MAXROW; }
+int row_walk_max_row(int p) {
+    return p == 1 ? LongWalkCfg<4>::MAXROW : p == 2 ? LongWalkCfg<10>::MAXROW : LongWalkCfg<20>::MAXROW;
+}
 
 }  // namespace phgb

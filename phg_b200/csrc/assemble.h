@@ -38,6 +38,11 @@ struct WalkArgs {
     int32_t *cols, *bcols;
     double *vals, *bvals, *rhs, *diag;
     int *status;
+    // rows longer than the walk's shared-memory table: listed by the walk and
+    // assembled by a second pass with a larger table (over_list: ndof
+    // entries; *nover zeroed before the walk)
+    int32_t *over_list;
+    int *nover;
 };
 
 cudaError_t launch_element_kernel(int p, const ElemArgs &a, cudaStream_t s);
@@ -51,6 +56,8 @@ cudaError_t launch_scan(int64_t n, const int32_t *in, int32_t *out, int64_t *ws,
 // then, after the counts are scanned into ptr/bptr, the copy into the CSR.
 cudaError_t launch_row_walk(int p, const WalkArgs &a, cudaStream_t s);
 cudaError_t launch_compact(int N, const WalkArgs &a, cudaStream_t s);
+// Longest row the walk assembles (its second pass); longer rows are
+// PHG_GPU_ERR_LIMIT.
 int row_walk_max_row(int p);
 int64_t geometry_doubles(int64_t nelem);
 

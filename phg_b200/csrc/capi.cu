@@ -176,6 +176,8 @@ struct phgGpuSystem_ {
     DevBuf<int32_t> sc_cols;          // row-walk scratch (nelem * N * N entries)
     DevBuf<double> sc_vals;
     DevBuf<int32_t> cnt_keep, cnt_bdry;
+    DevBuf<int32_t> over_list;        // rows the row walk's second pass assembles
+    DevBuf<int> nover;
 
     // assembled system
     int64_t n = 0, nnz = 0, bnnz = 0;
@@ -911,8 +913,11 @@ static int build_system(phgGpuSystem *s, const double *kappa, double mass, const
     wa.cnt_keep = s->cnt_keep.p; wa.cnt_bdry = s->cnt_bdry.p; wa.status = s->status.p;
     wa.sc_cols = s->sc_cols.p; wa.sc_vals = s->sc_vals.p;
     wa.rhs = s->rhs.p; wa.diag = s->diag.p;
+    CHECK_RC(s->over_list.ensure((size_t)ndof));
+    CHECK_RC(s->nover.ensure(1));
+    wa.over_list = s->over_list.p; wa.nover = s->nover.p;
     CK(launch_row_walk(s->order, wa, s->stream));
-    s->launches += 7;   // walk + two scans
+    s->launches += 8;   // walk (two passes) + two scans
     CK(launch_scan(ndof, s->cnt_keep.p, s->rp.p, s->scan_ws.p, s->stream));
     int32_t tot[2];
     CK(cudaMemcpyAsync(&tot[0], s->rp.p + ndof, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
@@ -1392,6 +1397,7 @@ int pcg_core(phgGpuSystem *s, const double *drhs, double rtol, double btol, doub
     init.tol = tol;
     init.maxit = maxit;
     init.done = !(r0 > tol && 0 < maxit);
+    init.max_passes = maxit / kGraphChunk + 3;
     *s->h_st = init;
     CK(cudaMemcpyAsync(s->st.p, s->h_st, sizeof(PcgState), cudaMemcpyHostToDevice, s->stream));
     if (dhist) CK(cudaMemcpyAsync(dhist, &s->h_st->residual, sizeof(double), cudaMemcpyHostToDevice, s->stream));
@@ -1403,23 +1409,23 @@ int pcg_core(phgGpuSystem *s, const double *drhs, double rtol, double btol, doub
     plan_key(s, key);
     if (s->graph == nullptr || !(s->gkey == key)) {
         if (s->graph != nullptr) { cudaGraphExecDestroy(s->graph); s->graph = nullptr; }
-        cudaGraph_t gr;
-        CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-        for (int i = 0; i < kGraphChunk; i++) launch_pcg_iteration_plan(B, s->plan, s->stream);
-        CK(cudaStreamEndCapture(s->stream, &gr));
-        cudaError_t e = cudaGraphInstantiate(&s->graph, gr, 0);
-        cudaGraphDestroy(gr);
-        CK(e);
+        // one graph launch per solve: chunks of iterations in a WHILE loop
+        struct Ctx { PcgBuffers B; SpmvPlan P; } ctx{B, s->plan};
+        auto body = [](void *c, cudaStream_t st) {
+            const Ctx *x = (const Ctx *)c;
+            for (int i = 0; i < kGraphChunk; i++) launch_pcg_iteration_plan(x->B, x->P, st);
+        };
+        CK(build_pcg_loop_graph(s->stream, body, &ctx, s->st.p, &s->graph));
         s->gkey = key;
     }
-    while (!s->h_st->done) {
-        CK(cudaGraphLaunch(s->graph, s->stream));
-        s->launches += 3 * kGraphChunk;
-        CK(cudaMemcpyAsync(s->h_st, s->st.p, sizeof(PcgState), cudaMemcpyDeviceToHost, s->stream));
-        CK(cudaStreamSynchronize(s->stream));
-    }
+    if (!init.done) CK(cudaGraphLaunch(s->graph, s->stream));
+    CK(cudaMemcpyAsync(s->h_st, s->st.p, sizeof(PcgState), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    s->launches += 3 * (int64_t)kGraphChunk * s->h_st->passes + s->h_st->passes;
     const int nits = s->h_st->nits;
     if (residual) *residual = s->h_st->residual;
+    if (s->h_st->status == kStatusPassLimit)
+        return fail(PHG_GPU_ERR_STATE, "PCG: the iteration loop exceeded its pass bound");
     if (s->h_st->status == PCG_BREAKDOWN)
         warn("PCG stopped after %d iterations: the matrix may not be SPD", nits);
     if (s->h_st->status == PCG_NONFINITE)

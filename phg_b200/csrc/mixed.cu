@@ -210,6 +210,16 @@ __global__ void gear_loop_kernel(GearState *st, cudaGraphConditionalHandle hwhil
     cudaGraphSetConditional(hwhile, st->done ? 0u : 1u);
 }
 
+// The same for the FP64 PCG's state.
+__global__ void pcg_loop_kernel(PcgState *st, cudaGraphConditionalHandle hwhile) {
+    st->passes += 1;
+    if (!st->done && st->passes > st->max_passes) {
+        st->done = 1;
+        st->status = kStatusPassLimit;
+    }
+    cudaGraphSetConditional(hwhile, st->done ? 0u : 1u);
+}
+
 __global__ void __launch_bounds__(kVecThreads)
 gear_init_kernel(const GearBuffers B, const double *__restrict__ D64, unsigned *ticket, double *out) {
     grid_sum_init();
@@ -377,6 +387,26 @@ cudaError_t build_gear_graph(const GearBuffers &B, const GearLayouts &L, int chu
     if (e == cudaSuccess) e = cudaGraphInstantiate(exec, g, 0);
     cudaGraphDestroy(g);
     if (kernels_per_iteration != nullptr) *kernels_per_iteration = 2;
+    return e;
+}
+
+cudaError_t build_pcg_loop_graph(cudaStream_t stream, void (*body)(void *ctx, cudaStream_t s), void *ctx,
+                                 PcgState *st, cudaGraphExec_t *exec) {
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaGraphCreate(&g, 0);
+    if (e != cudaSuccess) return e;
+    cudaGraphConditionalHandle hw;
+    cudaGraphNode_t wnode, last;
+    cudaGraph_t wbody = nullptr;
+    e = cudaGraphConditionalHandleCreate(&hw, g, 1, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) e = add_conditional(g, nullptr, hw, cudaGraphCondTypeWhile, &wnode, &wbody);
+    if (e == cudaSuccess)
+        e = capture_into(stream, wbody, nullptr, [&] {
+            body(ctx, stream);
+            pcg_loop_kernel<<<1, 1, 0, stream>>>(st, hw);
+        }, &last);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
     return e;
 }
 

@@ -15,7 +15,7 @@ struct GearState {
     unsigned ticket[kRedTickets];
 };
 
-enum { GEAR_PASS_LIMIT = 3 };       // status: the graph loop ran out of passes
+enum { GEAR_PASS_LIMIT = kStatusPassLimit };   // status: the graph loop ran out of passes
 
 // Working vectors: x and rtrue FP64; r, u = r / D, w = A u, p, s = A p and
 // the correction y FP32.
@@ -54,5 +54,11 @@ cudaError_t build_gear_graph(const GearBuffers &B, const GearLayouts &L, int chu
                              cudaGraphExec_t *exec, int *kernels_per_iteration);
 // x += y unless the correction was already folded in.
 cudaError_t launch_gear_fold(const GearBuffers &B, cudaStream_t s);
+
+// A graph that repeats `body` (launches on `stream`, captured) in a
+// conditional WHILE loop until st->done, at most st->max_passes passes (then
+// st->status = kStatusPassLimit): one graph launch runs a whole solve.
+cudaError_t build_pcg_loop_graph(cudaStream_t stream, void (*body)(void *ctx, cudaStream_t s), void *ctx,
+                                 PcgState *st, cudaGraphExec_t *exec);
 
 }  // namespace phgb

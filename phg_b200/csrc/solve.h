@@ -33,8 +33,11 @@ struct PcgState {
     double rz_cur, rz_prev, pAp, alpha, residual, tol;
     int nits, done, status, maxit;
     unsigned ticket[kRedTickets];
-    int pad;
+    int passes, max_passes;   // passes of a graph loop, and their bound
 };
+
+// Status of a solve whose graph loop ran out of passes (a safeguard).
+constexpr int kStatusPassLimit = 3;
 
 struct CsrView {
     int64_t n;

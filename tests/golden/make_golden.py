@@ -49,15 +49,43 @@ CASES = {
     "p1_m6_gmres": (6, 1, "sine", None, 1e-10, 0.0, "gmres_r"),
     "p2_m5_kappa_gmres": (5, 2, "sine", 12, 1e-10, 0.0, "gmres_r"),
     "p3_m3_mass_gmres": (3, 3, "linear", None, 1e-12, 25.0, "gmres_r"),
+    # meshes PHG refined itself (the element and DOF numbering are PHG's):
+    # the reference's test/cube.dat bisected uniformly, and a Kuhn cube
+    # refined locally around the corner (0,0,0)
+    "p2_cubedat_refined": (1, 2, "sine", None, 1e-10, 0.0, "pcg", dict(mesh="cube.dat", refine=9)),
+    "p1_corner_refined": (2, 1, "linear", None, 1e-10, 0.0, "pcg", dict(refine=3, refine_corner=8)),
+    "p2_corner_refined": (2, 2, "sine", None, 1e-10, 0.0, "pcg", dict(refine=3, refine_corner=9)),
+    "p3_corner_refined": (2, 3, "linear", None, 1e-10, 0.0, "pcg", dict(refine=2, refine_corner=5)),
 }
 GMRES_RESTART = 10   # the reference's default (-gmres_restart)
 
 
-def run_case(name, m, P, case, kseed, rtol, mass=0.0, solver="pcg"):
-    with tempfile.TemporaryDirectory() as d:
+def mesh_args(name, d):
+    """Writes the case's input mesh into directory d and returns the driver
+    arguments that read (and, for the refined cases, refine) it."""
+    m = CASES[name][0]
+    opts = CASES[name][7] if len(CASES[name]) > 7 else {}
+    path = os.path.join(d, "m.mesh")
+    if opts.get("mesh") == "cube.dat":
+        path = os.path.join(d, "cube.dat")   # ALBERT format, recognised by its name
+        ref = os.environ.get("PHG_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference")
+        with open(os.path.join(ref, "test", "cube.dat")) as src, open(path, "w") as dst:
+            dst.write(src.read())
+    else:
         v, e = kuhn_cube(m)
-        write_medit(os.path.join(d, "m.mesh"), v, e)
-        args = [DUMP, "-mesh_file", os.path.join(d, "m.mesh"), "-dof_type", "P%d" % P,
+        write_medit(path, v, e)
+    args = ["-mesh_file", path]
+    if opts.get("refine"):
+        args += ["-refine", str(opts["refine"])]
+    if opts.get("refine_corner"):
+        args += ["-refine_corner", str(opts["refine_corner"])]
+    return args
+
+
+def run_case(name, m, P, case, kseed, rtol, mass=0.0, solver="pcg", opts=None):
+    with tempfile.TemporaryDirectory() as d:
+        e = kuhn_cube(m)[1]
+        args = [DUMP, *mesh_args(name, d), "-dof_type", "P%d" % P,
                 "-solver", "gmres" if solver == "gmres_r" else solver, "-pcg_pc_type", "jacobi", "-solver_rtol", repr(rtol),
                 "-solver_btol", "0", "-solver_atol", "0", "-solver_maxit", "10000",
                 "-map_reorder", "no", "-dump_dir", d, "-rhs_case", case]
