@@ -185,6 +185,18 @@ int phgGpuSolverGMRES(phgGpuSystem *sys, int restart, double rtol,
 		      double btol, double atol, int maxit, double *x,
 		      double *residual);
 
+/* PHG's default GMRES: the flexible, augmented FLGMRES_r
+ * (solver_FLGMRES_r, src/solver-phg.c:2063-2340; what phgSolverSolve runs
+ * with -solver gmres and the default -gmres_type flgmres_r), Jacobi
+ * preconditioner, FP64.  Cycle k takes restart + min(k, augk) steps, the
+ * steps past `restart` preconditioning the corrections of the last augk
+ * cycles (augk <= 0: 2, the reference's -lgmres_augk default); restart +
+ * augk <= 64.  Stopping rule, *residual and return value as
+ * phgGpuSolverGMRES. */
+int phgGpuSolverFLGMRES(phgGpuSystem *sys, int restart, int augk, double rtol,
+			double btol, double atol, int maxit, double *x,
+			double *residual);
+
 /* Jacobi-PCG for many right-hand sides at once: column k of B (n x nrhs,
  * row major: B[i * nrhs + k]) is solved by its own PCG recurrence and
  * stopping rule (rtol relative to ||b_k||, from x = 0), and the columns share

@@ -993,3 +993,160 @@ pho_gmres(int64_t n, const int64_t *ptr, const int32_t *cols,
 	*res = residual;
     return nits;
 }
+
+int
+pho_flgmres(int64_t n, const int64_t *ptr, const int32_t *cols,
+	    const double *vals, const double *diag, const double *b, double *x,
+	    int restart, int augk, int maxit, double rtol, double btol,
+	    double atol, double *res)
+/* solver_FLGMRES_r (solver-phg.c:2063-2340), PHG's default GMRES: flexible
+ * right-preconditioned GMRES whose basis is augmented with the corrections z
+ * of the last augk cycles (preconditioned like the basis vectors).  Cycle k
+ * (k = 0, 1, ...) runs up to mk + min(k, augk) steps, mk the restart; steps
+ * past mk precondition the stored corrections.  x += sum_j y_j M^-1 v_j with
+ * the preconditioned vectors kept (flv); the stored correction is sum_j y_j
+ * v_j over the unpreconditioned vectors (and the augmenting corrections).
+ * When a cycle ends without a step (happy breakdown at its first step) the
+ * reference adds the cycle's starting residual z to x, and so does this. */
+{
+    int R, mk, nits = 0, i, j, k, itr_out = 0, zi;
+    double b_norm, r0_norm, r_norm, residual, tol, tmp, h1, h2, x1 = 0.0;
+    double **V, **Z, **F, *H, *y, *s, *c1, *c2, *z, *r;
+    int64_t l;
+
+    if (restart <= 0)
+	restart = maxit + 1;
+    if (augk <= 0)
+	augk = 2;
+    b_norm = norm2(n, b);
+    if (IS_ZERO(b_norm)) {
+	memset(x, 0, n * sizeof(double));
+	if (res != NULL)
+	    *res = 0.0;
+	return 0;
+    }
+    mk = restart;
+    restart += augk;
+    R = restart + 2;
+    V = malloc(R * sizeof(*V));
+    F = malloc(R * sizeof(*F));
+    for (i = 0; i < R; i++) {
+	V[i] = malloc(n * sizeof(double));
+	F[i] = malloc(n * sizeof(double));
+    }
+    Z = malloc(augk * sizeof(*Z));
+    for (i = 0; i < augk; i++)
+	Z[i] = calloc(n, sizeof(double));
+    H = malloc((size_t)R * R * sizeof(double));
+    y = malloc(4 * R * sizeof(double));
+    s = y + R;
+    c1 = y + 2 * R;
+    c2 = y + 3 * R;
+    z = malloc(n * sizeof(double));
+    r = V[0];
+#define Hij(a, b) H[(size_t)(a) * R + (b)]
+
+    for (l = 0; l < n; l++)
+	x1 += fabs(x[l]);
+    if (x1 != 0.)
+	residual_vec(n, ptr, cols, vals, b, x, z);
+    else
+	memcpy(z, b, n * sizeof(double));
+    r0_norm = r_norm = residual = norm2(n, z);
+    tol = r0_norm * rtol;
+    if (tol < b_norm * btol)
+	tol = b_norm * btol;
+    if (tol < atol)
+	tol = atol;
+
+    s[0] = 1.;
+    while (nits < maxit) {
+	restart = itr_out <= augk ? mk + itr_out : mk + augk;
+	s[1] = r_norm = norm2(n, z);
+	scale_add(n, 1.0 / r_norm, z, 0, V[1]);
+	i = 0;
+	memset(H, 0, (size_t)R * R * sizeof(double));
+	while (i < restart && r_norm > tol && nits < maxit) {
+	    double *v1;
+	    const double *src;
+	    i++, nits++;
+	    v1 = V[i + 1];
+	    src = i <= mk ? V[i] : Z[i - mk - 1];
+	    for (l = 0; l < n; l++)
+		r[l] = src[l] / diag[l];
+	    pho_spmv(n, ptr, cols, vals, r, v1);
+	    memcpy(F[i], r, n * sizeof(double));
+	    for (k = 1; k <= i; k++) {
+		Hij(i, k) = dot(n, v1, V[k]);
+		scale_add(n, -Hij(i, k), V[k], 1, v1);
+	    }
+	    Hij(i, i + 1) = norm2(n, v1);
+	    if (IS_ZERO(Hij(i, i + 1))) {
+		i--;
+		break;
+	    }
+	    tmp = 1.0 / Hij(i, i + 1);
+	    for (l = 0; l < n; l++)
+		v1[l] *= tmp;
+	    for (j = 1; j < i; j++) {
+		h1 = c1[j] * Hij(i, j) + c2[j] * Hij(i, j + 1);
+		h2 = -c2[j] * Hij(i, j) + c1[j] * Hij(i, j + 1);
+		Hij(i, j) = h1;
+		Hij(i, j + 1) = h2;
+	    }
+	    tmp = sqrt(Hij(i, i) * Hij(i, i) + Hij(i, i + 1) * Hij(i, i + 1));
+	    if (IS_ZERO(tmp))
+		tmp = 1.e-16;
+	    c1[i] = Hij(i, i) / tmp;
+	    c2[i] = Hij(i, i + 1) / tmp;
+	    s[i + 1] = -c2[i] * s[i];
+	    s[i] = c1[i] * s[i];
+	    Hij(i, i) = c1[i] * Hij(i, i) + c2[i] * Hij(i, i + 1);
+	    r_norm = fabs(s[i + 1]);
+	    if (r_norm <= tol)
+		break;
+	}
+	for (j = i; j > 0; j--) {
+	    y[j] = s[j] / Hij(j, j);
+	    for (k = j - 1; k > 0; k--)
+		s[k] -= Hij(j, k) * y[j];
+	}
+	if (i > 0) {
+	    scale_add(n, y[1], F[1], 0, z);
+	    for (j = 2; j <= i; j++)
+		scale_add(n, y[j], F[j], 1, z);
+	}
+	for (l = 0; l < n; l++)
+	    x[l] = z[l] + x[l];
+	if (i > 0) {
+	    int top = i <= mk ? i : mk;
+	    scale_add(n, y[1], V[1], 0, z);
+	    for (j = 2; j <= top; j++)
+		scale_add(n, y[j], V[j], 1, z);
+	    if (i > mk) {
+		int ak = itr_out < augk ? itr_out : augk;
+		for (j = 1; j <= ak; j++)
+		    scale_add(n, y[j + mk], Z[j - 1], 1, z);
+	    }
+	}
+	zi = itr_out % augk;
+	memcpy(Z[zi], z, n * sizeof(double));
+	if (r_norm <= tol) {
+	    residual = r_norm;
+	    break;
+	}
+	residual_vec(n, ptr, cols, vals, b, x, z);
+	itr_out++;
+    }
+#undef Hij
+    for (i = 0; i < R; i++) {
+	free(V[i]);
+	free(F[i]);
+    }
+    for (i = 0; i < augk; i++)
+	free(Z[i]);
+    free(V); free(F); free(Z); free(H); free(y); free(z);
+    if (res != NULL)
+	*res = residual;
+    return nits;
+}

@@ -114,6 +114,15 @@ int pho_gmres(int64_t n, const int64_t *ptr, const int32_t *cols,
 	      double *x, int restart, int maxit, double rtol, double btol,
 	      double atol, double *residual);
 
+/* PHG's default GMRES, flexible augmented FLGMRES_r (solver_FLGMRES_r,
+ * solver-phg.c:2063-2340; -solver gmres, -gmres_type flgmres_r the default):
+ * restart steps plus up to augk (<= 0: 2) steps on the corrections of the
+ * previous cycles, Jacobi PC.  *residual as pho_gmres. */
+int pho_flgmres(int64_t n, const int64_t *ptr, const int32_t *cols,
+		const double *vals, const double *diag, const double *b,
+		double *x, int restart, int augk, int maxit, double rtol,
+		double btol, double atol, double *residual);
+
 #ifdef __cplusplus
 }
 #endif

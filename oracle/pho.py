@@ -44,6 +44,9 @@ def lib():
         L.pho_gmres.argtypes = [C.c_int64, P, P, P, P, P, P, C.c_int, C.c_int,
                                 C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)]
         L.pho_gmres.restype = C.c_int
+        L.pho_flgmres.argtypes = [C.c_int64, P, P, P, P, P, P, C.c_int, C.c_int, C.c_int,
+                                  C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)]
+        L.pho_flgmres.restype = C.c_int
         _LIB = L
     return _LIB
 
@@ -186,4 +189,19 @@ def gmres(ptr, cols, vals, diag, b, x0=None, restart=10, maxit=10000, rtol=1e-10
                            _ptr(np.ascontiguousarray(diag, np.float64)),
                            _ptr(np.ascontiguousarray(b, np.float64)), _ptr(x),
                            restart, maxit, rtol, btol, atol, C.byref(res))
+    return x, nits, res.value
+
+
+def flgmres(ptr, cols, vals, diag, b, x0=None, restart=10, augk=2, maxit=10000, rtol=1e-10, btol=0.0,
+            atol=0.0):
+    """PHG's default GMRES (FLGMRES_r), Jacobi PC.  Returns (x, nits, residual)."""
+    n = len(ptr) - 1
+    x = np.zeros(n) if x0 is None else np.array(x0, np.float64)
+    res = C.c_double()
+    nits = lib().pho_flgmres(n, _ptr(np.ascontiguousarray(ptr, np.int64)),
+                             _ptr(np.ascontiguousarray(cols, np.int32)),
+                             _ptr(np.ascontiguousarray(vals, np.float64)),
+                             _ptr(np.ascontiguousarray(diag, np.float64)),
+                             _ptr(np.ascontiguousarray(b, np.float64)), _ptr(x),
+                             restart, augk, maxit, rtol, btol, atol, C.byref(res))
     return x, nits, res.value

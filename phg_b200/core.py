@@ -45,6 +45,8 @@ SIGNATURES = {
                                        C.POINTER(C.c_double), _P]),
     "phgGpuSolverGMRES": (C.c_int, [_P, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, _P,
                                     C.POINTER(C.c_double)]),
+    "phgGpuSolverFLGMRES": (C.c_int, [_P, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,
+                                      _P, C.POINTER(C.c_double)]),
     "phgGpuSetSpMVPlan32": (C.c_int, [_P, C.c_int, C.c_int]),
     "phgGpuElementMatrices": (C.c_int, [_P, _P, C.c_double, _P, _P, _P]),
     "phgGpuGetLaunchCount": (C.c_int, [_P, C.POINTER(_I64)]),
@@ -367,6 +369,21 @@ class Solver:
         res = C.c_double()
         nits = _check(lib().phgGpuSolverGMRES(self._h, int(restart), rtol, btol, atol, int(maxit), _ptr(x),
                                               C.byref(res)))
+        return x, nits, res.value
+
+    def solve_flgmres(self, x0=None, restart=10, augk=2, rtol=1e-10, btol=1e-10, atol=0.0, maxit=10000,
+                      out=None):
+        """phgSolverSolve with -solver gmres (PHG's default -gmres_type
+        flgmres_r) -gmres_pc_type jacobi -gmres_restart `restart`
+        -lgmres_augk `augk`.  Returns (x, nits, residual)."""
+        n = self.sizes()[0]
+        if out is not None:
+            x = out
+        else:
+            x = np.zeros(n) if x0 is None else np.array(x0, dtype=np.float64)
+        res = C.c_double()
+        nits = _check(lib().phgGpuSolverFLGMRES(self._h, int(restart), int(augk), rtol, btol, atol, int(maxit),
+                                                _ptr(x), C.byref(res)))
         return x, nits, res.value
 
 

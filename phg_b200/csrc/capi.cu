@@ -1561,14 +1561,18 @@ int phgGpuSolverPCG(phgGpuSystem *s, double rtol, double btol, double atol, int 
     return nits;
 }
 
-int phgGpuSolverGMRES(phgGpuSystem *s, int restart, double rtol, double btol, double atol, int maxit, double *x,
-                      double *residual) {
+// GMRES_r (augk < 0) or FLGMRES_r (augk >= 1 augmenting corrections).
+static int gmres_impl(phgGpuSystem *s, int restart, int augk, double rtol, double btol, double atol, int maxit,
+                      double *x, double *residual) {
     g_last_warning.clear();
     if (s == nullptr || x == nullptr) return fail(PHG_GPU_ERR_ARG, "invalid arguments");
     if (!s->assembled) return fail(PHG_GPU_ERR_STATE, "no assembled system");
     if (maxit < 0) return fail(PHG_GPU_ERR_ARG, "maxit < 0");
-    if (restart < 1 || restart > kGmresMaxRestart)
-        return fail(PHG_GPU_ERR_LIMIT, "phgGpuSolverGMRES: restart must be in 1..%d", kGmresMaxRestart);
+    const bool flex = augk >= 0;
+    const int mk = restart;
+    if (flex) restart = mk + augk;   // the most steps a cycle takes
+    if (mk < 1 || restart > kGmresMaxRestart)
+        return fail(PHG_GPU_ERR_LIMIT, "GMRES: restart (plus augk) must be in 1..%d", kGmresMaxRestart);
     CHECK_RC(set_device(s));
     CHECK_RC(solver_buffers(s));
     const int64_t n = s->n;
@@ -1589,7 +1593,9 @@ int phgGpuSolverGMRES(phgGpuSystem *s, int restart, double rtol, double btol, do
     }
     CHECK_RC(tune_spmv(s));
     const int64_t stride = bicg_stride(n);
-    CHECK_RC(s->gm_vecs.ensure((size_t)stride * (restart + 3)));
+    // z, V_0..V_(R+1); FLGMRES_r also F_0..F_R and Z_0..Z_(augk-1)
+    const int nvec = (restart + 3) + (flex ? (restart + 1) + augk : 0);
+    CHECK_RC(s->gm_vecs.ensure((size_t)stride * nvec));
     CHECK_RC(s->gm_small.ensure((size_t)gmres_small_doubles(restart)));
     CHECK_RC(s->gm_st.ensure(1));
     if (s->h_gst == nullptr) CK(cudaMallocHost((void **)&s->h_gst, sizeof(GmresState)));
@@ -1601,6 +1607,9 @@ int phgGpuSolverGMRES(phgGpuSystem *s, int restart, double rtol, double btol, do
     init.maxit = maxit;
     init.restart = restart;
     init.first = 1;
+    init.flexible = flex ? 1 : 0;
+    init.mk = mk;
+    init.augk = flex ? augk : 0;
     init.H = s->gm_small.p;
     init.c1 = init.H + (size_t)R2 * R2;
     init.c2 = init.c1 + R2;
@@ -1610,11 +1619,14 @@ int phgGpuSolverGMRES(phgGpuSystem *s, int restart, double rtol, double btol, do
     CK(cudaMemsetAsync(s->gm_small.p, 0, sizeof(double) * (size_t)gmres_small_doubles(restart), s->stream));
     CK(cudaMemcpyAsync(s->gm_st.p, s->h_gst, sizeof(GmresState), cudaMemcpyHostToDevice, s->stream));
 
+    double *F = flex ? s->gm_vecs.p + (int64_t)(restart + 3) * stride : nullptr;
+    double *Zv = flex ? F + (int64_t)(restart + 1) * stride : nullptr;
+    if (flex) CK(cudaMemsetAsync(Zv, 0, sizeof(double) * (size_t)stride * augk, s->stream));
     GmresBuffers B{n, s->x.p, s->rhs.p, s->diag.p, s->gm_vecs.p, s->gm_vecs.p + stride, stride, s->partials.p,
-                   s->gm_st.p};
+                   s->gm_st.p, F, Zv};
     phgGpuSystem_::GraphKey key{};
     key.x = B.x; key.r = B.z; key.p = B.V; key.D = B.D; key.Ap = B.st;
-    key.n = n * 100 + restart; key.lpr = s->plan.kind * 100 + s->plan.lpr * 10 + s->plan.unroll; key.s = s->stream;
+    key.n = (n * 100 + restart) * 2 + (flex ? 1 : 0); key.lpr = s->plan.kind * 100 + s->plan.lpr * 10 + s->plan.unroll; key.s = s->stream;
     plan_key(s, key);
     if (s->graph_gmres == nullptr || !(s->gkey_gmres == key)) {
         if (s->graph_gmres != nullptr) { cudaGraphExecDestroy(s->graph_gmres); s->graph_gmres = nullptr; }
@@ -1627,7 +1639,7 @@ int phgGpuSolverGMRES(phgGpuSystem *s, int restart, double rtol, double btol, do
         CK(e);
         s->gkey_gmres = key;
     }
-    const int per_cycle = 3 + restart * 2 + restart * (restart + 1) / 2;
+    const int per_cycle = 3 + restart * 2 + restart * (restart + 1) / 2;   // at most
     do {
         CK(cudaGraphLaunch(s->graph_gmres, s->stream));
         s->launches += per_cycle;
@@ -1641,6 +1653,17 @@ int phgGpuSolverGMRES(phgGpuSystem *s, int restart, double rtol, double btol, do
     CHECK_RC(copy_out(s, x, s->x.p, (size_t)n));
     CK(cudaStreamSynchronize(s->stream));
     return nits;
+}
+
+int phgGpuSolverGMRES(phgGpuSystem *s, int restart, double rtol, double btol, double atol, int maxit, double *x,
+                      double *residual) {
+    return gmres_impl(s, restart, -1, rtol, btol, atol, maxit, x, residual);
+}
+
+int phgGpuSolverFLGMRES(phgGpuSystem *s, int restart, int augk, double rtol, double btol, double atol, int maxit,
+                        double *x, double *residual) {
+    if (augk <= 0) augk = 2;   // solver-phg.c:2086-2087
+    return gmres_impl(s, restart, augk, rtol, btol, atol, maxit, x, residual);
 }
 
 int phgGpuSolverBiCGstab(phgGpuSystem *s, double rtol, double btol, double atol, int maxit, double *x,

@@ -1,5 +1,6 @@
 // Restarted right-preconditioned GMRES (solver_GMRES_r, solver-phg.c:
-// 1050-1260) with the Jacobi preconditioner.  One restart cycle is
+// 1050-1260) and PHG's default flexible augmented variant (solver_FLGMRES_r,
+// solver-phg.c:2063-2340) with the Jacobi preconditioner.  One restart cycle is
 //   resid     z = b - A x, ||z|| -> s_1 (and the tolerance, first cycle)
 //   per inner step i = 1..restart:
 //     pc      v_i = v_i / h_(i-1,i) (v_1 = z / ||z||), V_0 = v_i / diag
@@ -68,6 +69,8 @@ struct EpiResid {
             st->first = 0;
         }
         st->ninner = 0;
+        if (st->flexible)   // cycle k takes mk + min(k, augk) steps (solver-phg.c:2160-2164)
+            st->restart = st->mk + (st->itr_out <= st->augk ? st->itr_out : st->augk);
         if (!isfinite(rn)) {
             st->status = GMRES_NONFINITE;
             st->finished = 1;
@@ -111,6 +114,23 @@ gmres_pc_kernel(int64_t n, int i, const double *src, double *vi, double *__restr
         const double v = rn_mul(scale, src[l]);
         vi[l] = v;
         v0[l] = __ddiv_rn(v, D[l]);
+    }
+}
+
+// FLGMRES_r: v_i = scale * v_i as above; the step preconditions v_i (i <= mk)
+// or the stored correction Z_(i-mk-1) (solver-phg.c:2183-2188) into F_i, the
+// vector the product takes and the update keeps.
+__global__ void __launch_bounds__(kThreads)
+flgmres_pc_kernel(int64_t n, int64_t stride, int i, const double *src, double *vi, const double *Z,
+                  double *__restrict__ fi, const double *__restrict__ D, const GmresState *st) {
+    if (!st->run || st->cycle_done) return;
+    const double scale = __ddiv_rn(1.0, i == 1 ? st->r_norm : Hat(st, i - 1, i));
+    const bool aug = i > st->mk;
+    const double *za = aug ? Z + (int64_t)(i - st->mk - 1) * stride : vi;
+    for (int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < n; l += (int64_t)gridDim.x * blockDim.x) {
+        const double v = rn_mul(scale, src[l]);
+        vi[l] = v;
+        fi[l] = __ddiv_rn(aug ? za[l] : v, D[l]);
     }
 }
 
@@ -178,6 +198,11 @@ __global__ void gmres_solve_kernel(GmresState *st) {
         y[j] = __ddiv_rn(s[j], Hat(st, j, j));
         for (int k = j - 1; k > 0; k--) s[k] = rn_sub(s[k], rn_mul(Hat(st, j, k), y[j]));
     }
+    if (st->flexible) {
+        st->zi = st->itr_out % st->augk;
+        st->ak = st->itr_out < st->augk ? st->itr_out : st->augk;
+        st->itr_out += 1;
+    }
     if (st->status != GMRES_OK) {
         st->finished = 1;
     } else if (st->r_norm <= st->tol) {
@@ -208,6 +233,35 @@ gmres_update_kernel(int64_t n, int64_t stride, const double *__restrict__ V, con
     }
 }
 
+// FLGMRES_r's update (solver-phg.c:2250-2290): x += sum_j y_j F_j (the
+// cycle's starting residual z when it made no step), and the cycle's
+// correction sum_j y_j v_j (j <= mk) + sum_j y_(mk+j) Z_(j-1) (j <= ak) --
+// z itself when there was no step -- is stored in Z_zi.
+__global__ void __launch_bounds__(kThreads)
+flgmres_update_kernel(int64_t n, int64_t stride, const double *__restrict__ V, const double *__restrict__ F,
+                      double *Z, const double *__restrict__ z, double *__restrict__ x, const GmresState *st) {
+    if (!st->run) return;
+    const int i = st->ninner, mk = st->mk;
+    const double *y = st->y;
+    for (int64_t l = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; l < n; l += (int64_t)gridDim.x * blockDim.x) {
+        double c, w;
+        if (i > 0) {
+            c = rn_mul(y[1], F[stride + l]);
+            for (int j = 2; j <= i; j++) c = rn_add(c, rn_mul(y[j], F[(int64_t)j * stride + l]));
+            const int top = i <= mk ? i : mk;
+            w = rn_mul(y[1], V[stride + l]);
+            for (int j = 2; j <= top; j++) w = rn_add(w, rn_mul(y[j], V[(int64_t)j * stride + l]));
+            if (i > mk)
+                for (int j = 1; j <= st->ak; j++) w = rn_add(w, rn_mul(y[j + mk], Z[(int64_t)(j - 1) * stride + l]));
+        } else {
+            c = z[l];
+            w = c;
+        }
+        x[l] = rn_add(c, x[l]);
+        Z[(int64_t)st->zi * stride + l] = w;
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_gmres_cycle(const GmresBuffers &B, const SpmvPlan &P, int restart, cudaStream_t s) {
@@ -215,16 +269,27 @@ cudaError_t launch_gmres_cycle(const GmresBuffers &B, const SpmvPlan &P, int res
     const int vb = vgrid(n);
     double *V0 = B.V;
     auto Vi = [&](int i) { return B.V + (int64_t)i * B.stride; };
+    const bool flex = B.F != nullptr;
     launch_spmv_epi(P, B.x, EpiResid{B.z, B.b, B.partials, B.st->ticket, B.st}, s);
     for (int i = 1; i <= restart; i++) {
-        gmres_pc_kernel<<<vb, kThreads, 0, s>>>(n, i, i == 1 ? B.z : Vi(i), Vi(i), V0, B.D, B.st);
-        launch_spmv_epi(P, V0, EpiArnoldi{Vi(i + 1), Vi(1), B.partials, B.st->ticket, B.st, i}, s);
+        double *in = V0;
+        if (flex) {
+            in = B.F + (int64_t)i * B.stride;
+            flgmres_pc_kernel<<<vb, kThreads, 0, s>>>(n, B.stride, i, i == 1 ? B.z : Vi(i), Vi(i), B.Z, in, B.D,
+                                                      B.st);
+        } else {
+            gmres_pc_kernel<<<vb, kThreads, 0, s>>>(n, i, i == 1 ? B.z : Vi(i), Vi(i), V0, B.D, B.st);
+        }
+        launch_spmv_epi(P, in, EpiArnoldi{Vi(i + 1), Vi(1), B.partials, B.st->ticket, B.st, i}, s);
         for (int k = 2; k <= i + 1; k++)
             gmres_mgs_kernel<<<vb, kThreads, 0, s>>>(n, i, k, Vi(i + 1), Vi(k - 1), k <= i ? Vi(k) : nullptr,
                                                      B.partials, B.st);
     }
     gmres_solve_kernel<<<1, 32, 0, s>>>(B.st);
-    gmres_update_kernel<<<vb, kThreads, 0, s>>>(n, B.stride, B.V, B.z, B.D, B.x, B.st);
+    if (flex)
+        flgmres_update_kernel<<<vb, kThreads, 0, s>>>(n, B.stride, B.V, B.F, B.Z, B.z, B.x, B.st);
+    else
+        gmres_update_kernel<<<vb, kThreads, 0, s>>>(n, B.stride, B.V, B.z, B.D, B.x, B.st);
     return cudaGetLastError();
 }
 

@@ -15,6 +15,10 @@ struct GmresState {
     double r_norm, tol, residual, rtol, btol_bnorm, atol;
     int nits, maxit, restart, ninner;
     int run, cycle_done, finished, first, status;
+    // FLGMRES_r: base restart mk, augmenting corrections augk, cycle count,
+    // and for the cycle's update the slot its correction goes to and the
+    // number of corrections its basis used
+    int flexible, mk, augk, itr_out, zi, ak;
     unsigned ticket[kRedTickets];
     double *H, *c1, *c2, *s, *y;
 };
@@ -30,12 +34,18 @@ struct GmresBuffers {
     int64_t stride;
     double *partials;
     GmresState *st;
+    // FLGMRES_r only: F_1..F_R the preconditioned vectors of the steps (F_i
+    // at F + i * stride), Z_0..Z_(augk-1) the stored corrections
+    double *F, *Z;
 };
 
 inline int64_t gmres_small_doubles(int restart) { return (int64_t)(restart + 2) * (restart + 2) + 4 * (restart + 2); }
 
 // One restart cycle: b - A x and its norm, `restart` Arnoldi steps (each a
 // no-op once the cycle is over), the triangular solve and x += M^-1 V y.
+// With st->flexible (FLGMRES_r, solver-phg.c:2063-2340) `restart` is mk +
+// augk, the most steps a cycle takes; the cycle's own length is set by the
+// state.
 cudaError_t launch_gmres_cycle(const GmresBuffers &B, const SpmvPlan &P, int restart, cudaStream_t s);
 
 }  // namespace phgb

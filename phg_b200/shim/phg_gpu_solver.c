@@ -18,8 +18,9 @@
  *   phgSolverGpuPCGMixed_  Jacobi-PCG, FP32 inner iteration with FP64
  *                          reliable updates, the same FP64 stopping rule
  *   phgSolverGpuBiCGstab_  Jacobi-BiCGstab, FP64  (-solver bicgstab)
- *   phgSolverGpuGMRES_     restarted Jacobi-GMRES, FP64 (-solver gmres
- *                          -gmres_type gmres_r; restart from -gmres_restart)
+ *   phgSolverGpuGMRES_     restarted Jacobi-GMRES, FP64: PHG's -gmres_type
+ *                          (its default flgmres_r, or gmres_r), restart from
+ *                          -gmres_restart, augmentation from -lgmres_augk
  *
  * Tolerances, maxit and the initial guess are PHG's (solver->rtol, btol,
  * atol, maxit, x).  A PCG breakdown prints the reference's warning once and
@@ -48,6 +49,8 @@ typedef struct {
 #define _g ((GPU_DATA *)solver->oem_data)
 
 static INT gmres_restart = 10;	/* PHG's default (-gmres_restart) */
+static INT lgmres_augk = 2;	/* PHG's default (-lgmres_augk) */
+static int gmres_flexible = 1;	/* PHG's default -gmres_type is flgmres_r */
 
 static int
 Init(SOLVER *solver)
@@ -124,9 +127,15 @@ Solve(SOLVER *solver, VEC *x, BOOLEAN destroy)
 					&res, NULL);
 	    break;
 	default:
-	    nits = phgGpuSolverGMRES(_g->sys, gmres_restart, solver->rtol,
-				     solver->btol, solver->atol, solver->maxit,
-				     x->data, &res);
+	    if (gmres_flexible)
+		nits = phgGpuSolverFLGMRES(_g->sys, gmres_restart, lgmres_augk,
+					   solver->rtol, solver->btol,
+					   solver->atol, solver->maxit, x->data,
+					   &res);
+	    else
+		nits = phgGpuSolverGMRES(_g->sys, gmres_restart, solver->rtol,
+					 solver->btol, solver->atol,
+					 solver->maxit, x->data, &res);
 	    break;
     }
     if (nits < 0) {
@@ -163,13 +172,21 @@ static int
 InitGMRES(SOLVER *solver)
 {
     INT r;
+    const char *type;
 
     Init(solver);
     _g->kind = GPU_GMRES;
-    /* PHG's own -gmres_restart (registered by its GMRES, solver-phg.c:466) */
+    /* PHG's own GMRES options (registered by its GMRES, solver-phg.c:454-470) */
     r = phgOptionsGetInt("-gmres_restart");
     if (r > 0)
 	gmres_restart = r;
+    r = phgOptionsGetInt("-lgmres_augk");
+    lgmres_augk = r > 0 ? r : 2;
+    type = phgOptionsGetKeyword("-gmres_type");
+    if (type != NULL && strcmp(type, "flgmres_r") != 0 && strcmp(type, "gmres_r") != 0)
+	phgError(1, "%s: -gmres_type %s has no GPU counterpart (flgmres_r, gmres_r)\n",
+		 solver->oem_solver->name, type);
+    gmres_flexible = (type == NULL || strcmp(type, "flgmres_r") == 0);
     return 0;
 }
 

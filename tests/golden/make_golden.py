@@ -3,7 +3,8 @@ reference (PHG 0.9.7) built from its own sources by `make -C oracle ref`.
 
 For every case it writes the mesh as Medit, runs oracle/_ref/phg_dump (the
 reference's element loop + phgSolverAssemble + phgSolverUpdateRHS +
-phgSolverSolve with -solver pcg, bicgstab or gmres (gmres_r), see oracle/ref_driver/phg_dump.c) and stores
+phgSolverSolve with -solver pcg, bicgstab or gmres (gmres_r or PHG's default
+flgmres_r), see oracle/ref_driver/phg_dump.c) and stores
 the reference's own inputs (coordinates, element vertices and element->DOF
 maps as PHG numbered them, f and g at the DOF nodes, Dirichlet flags, kappa)
 and outputs (matrix rows before and after boundary elimination, saved
@@ -49,6 +50,10 @@ CASES = {
     "p1_m6_gmres": (6, 1, "sine", None, 1e-10, 0.0, "gmres_r"),
     "p2_m5_kappa_gmres": (5, 2, "sine", 12, 1e-10, 0.0, "gmres_r"),
     "p3_m3_mass_gmres": (3, 3, "linear", None, 1e-12, 25.0, "gmres_r"),
+    # PHG's default GMRES (FLGMRES_r: restart 10, two augmenting corrections)
+    "p1_m6_flgmres": (6, 1, "sine", None, 1e-10, 0.0, "flgmres_r"),
+    "p2_m5_kappa_flgmres": (5, 2, "sine", 12, 1e-10, 0.0, "flgmres_r"),
+    "p3_m3_mass_flgmres": (3, 3, "linear", None, 1e-12, 25.0, "flgmres_r"),
     # meshes PHG refined itself (the element and DOF numbering are PHG's):
     # the reference's test/cube.dat bisected uniformly, and a Kuhn cube
     # refined locally around the corner (0,0,0)
@@ -58,6 +63,7 @@ CASES = {
     "p3_corner_refined": (2, 3, "linear", None, 1e-10, 0.0, "pcg", dict(refine=2, refine_corner=5)),
 }
 GMRES_RESTART = 10   # the reference's default (-gmres_restart)
+LGMRES_AUGK = 2      # the reference's default (-lgmres_augk)
 
 
 def mesh_args(name, d):
@@ -86,14 +92,15 @@ def run_case(name, m, P, case, kseed, rtol, mass=0.0, solver="pcg", opts=None):
     with tempfile.TemporaryDirectory() as d:
         e = kuhn_cube(m)[1]
         args = [DUMP, *mesh_args(name, d), "-dof_type", "P%d" % P,
-                "-solver", "gmres" if solver == "gmres_r" else solver, "-pcg_pc_type", "jacobi", "-solver_rtol", repr(rtol),
+                "-solver", "gmres" if solver in ("gmres_r", "flgmres_r") else solver, "-pcg_pc_type", "jacobi",
+                "-solver_rtol", repr(rtol),
                 "-solver_btol", "0", "-solver_atol", "0", "-solver_maxit", "10000",
                 "-map_reorder", "no", "-dump_dir", d, "-rhs_case", case]
         if mass != 0.0:
             args += ["-mass_coef", repr(mass)]
-        if solver == "gmres_r":
-            args += ["-gmres_type", "gmres_r", "-gmres_pc_type", "jacobi",
-                     "-gmres_restart", str(GMRES_RESTART)]
+        if solver in ("gmres_r", "flgmres_r"):
+            args += ["-gmres_type", solver, "-gmres_pc_type", "jacobi",
+                     "-gmres_restart", str(GMRES_RESTART), "-lgmres_augk", str(LGMRES_AUGK)]
         kappa = None
         if kseed is not None:
             kappa = np.exp(np.random.default_rng(kseed).standard_normal(len(e)))

@@ -51,14 +51,18 @@ def test_golden_assembly_bitexact(gpu, name):
 
 @pytest.mark.parametrize("name", golden_cases())
 def test_golden_solve(gpu, name):
-    """The reference's solver of each golden case (PCG, BiCGstab or GMRES)."""
+    """The reference's solver of each golden case (PCG, BiCGstab, GMRES_r or
+    PHG's default GMRES, FLGMRES_r)."""
     G = load_golden(name)
     s = build(gpu, int(G["order"]), G["verts"], G["elems"], G["e2l"], G["bdry"], G["f"], G["g"],
               G.get("kappa"), float(G.get("mass", 0.0)))
     rtol = float(G["rtol"])
     solver = str(G["solver"]) if "solver" in G else "pcg"
-    if solver == "gmres_r":
-        x, nits, res = s.solve_gmres(restart=int(G["restart"]), rtol=rtol, btol=0.0, atol=0.0)
+    if solver in ("gmres_r", "flgmres_r"):
+        if solver == "gmres_r":
+            x, nits, res = s.solve_gmres(restart=int(G["restart"]), rtol=rtol, btol=0.0, atol=0.0)
+        else:
+            x, nits, res = s.solve_flgmres(restart=int(G["restart"]), augk=2, rtol=rtol, btol=0.0, atol=0.0)
         assert abs(nits - int(G["nits"])) <= 2
         ref = G["x"]
         assert np.linalg.norm(x - ref) <= solution_tol(rtol) * np.linalg.norm(ref)

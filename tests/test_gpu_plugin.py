@@ -49,7 +49,7 @@ def run(name, gpu_solver, extra=()):
                 "stdout": p.stdout}
 
 
-PLUGIN_OF = {"pcg": "pcg", "bicgstab": "bicgstab", "gmres_r": "gmres"}
+PLUGIN_OF = {"pcg": "pcg", "bicgstab": "bicgstab", "gmres_r": "gmres", "flgmres_r": "gmres"}
 
 
 def solver_of(name):
@@ -60,7 +60,9 @@ def solver_of(name):
 @pytest.mark.parametrize("name", golden_cases())
 def test_reference_program_through_gpu_oem_solver(name):
     G = load_golden(name)
-    out = run(name, PLUGIN_OF[solver_of(name)])
+    solver = solver_of(name)
+    extra = ("-gmres_type", solver) if solver in ("gmres_r", "flgmres_r") else ()
+    out = run(name, PLUGIN_OF[solver], extra)
     rtol = float(G["rtol"])
     assert np.array_equal(out["rhs"], G["rhs"])   # PHG's own assembly, unchanged
     assert abs(out["nits"] - int(G["nits"])) <= 2, (out["nits"], int(G["nits"]))

@@ -36,7 +36,8 @@ def solver_of(G):
 @pytest.mark.parametrize("name", golden_cases())
 def test_solver_bitexact(oracle, name):
     """Iteration count, final residual and solution of the reference's
-    solve_pcg, solver_BiCGstab or solver_GMRES_r, bit for bit."""
+    solve_pcg, solver_BiCGstab, solver_GMRES_r or solver_FLGMRES_r, bit for
+    bit."""
     G = load_golden(name)
     args = (G["rows_ptr"], G["rows_cols"], G["rows_vals"], G["diag"], G["rhs"])
     if solver_of(G) == "bicgstab":
@@ -45,6 +46,10 @@ def test_solver_bitexact(oracle, name):
     elif solver_of(G) == "gmres_r":
         x, nits, res = oracle.gmres(*args, restart=int(G["restart"]), rtol=float(G["rtol"]), btol=0.0,
                                     atol=0.0)
+        hist = None
+    elif solver_of(G) == "flgmres_r":
+        x, nits, res = oracle.flgmres(*args, restart=int(G["restart"]), augk=2, rtol=float(G["rtol"]),
+                                      btol=0.0, atol=0.0)
         hist = None
     else:
         x, nits, res, hist = oracle.pcg(*args, rtol=float(G["rtol"]), btol=0.0, atol=0.0)
