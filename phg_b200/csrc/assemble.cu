@@ -288,6 +288,126 @@ element_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, cons
 }
 
 // ---------------------------------------------------------------------------
+// Element kernel for P1 and P2: a lane per basis function, 32 / N elements
+// per warp (P1 eight, P2 three).  Lane b computes the gradients of basis b
+// at the stiffness points in registers and publishes them in shared memory;
+// then it computes column b of the element matrix, reading the gradient of
+// basis a (a = 0..N-1) with loads every lane of the element shares, and
+// stores Ke[e][a][b] directly (the lanes of an element write a row's N
+// consecutive entries).  Entry (a, b) and its mirror (b, a) come out bit for
+// bit equal to the reference's single evaluation of the pair: each product of
+// gradient components commutes and the sums run over the same components in
+// the same order.  Every operation is the one the warp-per-element kernel
+// performs (the reference's order, round-to-nearest, no contraction); what
+// changes is where the operands live: the pair sums read 40 shared-memory
+// words an element instead of hundreds, and the element matrix goes straight
+// to global memory.
+template <int P>
+__global__ void __launch_bounds__(128)
+element_lanes_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, const int32_t *__restrict__ e2l,
+                     const double *__restrict__ kappa, const double mass, const double *__restrict__ f,
+                     const ElemWeights Wt, const double *__restrict__ gk, const double *__restrict__ br,
+                     const double *__restrict__ brt, double *__restrict__ Ke, double *__restrict__ Re, int *status) {
+    using D = ElemDims<P>;
+    constexpr int N = D::N, QK = D::QK, QR = D::QR, W = 4;
+    constexpr int EPW = 32 / N;                  // elements per warp
+    constexpr int CS = QK * N;                   // component stride of the gk table
+    __shared__ double s_g[W][EPW][QK * 3][N];   // gradient component c at point q of basis b: [q * 3 + c][b]
+    __shared__ double s_f[W][EPW][N];
+    __shared__ double s_fq[W][EPW][QR];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int sub = lane / N, b = lane - sub * N;
+    const bool lane_ok = sub < EPW;
+    const int sl = lane_ok ? sub : 0;
+    double(*G)[N] = s_g[w][sl];
+    double *fl = s_f[w][sl], *fq = s_fq[w][sl];
+
+    for (int64_t e0 = ((int64_t)blockIdx.x * W + w) * EPW; e0 < nelem; e0 += (int64_t)gridDim.x * W * EPW) {
+        const int64_t e = e0 + sub;
+        const bool act = lane_ok && e < nelem;
+        const double *J = geo + (size_t)(act ? e : 0) * kGeo;
+        double kap = 0.0;
+        if (act && kappa != nullptr) {
+            kap = kappa[e];
+            if (b == 0 && !isfinite(kap)) atomicExch(status, PHGB_DEV_NONFINITE);
+        }
+        // gradients of basis b at the stiffness points
+        double g[QK][3];
+#pragma unroll
+        for (int q = 0; q < QK; q++) {
+            if (P == 1) {
+#pragma unroll
+                for (int c = 0; c < 3; c++) g[q][c] = act ? J[4 * b + c] : 0.0;
+            } else if (b < 4) {
+                const double d = gk[(b * QK + q) * N + b];
+#pragma unroll
+                for (int c = 0; c < 3; c++) g[q][c] = rn_mul(d, act ? J[4 * b + c] : 0.0);
+            } else {
+                const double *Gk = gk + q * N + b;
+                const double g0 = Gk[0], g1 = Gk[CS], g2 = Gk[2 * CS], g3 = Gk[3 * CS];
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const double j0 = act ? J[c] : 0.0, j1 = act ? J[4 + c] : 0.0;
+                    const double j2 = act ? J[8 + c] : 0.0, j3 = act ? J[12 + c] : 0.0;
+                    g[q][c] = rn_add(rn_add(rn_add(rn_mul(g0, j0), rn_mul(g1, j1)), rn_mul(g2, j2)), rn_mul(g3, j3));
+                }
+            }
+        }
+        double fv = 0.0;
+        if (act && f != nullptr) {
+            const int32_t d = e2l[(size_t)e * N + b];
+            if (d < 0 || d >= ndof) atomicExch(status, PHGB_DEV_BAD_INDEX);
+            else fv = f[d];
+            if (!isfinite(fv)) atomicExch(status, PHGB_DEV_NONFINITE);
+        }
+        if (lane_ok) {
+#pragma unroll
+            for (int q = 0; q < QK; q++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) G[q * 3 + c][b] = g[q][c];
+            fl[b] = fv;
+        }
+        __syncwarp();
+        // f_h at the RHS points (phgDofEval_: sum over the element's nodes)
+        if (lane_ok)
+            for (int q = b; q < QR; q += N) {
+                double v = 0.0;
+                for (int k = 0; k < N; k++) v = rn_add(v, rn_mul(brt[k * QR + q], fl[k]));
+                fq[q] = v;
+            }
+        __syncwarp();
+        const double vol = act ? J[16] : 0.0;
+        // column b of the element matrix
+        for (int a = 0; a < N; a++) {
+            double d = 0.;
+#pragma unroll
+            for (int q = 0; q < QK; q++) {
+                const double d0 = rn_add(0., rn_add(rn_add(rn_mul(g[q][0], G[q * 3][a]), rn_mul(g[q][1], G[q * 3 + 1][a])),
+                                                    rn_mul(g[q][2], G[q * 3 + 2][a])));
+                const double t = rn_mul(d0, Wt.wk[q]);
+                d = rn_add(d, kappa != nullptr ? rn_mul(t, kap) : t);
+            }
+            double v = rn_mul(d, vol);
+            if (mass != 0.0) {
+                double dm = 0.;
+                for (int q = 0; q < QR; q++) {
+                    const double d0 = rn_add(0., rn_mul(br[q * N + b], br[q * N + a]));
+                    dm = rn_add(dm, rn_mul(d0, Wt.wr[q]));
+                }
+                v = rn_add(v, rn_mul(mass, rn_mul(dm, vol)));
+            }
+            if (act) Ke[((size_t)e * N + a) * N + b] = v;
+        }
+        if (act) {
+            double d = 0.0;
+            for (int q = 0; q < QR; q++) d = rn_add(d, rn_mul(rn_mul(br[q * N + b], Wt.wr[q]), fq[q]));
+            Re[(size_t)e * N + b] = rn_mul(d, vol);
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
 // DOF -> (element, basis) incidence lists.
 
 __global__ void inc_count_kernel(int64_t nkeys, int N, int64_t ndof, const int32_t *__restrict__ e2l,
@@ -402,6 +522,14 @@ struct WalkCfg {
     static constexpr bool LONG = false;   // overflowing rows go to the list
 };
 
+// The pattern a build records for the next ones (phgGpuBuildLinearSystem
+// with the same mesh and DOF map): per contribution (row incidence, element
+// column) its first-touch position in the row or kSlotZero (an exact zero,
+// dropped); per first-touch position its place among the row's kept entries
+// (k) or, with kTmapBdry set, among its saved boundary columns (j).
+constexpr uint16_t kSlotZero = 0xffff;
+constexpr uint16_t kTmapBdry = 0x8000;
+
 // The second pass over the rows the first one could not hold (high-valence
 // vertices of locally refined meshes): a warp per row, a table of 2048 slots
 // for up to 1024 entries.
@@ -435,7 +563,8 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
                 int32_t *__restrict__ cnt_keep, int32_t *__restrict__ cnt_bdry,
                 int32_t *__restrict__ sc_cols, double *__restrict__ sc_vals,
                 double *__restrict__ rhs, double *__restrict__ diag, int *status,
-                int32_t *__restrict__ over_list, int *nover) {
+                int32_t *__restrict__ over_list, int *nover, uint16_t *__restrict__ slot,
+                uint16_t *__restrict__ tmap) {
     constexpr int G = C::G, R = C::R, HS = C::HS, MAXROW = C::MAXROW, W = C::WARPS;
     __shared__ int32_t s_key[W][R][HS];
     __shared__ int16_t s_pos[W][R][HS];
@@ -557,6 +686,10 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
             } else if (nz) {
                 sval[pos] = rn_add(sval[pos], v);
             }
+            // the pattern of later builds: where this contribution went (its
+            // first-touch position in the row), or that it was an exact zero
+            if (slot != nullptr && f0.ok)
+                slot[((int64_t)i0 + ii) * N + gl] = nz ? (uint16_t)min(pos, MAXROW) : kSlotZero;
             L += __popc(newm);
             f0 = f1; f1 = f2; f2 = f3;
             __syncwarp();
@@ -603,14 +736,18 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
             const unsigned km = __ballot_sync(0xffffffffu, valid && !isbc) & gmask;
             const unsigned bm = __ballot_sync(0xffffffffu, valid && isbc) & gmask;
             if (valid && !isbc) {
-                const int64_t q = rbase + nk + __popc(km & lt_mask);
+                const int k = nk + __popc(km & lt_mask);
+                const int64_t q = rbase + k;
                 sc_cols[q] = c;
                 sc_vals[q] = val;
+                if (tmap != nullptr) tmap[rbase + t] = (uint16_t)k;
             }
             if (valid && isbc) {
-                const int64_t q = rbase + rcap - 1 - (nb + __popc(bm & lt_mask));
+                const int j = nb + __popc(bm & lt_mask);
+                const int64_t q = rbase + rcap - 1 - j;
                 sc_cols[q] = c;
                 sc_vals[q] = val;
+                if (tmap != nullptr) tmap[rbase + t] = (uint16_t)(kTmapBdry | j);
             }
             nk += __popc(km);
             nb += __popc(bm);
@@ -637,6 +774,126 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
             // lift the boundary columns in first-touch order: r -= term
             for (int t = 0; t < L; t++)
                 if (scol[t] >= 0) r = rn_sub(r, sval[t]);
+            rhs[d] = r;
+        }
+        __syncwarp();
+    }
+}
+
+// A later build on the same pattern: the rows' values from the recorded
+// slots, without the column search.  Per row, the contributions are added in
+// element order at their recorded first-touch positions (so every entry is
+// the same sum in the same order as the full walk makes), then written to
+// their places in the CSR and the saved boundary columns, with the RHS
+// lifted as the walk does.  A contribution whose zero/non-zero status
+// differs from the recorded one means the pattern changed (status
+// PHGB_DEV_PATTERN_CHANGED): the caller runs the full walk instead.
+template <int N, class C>
+__global__ void __launch_bounds__(C::WARPS * 32, C::LONG ? 1 : 8)
+value_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t *__restrict__ inc,
+                  const uint8_t *__restrict__ bdry, const double *__restrict__ Ke, const double *__restrict__ Re,
+                  const double *__restrict__ g, const uint16_t *__restrict__ slot, const uint16_t *__restrict__ tmap,
+                  const int32_t *__restrict__ ptr, const int32_t *__restrict__ cols, const int32_t *__restrict__ bptr,
+                  const int32_t *__restrict__ bcols, double *__restrict__ vals, double *__restrict__ bvals,
+                  double *__restrict__ rhs, double *__restrict__ diag, int *status,
+                  const int32_t *__restrict__ over_list, const int *nover) {
+    constexpr int G = C::G, R = C::R, MAXROW = C::MAXROW, W = C::WARPS;
+    __shared__ double s_val[W][R][MAXROW];
+    __shared__ uint8_t s_isb[W][R][MAXROW];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int grp = lane / G, gl = lane % G;
+    double *sval = s_val[w][grp];
+    uint8_t *sisb = s_isb[w][grp];
+
+    const int64_t nwarps = (int64_t)gridDim.x * W;
+    const int64_t nrows = C::LONG ? (int64_t)*nover : ndof;
+    for (int64_t wb = ((int64_t)blockIdx.x * W + w) * R; wb < nrows; wb += nwarps * R) {
+        const int64_t d = C::LONG ? (wb + grp < nrows ? (int64_t)over_list[wb + grp] : ndof) : wb + grp;
+        const bool active = d < ndof;
+        int32_t i0 = 0, i1 = 0, p0 = 0, nk = 0, b0 = 0, nb = 0;
+        bool isb = false;
+        if (active) {
+            i0 = inc_ptr[d];
+            i1 = inc_ptr[d + 1];
+            isb = bdry[d] != 0;
+            p0 = ptr[d];
+            nk = ptr[d + 1] - p0;
+            b0 = bptr[d];
+            nb = bptr[d + 1] - b0;
+        }
+        const int L = nk + nb;
+        if (active && isb && gl == 0) {   // the Dirichlet row, as the walk makes it
+            const int mult = i1 - i0;
+            if (g != nullptr && !isfinite(g[d])) atomicExch(status, PHGB_DEV_NONFINITE);
+            double m = 0.0;
+            for (int i = 0; i < mult; i++) m = rn_add(m, 1.0);
+            if (mult > 0) {
+                vals[p0] = m;
+                bvals[b0] = m;
+            }
+            diag[d] = m;
+            rhs[d] = bdry_rhs(g, (int32_t)d, mult);
+        }
+        // rows the first pass cannot hold are the second pass's
+        const bool mine = C::LONG ? true : L <= MAXROW;
+        const bool walk = active && !isb && mine;
+        const int nwalk = walk ? i1 - i0 : 0;
+        const int maxwalk = __reduce_max_sync(0xffffffffu, (unsigned)nwalk);
+        if (maxwalk == 0) continue;   // warp-uniform
+        const int Lw = walk ? L : 0;
+        for (int t = gl; t < Lw; t += G) sval[t] = 0.0;
+        __syncwarp();
+        bool changed = false;
+        for (int ii = 0; ii < maxwalk; ii++) {
+            if (ii < nwalk && gl < N) {
+                const int32_t kk = inc[i0 + ii];
+                const int32_t e = kk / N, a = kk - e * N;
+                const double v = Ke[((size_t)e * N + a) * N + gl];
+                const uint16_t t = slot[((int64_t)i0 + ii) * N + gl];
+                if ((v != 0.0) != (t != kSlotZero) || (t != kSlotZero && t >= L)) changed = true;
+                else if (t != kSlotZero) sval[t] = rn_add(sval[t], v);
+            }
+            __syncwarp();
+        }
+        if (changed) atomicExch(status, PHGB_DEV_PATTERN_CHANGED);
+        // write the entries; boundary columns get their lift term in place
+        double dg = 0.0;
+        for (int t = gl; t < Lw; t += G) {
+            const uint16_t tm = tmap[(int64_t)i0 * N + t];
+            const double val = sval[t];
+            if (tm & kTmapBdry) {
+                const int j = tm & ~kTmapBdry;
+                const int32_t c = bcols[b0 + j];
+                bvals[b0 + j] = val;
+                const int mult = inc_ptr[c + 1] - inc_ptr[c];
+                double Dk = 0.0;
+                for (int m = 0; m < mult; m++) Dk = rn_add(Dk, 1.0);
+                const double rk = bdry_rhs(g, c, mult);
+                sval[t] = __ddiv_rn(rn_mul(rn_mul(1.0, rk), val), Dk);
+                sisb[t] = 1;
+            } else {
+                vals[p0 + tm] = val;
+                if (cols[p0 + tm] == d) dg = val;
+                sisb[t] = 0;
+            }
+        }
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) dg += __shfl_xor_sync(0xffffffffu, dg, o, G);
+        // element right-hand sides in element order, zeros skipped
+        double r = 0.0;
+        for (int base = 0; base < maxwalk; base += G) {
+            const int ii = base + gl;
+            const double bb = (walk && ii < nwalk) ? Re[inc[i0 + ii]] : 0.0;
+            for (int t = 0; t < G; t++) {
+                const double bt = __shfl_sync(0xffffffffu, bb, t, G);
+                if (gl == 0 && base + t < nwalk && bt != 0.0) r = rn_add(r, bt);
+            }
+        }
+        __syncwarp();
+        if (walk && gl == 0) {
+            diag[d] = dg;
+            for (int t = 0; t < L; t++)
+                if (sisb[t]) r = rn_sub(r, sval[t]);
             rhs[d] = r;
         }
         __syncwarp();
@@ -683,12 +940,19 @@ static void elem_launch(const ElemArgs &A, cudaStream_t s) {
     constexpr int W = ElemDims<P>::WARPS;
     geometry_kernel<<<grid_for(A.nelem, 128, 148 * 64), 128, 0, s>>>(A.nelem, A.nvert, A.verts, A.elems, A.geo,
                                                                     A.status);
-    const int blocks = grid_for(A.nelem, W, 148 * 64);
     ElemWeights Wt{};
     for (int q = 0; q < ElemDims<P>::QK; q++) Wt.wk[q] = A.wk_host[q];
     for (int q = 0; q < ElemDims<P>::QR; q++) Wt.wr[q] = A.wr_host[q];
-    element_kernel<P><<<blocks, W * 32, 0, s>>>(A.nelem, A.ndof, A.geo, A.e2l, A.kappa, A.mass, A.f, Wt, A.gk,
-                                                A.br, A.brt, A.Ke, A.Re, A.status);
+    if constexpr (P <= 2) {   // a lane per basis function
+        constexpr int EPB = 4 * (32 / ElemDims<P>::N);   // elements per block
+        const int blocks = grid_for(A.nelem, EPB, 148 * 64);
+        element_lanes_kernel<P><<<blocks, 128, 0, s>>>(A.nelem, A.ndof, A.geo, A.e2l, A.kappa, A.mass, A.f, Wt,
+                                                       A.gk, A.br, A.brt, A.Ke, A.Re, A.status);
+    } else {          // P3: a warp per element
+        const int blocks = grid_for(A.nelem, W, 148 * 64);
+        element_kernel<P><<<blocks, W * 32, 0, s>>>(A.nelem, A.ndof, A.geo, A.e2l, A.kappa, A.mass, A.f, Wt, A.gk,
+                                                    A.br, A.brt, A.Ke, A.Re, A.status);
+    }
 }
 
 cudaError_t launch_element_kernel(int p, const ElemArgs &A, cudaStream_t s) {
@@ -736,13 +1000,32 @@ static cudaError_t walk(const WalkArgs &A, cudaStream_t s) {
     if (e != cudaSuccess) return e;
     row_walk_kernel<N, WalkCfg<N>><<<blocks, W * 32, 0, s>>>(
         A.ndof, A.inc_ptr, A.inc, A.e2l, A.bdry, A.Ke, A.Re, A.g, A.cnt_keep, A.cnt_bdry, A.sc_cols, A.sc_vals,
-        A.rhs, A.diag, A.status, A.over_list, A.nover);
+        A.rhs, A.diag, A.status, A.over_list, A.nover, A.slot, A.tmap);
     // the rows the first pass listed (none in most meshes: the blocks return
     // after reading the count)
     row_walk_kernel<N, LongWalkCfg<N>><<<148 * 4, 32, 0, s>>>(
         A.ndof, A.inc_ptr, A.inc, A.e2l, A.bdry, A.Ke, A.Re, A.g, A.cnt_keep, A.cnt_bdry, A.sc_cols, A.sc_vals,
-        A.rhs, A.diag, A.status, A.over_list, A.nover);
+        A.rhs, A.diag, A.status, A.over_list, A.nover, A.slot, A.tmap);
     return cudaGetLastError();
+}
+
+template <int N>
+static cudaError_t value_walk(const WalkArgs &A, cudaStream_t s) {
+    constexpr int W = WalkCfg<N>::WARPS, R = WalkCfg<N>::R;
+    const int blocks = grid_for(ceil_div(A.ndof, R), W, 148 * 32);
+    value_walk_kernel<N, WalkCfg<N>><<<blocks, W * 32, 0, s>>>(
+        A.ndof, A.inc_ptr, A.inc, A.bdry, A.Ke, A.Re, A.g, A.slot, A.tmap, A.ptr, A.cols, A.bptr, A.bcols, A.vals,
+        A.bvals, A.rhs, A.diag, A.status, A.over_list, A.nover);
+    value_walk_kernel<N, LongWalkCfg<N>><<<148 * 4, 32, 0, s>>>(
+        A.ndof, A.inc_ptr, A.inc, A.bdry, A.Ke, A.Re, A.g, A.slot, A.tmap, A.ptr, A.cols, A.bptr, A.bcols, A.vals,
+        A.bvals, A.rhs, A.diag, A.status, A.over_list, A.nover);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_value_walk(int p, const WalkArgs &A, cudaStream_t s) {
+    if (p == 1) return value_walk<4>(A, s);
+    if (p == 2) return value_walk<10>(A, s);
+    return value_walk<20>(A, s);
 }
 
 cudaError_t launch_row_walk(int p, const WalkArgs &A, cudaStream_t s) {

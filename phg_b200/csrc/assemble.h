@@ -43,6 +43,9 @@ struct WalkArgs {
     // entries; *nover zeroed before the walk)
     int32_t *over_list;
     int *nover;
+    // the pattern: recorded by the walk when non-null (nelem * N * N
+    // entries each, indexed like the scratch regions), read by the value walk
+    uint16_t *slot, *tmap;
 };
 
 cudaError_t launch_element_kernel(int p, const ElemArgs &a, cudaStream_t s);
@@ -56,6 +59,10 @@ cudaError_t launch_scan(int64_t n, const int32_t *in, int32_t *out, int64_t *ws,
 // then, after the counts are scanned into ptr/bptr, the copy into the CSR.
 cudaError_t launch_row_walk(int p, const WalkArgs &a, cudaStream_t s);
 cudaError_t launch_compact(int N, const WalkArgs &a, cudaStream_t s);
+// A build on the recorded pattern: writes vals, bvals, rhs and diag in place
+// (ptr, cols, bptr, bcols as the recording build left them); a changed
+// pattern sets PHGB_DEV_PATTERN_CHANGED.
+cudaError_t launch_value_walk(int p, const WalkArgs &a, cudaStream_t s);
 // Longest row the walk assembles (its second pass); longer rows are
 // PHG_GPU_ERR_LIMIT.
 int row_walk_max_row(int p);

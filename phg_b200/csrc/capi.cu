@@ -178,6 +178,12 @@ struct phgGpuSystem_ {
     DevBuf<int32_t> cnt_keep, cnt_bdry;
     DevBuf<int32_t> over_list;        // rows the row walk's second pass assembles
     DevBuf<int> nover;
+    // the assembly pattern of this mesh and DOF map (slots of the
+    // contributions, places of the row entries), for builds that only change
+    // kappa, f, g or the mass coefficient: 0 none yet, 1 one build done (the
+    // next records the pattern), 2 recorded (builds use the value walk)
+    int pattern_state = 0;
+    DevBuf<uint16_t> slot, tmap;
 
     // assembled system
     int64_t n = 0, nnz = 0, bnnz = 0;
@@ -235,6 +241,7 @@ struct phgGpuSystem_ {
     DevBuf<uint16_t> q16_len, q16_split, q16_cols;
     DevBuf<float> q16_v32;
     DevBuf<double> q16_v64;
+    DevBuf<int32_t> q16_src;          // CSR index of each stored q16 entry (value refills)
     DevBuf<int> q16_nofit;
     int *h_nofit = nullptr;
     int64_t sell2_total = 0, q16_total = 0;   // stored entries (padding included)
@@ -368,6 +375,29 @@ int solver_buffers(phgGpuSystem *s) {
 }
 
 // Forgets every layout derived from the matrix (called when it changes).
+// New values in an unchanged pattern: the layouts built so far keep their
+// structure and take the values again.
+int refresh_layout_values(phgGpuSystem *s) {
+    const int64_t n = s->n;
+    if (s->sell_valid) {
+        CK(launch_sell_fill(n, s->rp.p, s->ci.p, s->va.p, s->sell_perm.p, s->sell_len.p, s->sell_sptr.p,
+                            s->sell_cols.p, s->sell_vals.p, s->sell_vals32.p, s->stream));
+        s->launches += 1;
+    }
+    if (s->sell2_valid) {
+        const int64_t nsl = sell_positions(n) / 32;
+        const SellView S{n, nsl, s->sell_perm.p, s->sell_len.p, nullptr, nullptr, nullptr, nullptr};
+        CK(launch_sell2_fill(S, s->rp.p, s->ci.p, s->va.p, s->sell2_order.p, s->sell2_sptr.p, s->sell2_perm.p,
+                             s->sell2_len.p, s->sell2_cols.p, s->sell2_vals.p, s->stream));
+        s->launches += 1;
+    }
+    if (s->q16_valid && s->q16_fits) {
+        CK(launch_q16_refill(s->q16_total, s->q16_src.p, s->va.p, s->q16_v32.p, s->q16_v64.p, s->stream));
+        s->launches += 1;
+    }
+    return PHG_GPU_OK;
+}
+
 void invalidate_layouts(phgGpuSystem *s) {
     s->sell_sorted = false;
     s->order_valid = false;
@@ -507,6 +537,7 @@ int ensure_q16(phgGpuSystem *s) {
     CHECK_RC(s->q16_cols.ensure((size_t)total));
     CHECK_RC(s->q16_v32.ensure((size_t)total));
     CHECK_RC(s->q16_v64.ensure((size_t)total));
+    CHECK_RC(s->q16_src.ensure((size_t)total));
     CHECK_RC(s->q16_perm.ensure((size_t)npos));
     CHECK_RC(s->q16_len.ensure((size_t)npos));
     CHECK_RC(s->q16_split.ensure((size_t)npos));
@@ -514,7 +545,7 @@ int ensure_q16(phgGpuSystem *s) {
     CHECK_RC(s->q16_b1.ensure((size_t)npos));
     CK(cudaMemsetAsync(s->q16_nofit.p, 0, sizeof(int), s->stream));
     const Q16Out O{s->q16_sptr.p, s->q16_perm.p, s->q16_len.p, s->q16_split.p, s->q16_b0.p, s->q16_b1.p,
-                   s->q16_cols.p, s->q16_v32.p, s->q16_v64.p};
+                   s->q16_cols.p, s->q16_v32.p, s->q16_v64.p, s->q16_src.p};
     CK(launch_q16_fill(nsl, s->rp.p, s->ci.p, s->va.p, s->sell_perm.p, s->sell_len.p, s->sell2_order.p, O,
                        s->q16_nofit.p, s->stream));
     CK(cudaMemcpyAsync(s->h_nofit, s->q16_nofit.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
@@ -829,6 +860,7 @@ int phgGpuSetMesh(phgGpuSystem *s, int64_t nvert, const double *verts, int64_t n
     CHECK_RC(copy_in(s, s->elems.p, elem_verts, 4 * (size_t)nelem));
     s->nvert = nvert;
     s->nelem = nelem;
+    s->pattern_state = 0;
     s->have_mesh = true;
     s->have_dofs = false;
     s->assembled = false;
@@ -860,6 +892,7 @@ int phgGpuSetDofMap(phgGpuSystem *s, int order, int64_t ndof, const int32_t *e2l
     s->order = order;
     s->N = N;
     s->ndof = ndof;
+    s->pattern_state = 0;
     CHECK_RC(check_status(s, "phgGpuSetDofMap"));
     s->have_dofs = true;
     s->assembled = false;
@@ -916,6 +949,37 @@ static int build_system(phgGpuSystem *s, const double *kappa, double mass, const
     CHECK_RC(s->over_list.ensure((size_t)ndof));
     CHECK_RC(s->nover.ensure(1));
     wa.over_list = s->over_list.p; wa.nover = s->nover.p;
+    if (s->pattern_state == 2 && s->assembled && s->have_bdry_cols) {
+        // the recorded pattern: values only, written in place
+        wa.slot = s->slot.p; wa.tmap = s->tmap.p;
+        wa.ptr = s->rp.p; wa.cols = s->ci.p; wa.vals = s->va.p;
+        wa.bptr = s->brp.p; wa.bcols = s->bci.p; wa.bvals = s->bva.p;
+        CK(launch_value_walk(s->order, wa, s->stream));
+        s->launches += 2;
+        CK(cudaMemcpyAsync(s->h_status, s->status.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+        if (*s->h_status == PHGB_DEV_PATTERN_CHANGED) {   // an exact zero appeared or went: walk again
+            *s->h_status = 0;
+            CK(cudaMemsetAsync(s->status.p, 0, sizeof(int), s->stream));
+            s->pattern_state = 1;
+        } else {
+            CHECK_RC(check_status(s, "phgGpuBuildLinearSystem"));
+            CHECK_RC(refresh_layout_values(s));
+            s->mass = mass;
+            return PHG_GPU_OK;
+        }
+    }
+    // the second build on this mesh and DOF map records the pattern
+    const bool record = s->pattern_state == 1;
+    if (record) {
+        CHECK_RC(s->slot.ensure(nscratch));
+        CHECK_RC(s->tmap.ensure(nscratch));
+        wa.slot = s->slot.p;
+        wa.tmap = s->tmap.p;
+    } else {
+        wa.slot = nullptr;
+        wa.tmap = nullptr;
+    }
     CK(launch_row_walk(s->order, wa, s->stream));
     s->launches += 8;   // walk (two passes) + two scans
     CK(launch_scan(ndof, s->cnt_keep.p, s->rp.p, s->scan_ws.p, s->stream));
@@ -942,6 +1006,7 @@ static int build_system(phgGpuSystem *s, const double *kappa, double mass, const
     invalidate_layouts(s);
     s->lpr = spmv_lanes_for((double)s->nnz / (double)ndof);
     s->mass = mass;
+    s->pattern_state = record ? 2 : 1;
     return PHG_GPU_OK;
 }
 
@@ -998,6 +1063,7 @@ int phgGpuSetMatrix(phgGpuSystem *s, int64_t n, const int64_t *ptr, const int32_
     s->n = n;
     s->nnz = nnz;
     s->bnnz = 0;
+    s->pattern_state = 0;
     s->assembled = true;
     s->have_bdry_cols = false;
     invalidate_layouts(s);

@@ -36,7 +36,8 @@ q16_fill_kernel(int64_t npos, const int32_t *__restrict__ rp, const int32_t *__r
                 const uint16_t *__restrict__ sell_len, const int32_t *__restrict__ order,
                 const int32_t *__restrict__ sptr, int32_t *__restrict__ perm, uint16_t *__restrict__ len,
                 uint16_t *__restrict__ split, int32_t *__restrict__ base0, int32_t *__restrict__ base1,
-                uint16_t *__restrict__ cols, float *__restrict__ vals32, double *__restrict__ vals64, int *nofit) {
+                uint16_t *__restrict__ cols, float *__restrict__ vals32, double *__restrict__ vals64,
+                int32_t *__restrict__ src, int *nofit) {
     for (int64_t pos = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pos < npos;
          pos += (int64_t)gridDim.x * blockDim.x) {
         const int64_t k = pos >> 5;
@@ -76,6 +77,7 @@ q16_fill_kernel(int64_t npos, const int32_t *__restrict__ rp, const int32_t *__r
                 const double v = va[r0 + t];
                 vals64[idx] = v;
                 vals32[idx] = (float)v;
+                src[idx] = (int32_t)(r0 + t);
             }
             j = l;
         }
@@ -84,6 +86,7 @@ q16_fill_kernel(int64_t npos, const int32_t *__restrict__ rp, const int32_t *__r
             cols[idx] = 0;
             vals64[idx] = 0.0;
             vals32[idx] = 0.0f;
+            src[idx] = -1;
         }
         perm[pos] = row;
         len[pos] = (uint16_t)l;
@@ -177,7 +180,23 @@ cudaError_t launch_q16_fill(int64_t nslices, const int32_t *rp, const int32_t *c
     const int64_t npos = nslices * 32;
     q16_fill_kernel<<<vec_blocks(npos), kVecThreads, 0, s>>>(npos, rp, ci, va, sell_perm, sell_len, order, O.sptr,
                                                              O.perm, O.len, O.split, O.base0, O.base1, O.cols,
-                                                             O.vals32, O.vals64, nofit);
+                                                             O.vals32, O.vals64, O.src, nofit);
+    return cudaGetLastError();
+}
+
+__global__ void q16_refill_kernel(int64_t total, const int32_t *__restrict__ src, const double *__restrict__ va,
+                                  float *__restrict__ vals32, double *__restrict__ vals64) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t k = src[i];
+        const double v = k >= 0 ? va[k] : 0.0;
+        vals64[i] = v;
+        vals32[i] = (float)v;
+    }
+}
+
+cudaError_t launch_q16_refill(int64_t total, const int32_t *src, const double *va, float *vals32, double *vals64,
+                              cudaStream_t s) {
+    q16_refill_kernel<<<vec_blocks(total), kVecThreads, 0, s>>>(total, src, va, vals32, vals64);
     return cudaGetLastError();
 }
 

@@ -13,6 +13,7 @@ struct Q16Out {
     uint16_t *cols;
     float *vals32;
     double *vals64;
+    int32_t *src;      // CSR index of each stored entry, -1 for padding (for value refills)
 };
 
 // Slice sizes (entries) of the stored slices; then the fill from CSR.
@@ -27,6 +28,10 @@ cudaError_t launch_q16_fill(int64_t nslices, const int32_t *rp, const int32_t *c
                             const Q16Out &O, int *nofit, cudaStream_t s);
 
 // FP32 product y = A x (unroll 1 or 2 steps), FP64 product y = A x.
+// New values for the same pattern: vals64[i] = va[src[i]], vals32[i] its
+// rounding (0 for padding), over the `total` stored entries.
+cudaError_t launch_q16_refill(int64_t total, const int32_t *src, const double *va, float *vals32, double *vals64,
+                              cudaStream_t s);
 cudaError_t launch_q16_spmv32(const Q16View &Q, int unroll, const float *x, float *y, cudaStream_t s);
 cudaError_t launch_q16_spmv64(const Q16View &Q, const double *x, double *y, cudaStream_t s);
 

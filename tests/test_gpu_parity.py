@@ -289,3 +289,41 @@ def test_zero_rhs_gives_zero(gpu):
     x, nits, res = s.solve_pcg(x0=np.ones(len(G["bdry"])))
     assert nits == 0 and not x.any()
     s.close()
+
+
+def test_rebuild_on_recorded_pattern(gpu, oracle):
+    """Repeated builds on one mesh and DOF map: the second records the
+    pattern, later ones add the contributions at their recorded places (the
+    value walk).  Every build is bit for bit the oracle's, including a kappa
+    with zeros (whole element matrices vanish: the pattern changes and the
+    build walks the rows again) and the return to the old pattern; solves on
+    the refreshed layouts match the oracle's."""
+    import phg_b200 as pb
+    v, e = pb.kuhn_cube(7)
+    e2l, bdry, nodes = pb.lagrange_dofs(v, e, 2)
+    f = pb.sine_source(nodes)
+    rng = np.random.default_rng(5)
+    kappas = [np.exp(rng.standard_normal(len(e))) for _ in range(4)]
+    kz = kappas[3].copy()
+    kz[rng.choice(len(e), 40, replace=False)] = 0.0
+    seq = [kappas[0], kappas[1], kappas[2], kz, kappas[3], kappas[0]]
+    with gpu.Solver(0) as s:
+        s.set_mesh(v, e)
+        s.set_dof_map(2, e2l, bdry)
+        for i, k in enumerate(seq):
+            s.build_linear_system(kappa=k, f=f)
+            o = oracle.assemble(2, v, e, e2l, bdry, f, kappa=k)
+            ptr, cols, vals = s.get_matrix()
+            assert np.array_equal(ptr, o["ptr"]) and np.array_equal(cols, o["cols"]), i
+            assert np.array_equal(vals, o["vals"]), i
+            bp, bc, bv = s.get_bdry_columns()
+            assert np.array_equal(bc, o["bcols"]) and np.array_equal(bv, o["bvals"]), i
+            assert np.array_equal(s.get_rhs(), o["rhs"]) and np.array_equal(s.get_diagonal(), o["diag"]), i
+            if i in (2, 5):   # solves on the layouts refreshed in place
+                x, nits, _ = s.solve_pcg(rtol=1e-10, btol=0.0, atol=0.0)
+                xm, nm, rm, _ = s.solve_pcg_mixed(rtol=1e-10)
+                xo, no, _, _ = oracle.pcg(o["ptr"], o["cols"], o["vals"], o["diag"], o["rhs"], rtol=1e-10,
+                                          btol=0.0, atol=0.0)
+                assert abs(nits - no) <= 2
+                assert np.linalg.norm(x - xo) <= 1e-7 * np.linalg.norm(xo)
+                assert rm <= 1e-10 * np.linalg.norm(o["rhs"]) * (1 + 1e-9)
