@@ -7,15 +7,18 @@
  *
  *   FLOAT  phgQuadGradBasAGradBas(ELEMENT *e, DOF *u, int n, DOF *A,
  *                                 DOF *v, int m, int order)
+ *   FLOAT  phgQuadBasABas(ELEMENT *e, DOF *u, int n, DOF *A, DOF *v,
+ *                         int m, int order)
  *   FLOAT *phgQuadDofTimesBas(ELEMENT *e, DOF *u, DOF *v, int n, int order,
  *                             FLOAT *res)
  *
- * with the reference's signatures (include/phg/quad.h:136-139).  For the
+ * with the reference's signatures (include/phg/quad.h:136-146).  For the
  * cases the GPU element kernel covers -- u == v a scalar Lagrange P1/P2/P3
- * DOF, A NULL or a scalar P0 coefficient, the default quadrature order --
- * the first call for a mesh computes every element's matrix (or right-hand
- * side) with phgGpuElementMatrices and later calls read the table: the
- * values are bit for bit those of src/quad.c:5260-5344 and 5481-5530.
+ * DOF, A NULL or a scalar P0 coefficient (NULL only, for the mass matrix
+ * phgQuadBasDotBas), the default quadrature order -- the first call for a
+ * mesh computes every element's matrix (or right-hand side) with
+ * phgGpuElementMatrices and later calls read the table: the values are bit
+ * for bit those of src/quad.c:5260-5344, 5582-5674 and 5481-5530.
  * Every other call goes to PHG's own function (dlsym RTLD_NEXT), so an
  * unmodified user program (examples/poisson.c) runs unchanged.
  *
@@ -39,6 +42,7 @@
 
 typedef FLOAT (*gbag_fn)(ELEMENT *, DOF *, int, DOF *, DOF *, int, int);
 typedef FLOAT *(*dtb_fn)(ELEMENT *, DOF *, DOF *, int, int, FLOAT *);
+typedef FLOAT (*baab_fn)(ELEMENT *, DOF *, int, DOF *, DOF *, int, int);
 
 typedef struct {
     FLOAT *val;              /* nelem x N x N (matrices) or nelem x N (rhs) */
@@ -57,8 +61,8 @@ static struct {
     INT nelem;
     DOF_TYPE *type;
     int N, p;
-    Table K, R;
-    long served_k, served_r, forwarded;
+    Table K, R, M;
+    long served_k, served_r, served_m, forwarded;
     int stats_registered;
 } S = {PTHREAD_MUTEX_INITIALIZER};
 
@@ -71,6 +75,12 @@ static gbag_fn orig_gbag(void) {
 static dtb_fn orig_dtb(void) {
     static dtb_fn f = NULL;
     if (f == NULL) f = (dtb_fn)dlsym(RTLD_NEXT, "phgQuadDofTimesBas");
+    return f;
+}
+
+static baab_fn orig_baab(void) {
+    static baab_fn f = NULL;
+    if (f == NULL) f = (baab_fn)dlsym(RTLD_NEXT, "phgQuadBasABas");
     return f;
 }
 
@@ -96,8 +106,8 @@ static uint64_t checksum(DOF *d) {
 }
 
 static void print_stats(void) {
-    fprintf(stderr, "phg_quad_shim: stiffness %ld from the GPU table, rhs %ld, forwarded %ld\n", S.served_k,
-            S.served_r, S.forwarded);
+    fprintf(stderr, "phg_quad_shim: stiffness %ld from the GPU table, rhs %ld, mass %ld, forwarded %ld\n",
+            S.served_k, S.served_r, S.served_m, S.forwarded);
 }
 
 static void fail(const char *what) {
@@ -135,7 +145,7 @@ static void prepare(GRID *g, DOF *u) {
     S.serial = g->serial_no;
     S.nelem = g->nelem;
     S.type = u->type;
-    S.K.valid = S.R.valid = 0;
+    S.K.valid = S.R.valid = S.M.valid = 0;
     if (!S.stats_registered && getenv("PHG_QUAD_SHIM_STATS") != NULL) {
         atexit(print_stats);
         S.stats_registered = 1;
@@ -159,6 +169,18 @@ static void build_K(DOF *A, ELEMENT *e, int n, int m) {
     S.K.first_n = n;
     S.K.first_m = m;
     S.K.valid = 1;
+}
+
+/* The mass matrices: with kappa = 0 the element kernel's entry is
+ * 0 + 1 * (vol * sum_q w_q phi_n phi_m), the reference's phgQuadBasABas
+ * value (A = NULL, order 2p). */
+static void build_M(void) {
+    FLOAT *zero = (FLOAT *)calloc((size_t)S.nelem, sizeof(FLOAT));
+    S.M.val = (FLOAT *)realloc(S.M.val, sizeof(FLOAT) * (size_t)S.nelem * S.N * S.N);
+    if (phgGpuElementMatrices(S.sys, zero, 1.0, NULL, S.M.val, NULL) != PHG_GPU_OK) fail("phgGpuElementMatrices");
+    free(zero);
+    S.M.coef = NULL;
+    S.M.valid = 1;
 }
 
 static void build_R(DOF *f, ELEMENT *e, int n) {
@@ -210,4 +232,23 @@ FLOAT *phgQuadDofTimesBas(ELEMENT *e, DOF *u, DOF *v, int n, int order, FLOAT *r
     S.served_r++;
     pthread_mutex_unlock(&S.lock);
     return res;
+}
+
+FLOAT phgQuadBasABas(ELEMENT *e, DOF *u, int n, DOF *A, DOF *v, int m, int order) {
+    const int p = lagrange_order(u);
+    FLOAT r;
+    /* A != NULL, another order, or a type with mass lumping go to PHG */
+    if (p == 0 || v != u || A != NULL || (order >= 0 && order != 2 * p) ||
+        (u->type->mass_lumping != NULL && u->type->mass_lumping->weights != NULL)) {
+        __atomic_add_fetch(&S.forwarded, 1, __ATOMIC_RELAXED);
+        return orig_baab()(e, u, n, A, v, m, order);
+    }
+    pthread_mutex_lock(&S.lock);
+    prepare(u->g, u);
+    if (!S.M.valid)
+        build_M();
+    r = S.M.val[((size_t)e->index * S.N + m) * S.N + n];
+    S.served_m++;
+    pthread_mutex_unlock(&S.lock);
+    return r;
 }

@@ -66,6 +66,20 @@ GMRES_RESTART = 10   # the reference's default (-gmres_restart)
 LGMRES_AUGK = 2      # the reference's default (-lgmres_augk)
 
 
+def input_mesh(name):
+    """Text of a case's input mesh file that is not generated here: the
+    reference's test/cube.dat, read from the reference tree when generating
+    and kept in the case's fixture (key input_mesh) for runs without it."""
+    fx = os.path.join(HERE, name + ".npz")
+    if os.path.exists(fx):
+        with np.load(fx) as z:
+            if "input_mesh" in z.files:
+                return str(z["input_mesh"])
+    ref = os.environ.get("PHG_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference")
+    with open(os.path.join(ref, "test", "cube.dat")) as src:
+        return src.read()
+
+
 def mesh_args(name, d):
     """Writes the case's input mesh into directory d and returns the driver
     arguments that read (and, for the refined cases, refine) it."""
@@ -74,9 +88,8 @@ def mesh_args(name, d):
     path = os.path.join(d, "m.mesh")
     if opts.get("mesh") == "cube.dat":
         path = os.path.join(d, "cube.dat")   # ALBERT format, recognised by its name
-        ref = os.environ.get("PHG_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference")
-        with open(os.path.join(ref, "test", "cube.dat")) as src, open(path, "w") as dst:
-            dst.write(src.read())
+        with open(path, "w") as dst:
+            dst.write(input_mesh(name))
     else:
         v, e = kuhn_cube(m)
         write_medit(path, v, e)
@@ -124,6 +137,8 @@ def run_case(name, m, P, case, kseed, rtol, mass=0.0, solver="pcg", opts=None):
             diag=L("diag.f64", np.float64), x=L("x.f64", np.float64))
         if kappa is not None:
             out["kappa"] = L("kappa.f64", np.float64)
+        if (opts or {}).get("mesh") == "cube.dat":
+            out["input_mesh"] = np.array(input_mesh(name))
         for pre in ("rows_raw", "rows", "bdry_rows"):
             out[pre + "_ptr"] = L(pre + "_ptr.i64", np.int64)
             out[pre + "_cols"] = L(pre + "_cols.i32", np.int32)

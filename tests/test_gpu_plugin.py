@@ -20,18 +20,17 @@ pytestmark = pytest.mark.gpu
 
 DUMP = os.path.join(ROOT, "oracle", "_ref", "phg_dump_gpu")
 sys.path.insert(0, GOLDEN)
-from make_golden import CASES, GMRES_RESTART  # noqa: E402
+from make_golden import CASES, GMRES_RESTART, mesh_args  # noqa: E402
 
 
 def run(name, gpu_solver, extra=()):
     m, P, case, kseed, rtol, *rest = CASES[name]
     mass = rest[0] if rest else 0.0
     solver = rest[1] if len(rest) > 1 else "pcg"
-    from phg_b200.mesh import kuhn_cube, write_medit
+    from phg_b200.mesh import kuhn_cube
     with tempfile.TemporaryDirectory() as d:
-        v, e = kuhn_cube(m)
-        write_medit(os.path.join(d, "m.mesh"), v, e)
-        args = [DUMP, "-mesh_file", os.path.join(d, "m.mesh"), "-dof_type", "P%d" % P,
+        e = kuhn_cube(m)[1]
+        args = [DUMP, *mesh_args(name, d), "-dof_type", "P%d" % P,
                 "-solver_rtol", repr(rtol), "-solver_btol", "0", "-solver_atol", "0",
                 "-solver_maxit", "10000", "-map_reorder", "no", "-dump_dir", d, "-rhs_case", case,
                 "-gpu_solver", gpu_solver, "-gmres_restart", str(GMRES_RESTART), *extra]
