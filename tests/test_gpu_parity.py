@@ -237,10 +237,12 @@ def test_nonfinite_input_reported(gpu):
         assert ei.value.code == -6, kw.keys()
     v = G["verts"].copy(); v[2, 1] = np.nan
     s.set_mesh(v, G["elems"])
+    s.set_dof_map(2, G["e2l"], G["bdry"])
     with pytest.raises(gpu.PhgGpuError) as ei:
         s.build_linear_system(f=G["f"])
     assert ei.value.code == -6
     s.set_mesh(G["verts"], G["elems"])
+    s.set_dof_map(2, G["e2l"], G["bdry"])
     s.build_linear_system(f=G["f"])
     assert np.array_equal(s.get_rhs(), G["rhs"])
     r = G["rhs"].copy(); r[1] = np.nan
