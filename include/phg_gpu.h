@@ -120,6 +120,22 @@ int phgGpuElementMatrices(phgGpuSystem *sys, const double *kappa,
 int phgGpuSetMatrix(phgGpuSystem *sys, int64_t n, const int64_t *ptr,
 		    const int32_t *cols, const double *vals, const double *rhs);
 
+/* Rows from recorded row segments, the way phgMatAddEntries_ builds them
+ * (src/matvec.c:5348-5493 -> add_columns_to_row :3045-3332): segment r adds
+ * the values rec_vals[rec_ptr[r] .. rec_ptr[r + 1]) at columns rec_cols[..]
+ * to row rec_row[r] (0 <= row < n), segments applied in their order; exact
+ * zeros and negative columns are skipped, a column's first appearance fixes
+ * its place in the row, later ones add to it.  The result -- PHG's rows
+ * before phgMatAssemble -- becomes the system's matrix (phgGpuGetMatrix
+ * returns it; the right-hand side is zero).  rec_ptr is int64 (nrec + 1,
+ * rec_ptr[0] = 0).  A row whose first non-empty segment names a column twice
+ * (which the reference would keep twice) is PHG_GPU_ERR_ARG; rows longer
+ * than 1024 entries are PHG_GPU_ERR_LIMIT.  Serves the per-call shim of
+ * phgMatAddEntries_ (phg_b200/shim). */
+int phgGpuAssembleRows(phgGpuSystem *sys, int64_t n, int64_t nrec,
+		       const int32_t *rec_row, const int64_t *rec_ptr,
+		       const int32_t *rec_cols, const double *rec_vals);
+
 /* Replaces the right-hand side the solvers use (n values, boundary
  * elimination already applied) and keeps the matrix: a new phgSolverVecSolve
  * on the same matrix (src/solver.c:1131-1150) or a change of

@@ -33,6 +33,7 @@ SIGNATURES = {
     "phgGpuBuildLinearSystemMass": (C.c_int, [_P, _P, C.c_double, _P, _P]),
     "phgGpuSetMatrix": (C.c_int, [_P, _I64, _P, _P, _P, _P]),
     "phgGpuSetRHS": (C.c_int, [_P, _P]),
+    "phgGpuAssembleRows": (C.c_int, [_P, _I64, _I64, _P, _P, _P, _P]),
     "phgGpuGetSizes": (C.c_int, [_P, C.POINTER(_I64), C.POINTER(_I64), C.POINTER(_I64)]),
     "phgGpuGetMatrix": (C.c_int, [_P, _P, _P, _P]),
     "phgGpuGetBdryColumns": (C.c_int, [_P, _P, _P, _P]),
@@ -195,6 +196,14 @@ class Solver:
         ptr, cols = _np(ptr, np.int64), _np(cols, np.int32)
         vals, rhs = _np(vals, np.float64), _np(rhs, np.float64)
         _check(lib().phgGpuSetMatrix(self._h, len(ptr) - 1, _ptr(ptr), _ptr(cols), _ptr(vals), _ptr(rhs)))
+
+    def assemble_rows(self, n, rec_row, rec_ptr, rec_cols, rec_vals):
+        """Rows from row segments in call order, as phgMatAddEntries_ builds
+        them (zeros dropped, first-touch column order)."""
+        rec_row, rec_ptr = _np(rec_row, np.int32), _np(rec_ptr, np.int64)
+        rec_cols, rec_vals = _np(rec_cols, np.int32), _np(rec_vals, np.float64)
+        _check(lib().phgGpuAssembleRows(self._h, int(n), len(rec_row), _ptr(rec_row), _ptr(rec_ptr),
+                                        _ptr(rec_cols), _ptr(rec_vals)))
 
     def set_rhs(self, rhs):
         """Replaces the right-hand side of the assembled system (after

@@ -900,6 +900,141 @@ value_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32
     }
 }
 
+// ---------------------------------------------------------------------------
+// Rows from recorded phgMatAddEntries_ calls (src/matvec.c:5348-5493): each
+// record is one row segment (row, columns, values) in call order.  A lane
+// group of 32 takes a row and its records in call order; within a record the
+// entries are taken 32 at a time in their order.  As add_columns_to_row
+// (matvec.c:3045-3332, SORT_COLUMNS 0) does, exact zeros and negative
+// columns are skipped, a column's first appearance fixes its place and later
+// ones add to it.  The reference copies a row's first non-empty segment
+// verbatim, so a column repeated inside that segment would appear twice; the
+// kernel flags that case (PHGB_DEV_DUPLICATE) rather than reproducing it.
+template <int HS_, int MAXROW_, int WARPS_, bool LONG_>
+struct RecCfg {
+    static constexpr int HS = HS_, MAXROW = MAXROW_, WARPS = WARPS_;
+    static constexpr bool LONG = LONG_;
+};
+using RecShort = RecCfg<512, 256, 4, false>;
+using RecLong = RecCfg<2048, 1024, 1, true>;
+
+template <class C>
+__global__ void __launch_bounds__(C::WARPS * 32)
+record_walk_kernel(int64_t n, const int32_t *__restrict__ rinc_ptr, const int32_t *__restrict__ rinc,
+                   const int64_t *__restrict__ rec_ptr, const int32_t *__restrict__ rec_cols,
+                   const double *__restrict__ rec_vals, const int32_t *__restrict__ cap_ptr,
+                   int32_t *__restrict__ cnt, int32_t *__restrict__ sc_cols, double *__restrict__ sc_vals,
+                   int *status, int32_t *__restrict__ over_list, int *nover) {
+    constexpr int HS = C::HS, MAXROW = C::MAXROW, W = C::WARPS;
+    __shared__ int32_t s_key[W][HS];
+    __shared__ int16_t s_pos[W][HS];
+    __shared__ int32_t s_col[W][MAXROW];
+    __shared__ double s_val[W][MAXROW];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    int32_t *key = s_key[w];
+    int16_t *hpos = s_pos[w];
+    int32_t *scol = s_col[w];
+    double *sval = s_val[w];
+    const int64_t nwarps = (int64_t)gridDim.x * W;
+    const int64_t nrows = C::LONG ? (int64_t)*nover : n;
+    for (int64_t k = (int64_t)blockIdx.x * W + w; k < nrows; k += nwarps) {
+        const int64_t d = C::LONG ? (int64_t)over_list[k] : k;
+        const int32_t r0 = rinc_ptr[d], r1 = rinc_ptr[d + 1];
+        for (int t = lane; t < HS; t += 32) key[t] = -1;
+        __syncwarp();
+        int L = 0;
+        bool overflow = false, dup = false;
+        for (int ri = r0; ri < r1; ri++) {
+            const int32_t rec = rinc[ri];
+            const int64_t e0 = rec_ptr[rec], e1 = rec_ptr[rec + 1];
+            const bool fresh = L == 0;   // the row's first non-empty segment
+            for (int64_t b = e0; b < e1; b += 32) {
+                const int64_t j = b + lane;
+                int32_t col = -1;
+                double v = 0.0;
+                if (j < e1) {
+                    col = rec_cols[j];
+                    v = rec_vals[j];
+                }
+                const bool nz = j < e1 && col >= 0 && v != 0.0;
+                int pos = -1;
+                if (nz) {
+                    unsigned h = hash32(col) & (HS - 1);
+                    for (int probe = 0; probe < HS; probe++) {
+                        const int32_t kk = key[h];
+                        if (kk == col) { pos = hpos[h]; break; }
+                        if (kk == -1) break;
+                        h = (h + 1) & (HS - 1);
+                    }
+                    if (pos >= 0 && fresh) dup = true;
+                }
+                const unsigned newm = __ballot_sync(0xffffffffu, nz && pos < 0);
+                if (nz && pos < 0) {
+                    pos = L + __popc(newm & lt_mask);
+                    if (pos < MAXROW) {
+                        unsigned h = hash32(col) & (HS - 1);
+                        for (int probe = 0; probe < HS; probe++) {
+                            const int32_t old = atomicCAS(&key[h], -1, col);
+                            if (old == -1) { hpos[h] = (int16_t)pos; break; }
+                            if (old == col) { dup = true; break; }   // the same column twice in one chunk
+                            h = (h + 1) & (HS - 1);
+                        }
+                        scol[pos] = col;
+                        sval[pos] = v;
+                    } else {
+                        overflow = true;
+                    }
+                } else if (nz) {
+                    sval[pos] = rn_add(sval[pos], v);
+                }
+                L += __popc(newm);
+                __syncwarp();
+            }
+        }
+        const bool bad = __any_sync(0xffffffffu, overflow) || L > MAXROW;
+        if (__any_sync(0xffffffffu, dup) && lane == 0) atomicExch(status, PHGB_DEV_DUPLICATE);
+        if (bad) {
+            if (lane == 0) {
+                if (C::LONG) atomicExch(status, PHGB_DEV_ROW_OVERFLOW);
+                else over_list[atomicAdd(nover, 1)] = (int32_t)d;
+            }
+        } else {
+            const int64_t base = cap_ptr[d];
+            for (int t = lane; t < L; t += 32) {
+                sc_cols[base + t] = scol[t];
+                sc_vals[base + t] = sval[t];
+            }
+            if (lane == 0) cnt[d] = L;
+        }
+        __syncwarp();
+    }
+}
+
+// Record lengths per row, for the rows' scratch capacities.
+__global__ void record_len_kernel(int64_t nrec, const int32_t *__restrict__ rec_row, const int64_t *__restrict__ rec_ptr,
+                                  int32_t *__restrict__ cap) {
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nrec; r += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(&cap[rec_row[r]], (int32_t)(rec_ptr[r + 1] - rec_ptr[r]));
+}
+
+// Copies each row's scratch entries (at cap_ptr) to the CSR at ptr.
+__global__ void __launch_bounds__(256)
+record_compact_kernel(int64_t n, const int32_t *__restrict__ cap_ptr, const int32_t *__restrict__ sc_cols,
+                      const double *__restrict__ sc_vals, const int32_t *__restrict__ ptr, int32_t *__restrict__ cols,
+                      double *__restrict__ vals) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t d = warp; d < n; d += nwarps) {
+        const int32_t src = cap_ptr[d], p0 = ptr[d], len = ptr[d + 1] - p0;
+        for (int j = lane; j < len; j += 32) {
+            cols[p0 + j] = sc_cols[src + j];
+            vals[p0 + j] = sc_vals[src + j];
+        }
+    }
+}
+
 // Copies every row's scratch region into the CSR arrays: kept entries to
 // ptr[d].., saved boundary columns (stored reversed at the region's end) to
 // bptr[d]...  One warp per row.
@@ -1019,6 +1154,31 @@ static cudaError_t value_walk(const WalkArgs &A, cudaStream_t s) {
     value_walk_kernel<N, LongWalkCfg<N>><<<148 * 4, 32, 0, s>>>(
         A.ndof, A.inc_ptr, A.inc, A.bdry, A.Ke, A.Re, A.g, A.slot, A.tmap, A.ptr, A.cols, A.bptr, A.bcols, A.vals,
         A.bvals, A.rhs, A.diag, A.status, A.over_list, A.nover);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_record_lengths(int64_t nrec, const int32_t *rec_row, const int64_t *rec_ptr, int32_t *cap,
+                                  cudaStream_t s) {
+    record_len_kernel<<<grid_for(nrec, 256, 148 * 16), 256, 0, s>>>(nrec, rec_row, rec_ptr, cap);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_record_walk(const RecordArgs &A, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(A.nover, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    record_walk_kernel<RecShort><<<grid_for(A.n, RecShort::WARPS, 148 * 16), RecShort::WARPS * 32, 0, s>>>(
+        A.n, A.rinc_ptr, A.rinc, A.rec_ptr, A.rec_cols, A.rec_vals, A.cap_ptr, A.cnt, A.sc_cols, A.sc_vals,
+        A.status, A.over_list, A.nover);
+    record_walk_kernel<RecLong><<<148 * 4, 32, 0, s>>>(A.n, A.rinc_ptr, A.rinc, A.rec_ptr, A.rec_cols, A.rec_vals,
+                                                      A.cap_ptr, A.cnt, A.sc_cols, A.sc_vals, A.status,
+                                                      A.over_list, A.nover);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_record_compact(const RecordArgs &A, const int32_t *ptr, int32_t *cols, double *vals,
+                                  cudaStream_t s) {
+    record_compact_kernel<<<grid_for(A.n * 32, 256, 148 * 16), 256, 0, s>>>(A.n, A.cap_ptr, A.sc_cols, A.sc_vals,
+                                                                          ptr, cols, vals);
     return cudaGetLastError();
 }
 

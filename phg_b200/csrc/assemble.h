@@ -66,6 +66,29 @@ cudaError_t launch_value_walk(int p, const WalkArgs &a, cudaStream_t s);
 // Longest row the walk assembles (its second pass); longer rows are
 // PHG_GPU_ERR_LIMIT.
 int row_walk_max_row(int p);
+
+// Rows from recorded row segments (phgMatAddEntries_ calls), in call order.
+struct RecordArgs {
+    int64_t n;                                // rows
+    const int32_t *rinc_ptr, *rinc;           // per row, its records in call order
+    const int64_t *rec_ptr;                   // entries of record r: [rec_ptr[r], rec_ptr[r + 1])
+    const int32_t *rec_cols;
+    const double *rec_vals;
+    const int32_t *cap_ptr;                   // scratch offset of each row (its entries' total)
+    int32_t *cnt;                             // entries of each row
+    int32_t *sc_cols;
+    double *sc_vals;
+    int *status;
+    int32_t *over_list;                       // rows over 256 entries, for the second pass
+    int *nover;
+};
+// Longest row the record walk assembles.
+constexpr int kRecordMaxRow = 1024;
+cudaError_t launch_record_lengths(int64_t nrec, const int32_t *rec_row, const int64_t *rec_ptr, int32_t *cap,
+                                  cudaStream_t s);
+cudaError_t launch_record_walk(const RecordArgs &a, cudaStream_t s);
+cudaError_t launch_record_compact(const RecordArgs &a, const int32_t *ptr, int32_t *cols, double *vals,
+                                  cudaStream_t s);
 int64_t geometry_doubles(int64_t nelem);
 
 }  // namespace phgb

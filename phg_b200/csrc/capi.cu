@@ -184,6 +184,10 @@ struct phgGpuSystem_ {
     // next records the pattern), 2 recorded (builds use the value walk)
     int pattern_state = 0;
     DevBuf<uint16_t> slot, tmap;
+    // rows assembled from recorded row segments (phgGpuAssembleRows)
+    DevBuf<int32_t> rec_row, rec_cols, rec_inc_ptr, rec_inc, rec_cnt, rec_cursor, rec_cap, rec_cap_ptr;
+    DevBuf<int64_t> rec_ptr;
+    DevBuf<double> rec_vals;
 
     // assembled system
     int64_t n = 0, nnz = 0, bnnz = 0;
@@ -1080,6 +1084,93 @@ int phgGpuSetRHS(phgGpuSystem *s, const double *rhs) {
     CK(cudaGetLastError());
     s->launches += 1;
     return check_status(s, "phgGpuSetRHS");
+}
+
+int phgGpuAssembleRows(phgGpuSystem *s, int64_t n, int64_t nrec, const int32_t *rec_row, const int64_t *rec_ptr,
+                       const int32_t *rec_cols, const double *rec_vals) {
+    if (s == nullptr || n <= 0 || nrec < 0 || (nrec > 0 && (rec_row == nullptr || rec_ptr == nullptr)))
+        return fail(PHG_GPU_ERR_ARG, "phgGpuAssembleRows: invalid arguments");
+    if (n >= INT32_MAX || nrec >= INT32_MAX) return fail(PHG_GPU_ERR_LIMIT, "phgGpuAssembleRows: too many rows");
+    CHECK_RC(set_device(s));
+    int64_t nent = 0;
+    if (nrec > 0) {
+        int64_t first = 0;
+        CK(cudaMemcpy(&nent, rec_ptr + nrec, sizeof(int64_t), cudaMemcpyDefault));
+        CK(cudaMemcpy(&first, rec_ptr, sizeof(int64_t), cudaMemcpyDefault));
+        if (first != 0 || nent < 0) return fail(PHG_GPU_ERR_ARG, "phgGpuAssembleRows: bad segment offsets");
+        if (nent >= INT32_MAX) return fail(PHG_GPU_ERR_LIMIT, "phgGpuAssembleRows: more than 2^31 entries");
+        if (nent > 0 && (rec_cols == nullptr || rec_vals == nullptr))
+            return fail(PHG_GPU_ERR_ARG, "phgGpuAssembleRows: invalid arguments");
+    }
+    const size_t un = (size_t)n;
+    const int32_t *drow = nullptr, *dcols = nullptr;
+    const int64_t *dptr = nullptr;
+    const double *dvals = nullptr;
+    CHECK_RC(stage(s, rec_row, (size_t)nrec, s->rec_row, &drow));
+    CHECK_RC(stage(s, rec_ptr, (size_t)nrec + 1, s->rec_ptr, &dptr));
+    CHECK_RC(stage(s, rec_cols, (size_t)nent, s->rec_cols, &dcols));
+    CHECK_RC(stage(s, rec_vals, (size_t)nent, s->rec_vals, &dvals));
+    CHECK_RC(s->rec_inc_ptr.ensure(un + 1));
+    CHECK_RC(s->rec_inc.ensure((size_t)nrec));
+    CHECK_RC(s->rec_cnt.ensure(un));
+    CHECK_RC(s->rec_cursor.ensure(un));
+    CHECK_RC(s->rec_cap.ensure(un));
+    CHECK_RC(s->rec_cap_ptr.ensure(un + 1));
+    CHECK_RC(s->scan_ws.ensure((size_t)scan_workspace_elems(n)));
+    CHECK_RC(s->sc_cols.ensure((size_t)nent));
+    CHECK_RC(s->sc_vals.ensure((size_t)nent));
+    CHECK_RC(s->over_list.ensure(un));
+    CHECK_RC(s->nover.ensure(1));
+    CHECK_RC(s->rp.ensure(un + 1));
+    CHECK_RC(s->rhs.ensure(un));
+    CHECK_RC(s->diag.ensure(un));
+    // each row's segments in call order (the incidence lists with one
+    // "basis" per segment), and each row's capacity (its segments' total)
+    CK(launch_incidence(1, nrec, n, drow, s->rec_cnt.p, s->rec_inc_ptr.p, s->rec_cursor.p, s->rec_inc.p,
+                        s->scan_ws.p, s->status.p, s->stream));
+    CK(cudaMemsetAsync(s->rec_cap.p, 0, sizeof(int32_t) * un, s->stream));
+    if (nrec > 0) CK(launch_record_lengths(nrec, drow, dptr, s->rec_cap.p, s->stream));
+    CK(launch_scan(n, s->rec_cap.p, s->rec_cap_ptr.p, s->scan_ws.p, s->stream));
+    CHECK_RC(check_status(s, "phgGpuAssembleRows (segments)"));
+    RecordArgs ra{};
+    ra.n = n; ra.rinc_ptr = s->rec_inc_ptr.p; ra.rinc = s->rec_inc.p; ra.rec_ptr = dptr; ra.rec_cols = dcols;
+    ra.rec_vals = dvals; ra.cap_ptr = s->rec_cap_ptr.p; ra.cnt = s->rec_cnt.p; ra.sc_cols = s->sc_cols.p;
+    ra.sc_vals = s->sc_vals.p; ra.status = s->status.p; ra.over_list = s->over_list.p; ra.nover = s->nover.p;
+    CK(launch_record_walk(ra, s->stream));
+    CK(launch_scan(n, s->rec_cnt.p, s->rp.p, s->scan_ws.p, s->stream));
+    int32_t tot = 0;
+    CK(cudaMemcpyAsync(&tot, s->rp.p + n, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaMemcpyAsync(s->h_status, s->status.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    s->launches += 12;
+    const int st = *s->h_status;
+    if (st != PHGB_DEV_OK) {
+        *s->h_status = 0;
+        CK(cudaMemsetAsync(s->status.p, 0, sizeof(int), s->stream));
+        s->assembled = false;
+        if (st == PHGB_DEV_DUPLICATE)
+            return fail(PHG_GPU_ERR_ARG, "phgGpuAssembleRows: a row's first segment names a column twice");
+        if (st == PHGB_DEV_ROW_OVERFLOW)
+            return fail(PHG_GPU_ERR_LIMIT, "phgGpuAssembleRows: a row has more than %d entries", kRecordMaxRow);
+        return fail(PHG_GPU_ERR_STATE, "phgGpuAssembleRows: internal consistency check failed (%d)", st);
+    }
+    s->nnz = tot;
+    s->bnnz = 0;
+    CHECK_RC(s->ci.ensure((size_t)s->nnz));
+    CHECK_RC(s->va.ensure((size_t)s->nnz));
+    CK(launch_record_compact(ra, s->rp.p, s->ci.p, s->va.p, s->stream));
+    CK(cudaMemsetAsync(s->rhs.p, 0, sizeof(double) * un, s->stream));
+    diag_kernel<<<vec_blocks(n), 256, 0, s->stream>>>(n, s->rp.p, s->ci.p, s->va.p, s->diag.p);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s->stream));
+    s->launches += 2;
+    s->n = n;
+    s->pattern_state = 0;
+    s->assembled = true;
+    s->have_bdry_cols = false;
+    invalidate_layouts(s);
+    s->lpr = spmv_lanes_for((double)s->nnz / (double)n);
+    return PHG_GPU_OK;
 }
 
 int phgGpuGetSizes(phgGpuSystem *s, int64_t *n, int64_t *nnz, int64_t *nnz_bdry) {

@@ -14,7 +14,8 @@ enum {
     PHGB_DEV_BAD_INDEX = 2,      // a DOF / vertex index out of range
     PHGB_DEV_COUNT_MISMATCH = 3, // two passes of the row walk disagreed
     PHGB_DEV_NONFINITE = 4,      // a coordinate, kappa, f or g value is NaN or infinite
-    PHGB_DEV_PATTERN_CHANGED = 5 // a rebuild found an exact zero where the pattern had none, or the reverse
+    PHGB_DEV_PATTERN_CHANGED = 5,// a rebuild found an exact zero where the pattern had none, or the reverse
+    PHGB_DEV_DUPLICATE = 6       // a row's first segment names a column twice
 };
 
 // IEEE round-to-nearest double arithmetic with no contraction into fused
