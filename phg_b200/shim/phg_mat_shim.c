@@ -125,7 +125,7 @@ static int eligible(MAT *mat, BOOLEAN rows_global, BOOLEAN cols_global, BOOLEAN 
     return 0;
 #else
     return !replace && !cols_global && !rows_global && mat->mode != PHG_REPLACE &&
-           mat->type != PHG_MATRIX_FREE && !mat->assembled && mat->rmap->nprocs == 1 &&
+           mat->type != PHG_MATRIX_FREE && mat->blocks == NULL && !mat->assembled && mat->rmap->nprocs == 1 &&
            mat->cmap->nprocs == 1 && mat->rmap->L2Vmap == NULL && mat->cmap->L2Vmap == NULL &&
            mat->rmap->localsize == mat->rmap->nlocal && mat->cmap->localsize == mat->cmap->nlocal;
 #endif
