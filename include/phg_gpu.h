@@ -68,6 +68,16 @@ int phgGpuSetStream(phgGpuSystem *sys, void *stream);
 int phgGpuSetMesh(phgGpuSystem *sys, int64_t nvert, const double *verts,
 		  int64_t nelem, const int32_t *elem_verts);
 
+/* PHG's stored element geometry, used instead of the one computed from the
+ * coordinates until the next phgGpuSetMesh: geo[17 * e + 0..15] is the
+ * element's Jacobian (phgGeomGetJacobian, src/geom.c:855-884; row c holds
+ * the gradient of barycentric c, then its constant term) and geo[17 * e + 16]
+ * its volume (phgGeomGetVolume, src/geom.c:809).  On elements PHG made by
+ * bisection these are interpolated from the parent (src/geom.c:460-565) and
+ * differ from the coordinates' in the last bits; the assembled rows follow
+ * PHG's values.  Non-finite values are PHG_GPU_ERR_ARG. */
+int phgGpuSetGeometry(phgGpuSystem *sys, int64_t nelem, const double *geo);
+
 /* The DOF layout of a scalar Lagrange P`order` space (order 1, 2 or 3):
  * e2l[e * nbas + k] = vector index of element basis k (phgSolverMapE2L,
  * include/phg/solver.h:297 -> phgDofMapE2D_, src/dof.c:4821-4881), and

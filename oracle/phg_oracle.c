@@ -330,20 +330,19 @@ basis_gradients(int p, const double *J, int np, const double *pts,
     }
 }
 
-void
-pho_elem_stiffness(int p, const double *x, double kappa, double *A)
-/* The reference user loop (examples/poisson.c:126-139) calls
- * phgQuadGradBasAGradBas(e, u, j, A, u, i, QUAD_DEFAULT) for j <= i
- * (quad.c:5260-5344): order (p-1)+(p-1) (+0 for a P0 coefficient),
- * d = sum_q (0 + g_j.g_i) * w_q [* kappa], times the volume. */
+/* The element integrals from the element's geometry (J, volume): PHG
+ * computes them from the coordinates (compute_jacobian, geom.c:103-169) on
+ * elements it imported and interpolates them from the parent on elements
+ * bisection made (geom.c:460-565); either way phgQuad* read the stored
+ * values (phgGeomGetJacobian_, geom.c:855-884). */
+static void
+elem_stiffness_geo(int p, const double *J, double vol, double kappa, double *A)
 {
     int n = pho_nbas(p), np, a, b, q, order = 2 * (p - 1);
     const double *pts, *w;
-    double J[16], vol, grad[20 * MAXQP * 3];
+    double grad[20 * MAXQP * 3];
 
     np = pho_quad_rule(order, &pts, &w);
-    pho_jacobian(x, J);
-    vol = pho_volume(x);
     basis_gradients(p, J, np, pts, grad);
     for (a = 0; a < n; a++)
 	for (b = 0; b <= a; b++) {
@@ -363,16 +362,25 @@ pho_elem_stiffness(int p, const double *x, double kappa, double *A)
 }
 
 void
-pho_elem_mass(int p, const double *x, double *M)
-/* phgQuadBasABas with A = NULL (quad.c:5582-5625): order p+p,
- * d = sum_q (0 + phi_j phi_i) * w_q, times the volume. */
+pho_elem_stiffness(int p, const double *x, double kappa, double *A)
+/* The reference user loop (examples/poisson.c:126-139) calls
+ * phgQuadGradBasAGradBas(e, u, j, A, u, i, QUAD_DEFAULT) for j <= i
+ * (quad.c:5260-5344): order (p-1)+(p-1) (+0 for a P0 coefficient),
+ * d = sum_q (0 + g_j.g_i) * w_q [* kappa], times the volume. */
+{
+    double J[16];
+    pho_jacobian(x, J);
+    elem_stiffness_geo(p, J, pho_volume(x), kappa, A);
+}
+
+static void
+elem_mass_vol(int p, double vol, double *M)
 {
     int n = pho_nbas(p), np, a, b, q;
     const double *pts, *w;
-    double vol, bas[MAXQP][20];
+    double bas[MAXQP][20];
 
     np = pho_quad_rule(2 * p, &pts, &w);
-    vol = pho_volume(x);
     for (q = 0; q < np; q++)
 	pho_bas(p, pts + 4 * q, bas[q]);
     for (a = 0; a < n; a++)
@@ -388,18 +396,21 @@ pho_elem_mass(int p, const double *x, double *M)
 }
 
 void
-pho_elem_rhs(int p, const double *x, const double *f_local, double *res)
-/* phgQuadDofTimesBas(e, f_h, u_h, i, QUAD_DEFAULT) (quad.c:5481-5530):
- * order p+p; f at the points by phgDofEval_ (dof-utils.c:100-300), i.e.
- * 0 + phi_0 f_0 + phi_1 f_1 + ... in basis order; then
- * d = sum_q phi_i * w_q * f_q, times the volume. */
+pho_elem_mass(int p, const double *x, double *M)
+/* phgQuadBasABas with A = NULL (quad.c:5582-5625): order p+p,
+ * d = sum_q (0 + phi_j phi_i) * w_q, times the volume. */
+{
+    elem_mass_vol(p, pho_volume(x), M);
+}
+
+static void
+elem_rhs_vol(int p, double vol, const double *f_local, double *res)
 {
     int n = pho_nbas(p), np, a, q, k;
     const double *pts, *w;
-    double vol, bas[MAXQP][20], fq[MAXQP];
+    double bas[MAXQP][20], fq[MAXQP];
 
     np = pho_quad_rule(2 * p, &pts, &w);
-    vol = pho_volume(x);
     for (q = 0; q < np; q++) {
 	double v = 0.0;
 	pho_bas(p, pts + 4 * q, bas[q]);
@@ -413,6 +424,16 @@ pho_elem_rhs(int p, const double *x, const double *f_local, double *res)
 	    d += bas[q][a] * w[q] * fq[q];
 	res[a] = d * vol;
     }
+}
+
+void
+pho_elem_rhs(int p, const double *x, const double *f_local, double *res)
+/* phgQuadDofTimesBas(e, f_h, u_h, i, QUAD_DEFAULT) (quad.c:5481-5530):
+ * order p+p; f at the points by phgDofEval_ (dof-utils.c:100-300), i.e.
+ * 0 + phi_0 f_0 + phi_1 f_1 + ... in basis order; then
+ * d = sum_q phi_i * w_q * f_q, times the volume. */
+{
+    elem_rhs_vol(p, pho_volume(x), f_local, res);
 }
 
 /*------------------------------ assembly ---------------------------------*/
@@ -461,7 +482,8 @@ int
 pho_assemble(int p, int64_t nvert, const double *verts, int64_t nelem,
 	     const int32_t *elems, const int32_t *e2l, int64_t ndof,
 	     const uint8_t *bdry, const double *f, const double *g,
-	     const double *kappa, double mass_coef, pho_system *S)
+	     const double *kappa, double mass_coef, const double *geom,
+	     pho_system *S)
 {
     int N = pho_nbas(p), a, b;
     int64_t e, i, j;
@@ -489,14 +511,25 @@ pho_assemble(int p, int64_t nvert, const double *verts, int64_t nelem,
 		return -3;
 	    fl[a] = f != NULL ? f[I[a]] : 0.0;
 	}
-	pho_elem_stiffness(p, x, kappa != NULL ? kappa[e] : -1.0, A);
-	/* stiffness + c * mass (examples/simplest.c:68-72) */
-	if (mass_coef != 0.0) {
-	    pho_elem_mass(p, x, M);
-	    for (a = 0; a < N * N; a++)
-		A[a] = A[a] + mass_coef * M[a];
+	{   /* the element's geometry: PHG's stored values when given */
+	    double J[16], vol;
+	    if (geom != NULL) {
+		memcpy(J, geom + 17 * e, 16 * sizeof(double));
+		vol = geom[17 * e + 16];
+	    }
+	    else {
+		pho_jacobian(x, J);
+		vol = pho_volume(x);
+	    }
+	    elem_stiffness_geo(p, J, vol, kappa != NULL ? kappa[e] : -1.0, A);
+	    /* stiffness + c * mass (examples/simplest.c:68-72) */
+	    if (mass_coef != 0.0) {
+		elem_mass_vol(p, vol, M);
+		for (a = 0; a < N * N; a++)
+		    A[a] = A[a] + mass_coef * M[a];
+	    }
+	    elem_rhs_vol(p, vol, fl, R);
 	}
-	pho_elem_rhs(p, x, fl, R);
 	for (a = 0; a < N; a++) {
 	    if (bdry[I[a]]) {
 		/* phgDofDirichletBC nodal path (dof-utils.c:1369-1392):

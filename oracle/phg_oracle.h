@@ -79,7 +79,8 @@ typedef struct {
 int pho_assemble(int p, int64_t nvert, const double *verts, int64_t nelem,
 		 const int32_t *elems, const int32_t *e2l, int64_t ndof,
 		 const uint8_t *bdry, const double *f, const double *g,
-		 const double *kappa, double mass_coef, pho_system *sys);
+		 const double *kappa, double mass_coef, const double *geom,
+		 pho_system *sys);
 void pho_system_free(pho_system *sys);
 
 /* y = A x for the CSR (ptr int64) (matvec.c:891-928). */

@@ -29,7 +29,7 @@ def lib():
         L.pho_elem_mass.argtypes = [C.c_int, P, P]
         L.pho_elem_rhs.argtypes = [C.c_int, P, P, P]
         L.pho_assemble.argtypes = [C.c_int, C.c_int64, P, C.c_int64, P, P,
-                                   C.c_int64, P, P, P, P, C.c_double, P]
+                                   C.c_int64, P, P, P, P, C.c_double, P, P]
         L.pho_assemble.restype = C.c_int
         L.pho_system_free.argtypes = [P]
         L.pho_spmv.argtypes = [C.c_int64, P, P, P, P, P]
@@ -103,9 +103,12 @@ def elem_mass(p, x):
     return M
 
 
-def assemble(p, verts, elems, e2l, bdry, f, g=None, kappa=None, mass=0.0):
+def assemble(p, verts, elems, e2l, bdry, f, g=None, kappa=None, mass=0.0, geom=None):
     """Returns a dict of numpy arrays (see pho_system in phg_oracle.h).
-    mass != 0 adds mass * (element mass matrix) to each element matrix."""
+    mass != 0 adds mass * (element mass matrix) to each element matrix.
+    geom (nelem x 17: Jacobian, volume) is the element geometry PHG stores;
+    None computes it from the coordinates (what PHG does on elements it did
+    not make by bisection)."""
     verts = np.ascontiguousarray(verts, np.float64)
     elems = np.ascontiguousarray(elems, np.int32)
     e2l = np.ascontiguousarray(e2l, np.int32)
@@ -113,11 +116,12 @@ def assemble(p, verts, elems, e2l, bdry, f, g=None, kappa=None, mass=0.0):
     f = np.ascontiguousarray(f, np.float64)
     g = None if g is None else np.ascontiguousarray(g, np.float64)
     kappa = None if kappa is None else np.ascontiguousarray(kappa, np.float64)
+    geom = None if geom is None else np.ascontiguousarray(geom, np.float64)
     ndof = len(bdry)
     S = _System()
     rc = lib().pho_assemble(p, len(verts), _ptr(verts), len(elems),
                             _ptr(elems), _ptr(e2l), ndof, _ptr(bdry), _ptr(f),
-                            _ptr(g), _ptr(kappa), C.c_double(mass), C.byref(S))
+                            _ptr(g), _ptr(kappa), C.c_double(mass), _ptr(geom), C.byref(S))
     if rc != 0:
         raise ValueError("pho_assemble failed: %d" % rc)
     n = S.n

@@ -307,6 +307,18 @@ main(int argc, char *argv[])
 	    write_bin("diag.f64", solver->mat->diag, sizeof(FLOAT), ndof);
 	    write_bin("verts.f64", g->verts, sizeof(FLOAT), 3 * g->nvert);
 	    write_bin("elems.i32", elems, sizeof(INT), NVert * g->nelem);
+	    {	/* PHG's element geometry (J, 16 values, then the volume):
+		 * on refined meshes it is interpolated from the parents
+		 * (geom.c:460-565), not computed from the coordinates */
+		FLOAT *geo = phgAlloc(17 * (size_t)g->nelem * sizeof(*geo));
+		ForAllElements(g, e) {
+		    memcpy(geo + 17 * (size_t)e->index, phgGeomGetJacobian(g, e),
+			   16 * sizeof(FLOAT));
+		    geo[17 * (size_t)e->index + 16] = phgGeomGetVolume(g, e);
+		}
+		write_bin("geom.f64", geo, sizeof(FLOAT), 17 * (size_t)g->nelem);
+		phgFree(geo);
+	    }
 	    write_bin("e2l.i32", e2l, sizeof(INT), nbas * g->nelem);
 	    write_bin("order.i32", order, sizeof(INT), g->nelem);
 	    write_bin("f.f64", f_h->data, sizeof(FLOAT), ndof);

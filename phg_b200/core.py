@@ -28,6 +28,7 @@ SIGNATURES = {
     "phgGpuDestroy": (C.c_int, [_P]),
     "phgGpuSetStream": (C.c_int, [_P, _P]),
     "phgGpuSetMesh": (C.c_int, [_P, _I64, _P, _I64, _P]),
+    "phgGpuSetGeometry": (C.c_int, [_P, _I64, _P]),
     "phgGpuSetDofMap": (C.c_int, [_P, C.c_int, _I64, _P, _P]),
     "phgGpuBuildLinearSystem": (C.c_int, [_P, _P, _P, _P]),
     "phgGpuBuildLinearSystemMass": (C.c_int, [_P, _P, C.c_double, _P, _P]),
@@ -167,6 +168,15 @@ class Solver:
         verts, elems = _np(verts, np.float64), _np(elems, np.int32)
         self.nelem = len(elems)
         _check(lib().phgGpuSetMesh(self._h, len(verts), _ptr(verts), len(elems), _ptr(elems)))
+
+    def set_geometry(self, geo):
+        """PHG's stored element geometry (nelem x 17: Jacobian, volume), used
+        instead of the coordinates' until the next set_mesh; on elements PHG
+        made by bisection it is interpolated from the parent."""
+        geo = _np(geo, np.float64)
+        if geo.ndim != 2 or geo.shape[1] != 17:
+            raise ValueError("geometry must be nelem x 17")
+        _check(lib().phgGpuSetGeometry(self._h, len(geo), _ptr(geo)))
 
     def set_dof_map(self, order, e2l, bdry):
         e2l, bdry = _np(e2l, np.int32), _np(bdry, np.uint8)

@@ -1073,8 +1073,9 @@ static int grid_for(int64_t work, int per_block, int max_blocks) {
 template <int P>
 static void elem_launch(const ElemArgs &A, cudaStream_t s) {
     constexpr int W = ElemDims<P>::WARPS;
-    geometry_kernel<<<grid_for(A.nelem, 128, 148 * 64), 128, 0, s>>>(A.nelem, A.nvert, A.verts, A.elems, A.geo,
-                                                                    A.status);
+    if (!A.geometry_given)
+        geometry_kernel<<<grid_for(A.nelem, 128, 148 * 64), 128, 0, s>>>(A.nelem, A.nvert, A.verts, A.elems,
+                                                                        A.geo, A.status);
     ElemWeights Wt{};
     for (int q = 0; q < ElemDims<P>::QK; q++) Wt.wk[q] = A.wk_host[q];
     for (int q = 0; q < ElemDims<P>::QR; q++) Wt.wr[q] = A.wr_host[q];
@@ -1098,6 +1099,7 @@ cudaError_t launch_element_kernel(int p, const ElemArgs &A, cudaStream_t s) {
 }
 
 int64_t geometry_doubles(int64_t nelem) { return nelem * kGeo; }
+int geometry_stride() { return kGeo; }
 
 
 cudaError_t launch_incidence(int N, int64_t nelem, int64_t ndof, const int32_t *e2l, int32_t *cnt,

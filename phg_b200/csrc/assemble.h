@@ -21,7 +21,8 @@ struct ElemArgs {
     // brt the same transposed (brt[k * QR + q])
     const double *gk, *br, *brt;
     const double *wk_host, *wr_host;         // quadrature weights (host; passed by value)
-    double *geo;                             // scratch: nelem * geometry_doubles
+    double *geo;                             // nelem * geometry_doubles: J (16), volume per element
+    bool geometry_given;                     // geo holds the caller's geometry (else computed here)
     double *Ke, *Re;
     int *status;
 };
@@ -90,5 +91,6 @@ cudaError_t launch_record_walk(const RecordArgs &a, cudaStream_t s);
 cudaError_t launch_record_compact(const RecordArgs &a, const int32_t *ptr, int32_t *cols, double *vals,
                                   cudaStream_t s);
 int64_t geometry_doubles(int64_t nelem);
+int geometry_stride();                       // doubles per element in geo
 
 }  // namespace phgb

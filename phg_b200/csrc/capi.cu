@@ -157,6 +157,7 @@ struct phgGpuSystem_ {
     DevBuf<double> verts;
     DevBuf<int32_t> elems;
     bool have_mesh = false;
+    bool geometry_given = false;           // s->geo holds PHG's geometry (phgGpuSetGeometry)
 
     // DOF layout
     int order = 0, N = 0;
@@ -866,7 +867,28 @@ int phgGpuSetMesh(phgGpuSystem *s, int64_t nvert, const double *verts, int64_t n
     s->nelem = nelem;
     s->pattern_state = 0;
     s->have_mesh = true;
+    s->geometry_given = false;
     s->have_dofs = false;
+    s->assembled = false;
+    return PHG_GPU_OK;
+}
+
+int phgGpuSetGeometry(phgGpuSystem *s, int64_t nelem, const double *geo) {
+    if (s == nullptr || geo == nullptr) return fail(PHG_GPU_ERR_ARG, "phgGpuSetGeometry: invalid arguments");
+    if (!s->have_mesh) return fail(PHG_GPU_ERR_STATE, "phgGpuSetGeometry: call phgGpuSetMesh first");
+    if (nelem != s->nelem) return fail(PHG_GPU_ERR_ARG, "phgGpuSetGeometry: %lld elements, the mesh has %lld",
+                                       (long long)nelem, (long long)s->nelem);
+    for (size_t i = 0; i < 17 * (size_t)nelem; i++)
+        if (!isfinite(geo[i])) return fail(PHG_GPU_ERR_ARG, "phgGpuSetGeometry: element %lld not finite",
+                                           (long long)(i / 17));
+    CHECK_RC(set_device(s));
+    CHECK_RC(s->geo.ensure((size_t)geometry_doubles(nelem)));
+    // 17 doubles per element on the host into the kernels' padded stride
+    CK(cudaMemcpy2DAsync(s->geo.p, (size_t)geometry_stride() * sizeof(double), geo, 17 * sizeof(double),
+                         17 * sizeof(double), (size_t)nelem, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    s->geometry_given = true;
+    s->pattern_state = 0;
     s->assembled = false;
     return PHG_GPU_OK;
 }
@@ -920,8 +942,9 @@ static int element_pass(phgGpuSystem *s, const double *kappa, double mass, const
     ea.kappa = dk; ea.f = df; ea.mass = mass;
     ea.gk = s->gk.p; ea.br = s->br.p; ea.brt = s->brt.p; ea.wk_host = s->wk.data(); ea.wr_host = s->wr.data();
     ea.Ke = s->Ke.p; ea.Re = s->Re.p; ea.geo = s->geo.p; ea.status = s->status.p;
+    ea.geometry_given = s->geometry_given;
     CK(launch_element_kernel(s->order, ea, s->stream));
-    s->launches += 2;
+    s->launches += s->geometry_given ? 1 : 2;
     return PHG_GPU_OK;
 }
 

@@ -119,6 +119,7 @@ static void fail(const char *what) {
 static void prepare(GRID *g, DOF *u) {
     ELEMENT *e;
     INT *elems, *e2l;
+    double *geo;
     unsigned char *bdry;
     INT ndof, it;
     int k;
@@ -137,6 +138,16 @@ static void prepare(GRID *g, DOF *u) {
         for (k = 0; k < S.N; k++) e2l[(size_t)S.N * e->index + k] = phgDofMapE2D_(u, e, k, FALSE);
     }
     if (phgGpuSetMesh(S.sys, g->nvert, &g->verts[0][0], g->nelem, elems) != PHG_GPU_OK) fail("phgGpuSetMesh");
+    /* PHG's own Jacobians and volumes (interpolated from the parent on
+     * elements made by bisection, geom.c:460-565), which its phgQuad* use */
+    geo = (double *)malloc(sizeof(double) * 17 * (size_t)g->nelem);
+    ForAllElements2(g, e, it) {
+        const FLOAT *J = phgGeomGetJacobian(g, e);
+        for (k = 0; k < 16; k++) geo[17 * (size_t)e->index + k] = J[k];
+        geo[17 * (size_t)e->index + 16] = phgGeomGetVolume(g, e);
+    }
+    if (phgGpuSetGeometry(S.sys, g->nelem, geo) != PHG_GPU_OK) fail("phgGpuSetGeometry");
+    free(geo);
     if (phgGpuSetDofMap(S.sys, S.p, ndof, e2l, bdry) != PHG_GPU_OK) fail("phgGpuSetDofMap");
     free(elems);
     free(e2l);

@@ -15,7 +15,7 @@ def pytest_configure(config):
 
 
 def golden_cases():
-    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "p*_m*.npz")))
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "p[123]_*.npz")))
 
 
 def load_golden(name):

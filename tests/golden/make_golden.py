@@ -6,7 +6,8 @@ reference's element loop + phgSolverAssemble + phgSolverUpdateRHS +
 phgSolverSolve with -solver pcg, bicgstab or gmres (gmres_r or PHG's default
 flgmres_r), see oracle/ref_driver/phg_dump.c) and stores
 the reference's own inputs (coordinates, element vertices and element->DOF
-maps as PHG numbered them, f and g at the DOF nodes, Dirichlet flags, kappa)
+maps as PHG numbered them, PHG's element geometry (Jacobian and volume), f
+and g at the DOF nodes, Dirichlet flags, kappa)
 and outputs (matrix rows before and after boundary elimination, saved
 boundary columns, RHS before/after update_rhs, Jacobi diagonal, solution,
 iteration count, residual) in one compressed .npz per case, plus the
@@ -134,7 +135,8 @@ def run_case(name, m, P, case, kseed, rtol, mass=0.0, solver="pcg", opts=None):
             e2l=L("e2l.i32", np.int32).reshape(-1, N),
             bdry=L("bdry.u8", np.uint8), f=L("f.f64", np.float64), g=L("g.f64", np.float64),
             rhs_raw=L("rhs_raw.f64", np.float64), rhs=L("rhs.f64", np.float64),
-            diag=L("diag.f64", np.float64), x=L("x.f64", np.float64))
+            diag=L("diag.f64", np.float64), x=L("x.f64", np.float64),
+            geom=L("geom.f64", np.float64).reshape(-1, 17))
         if kappa is not None:
             out["kappa"] = L("kappa.f64", np.float64)
         if (opts or {}).get("mesh") == "cube.dat":

@@ -18,12 +18,20 @@ from conftest import golden_cases, load_golden
 pytestmark = pytest.mark.gpu
 
 
-def build(pb, order, verts, elems, e2l, bdry, f, g=None, kappa=None, mass=0.0):
+def build(pb, order, verts, elems, e2l, bdry, f, g=None, kappa=None, mass=0.0, geom=None):
     s = pb.Solver(0)
     s.set_mesh(verts, elems)
+    if geom is not None:
+        s.set_geometry(geom)
     s.set_dof_map(order, e2l, bdry)
     s.build_linear_system(kappa=kappa, f=f, g=g, mass=mass)
     return s
+
+
+def phg_geometry(name, G):
+    """PHG's stored geometry for meshes it refined by bisection (interpolated
+    from the parents, geom.c:460-565); None (the coordinates') otherwise."""
+    return G["geom"] if "refined" in name else None
 
 
 def solution_tol(rtol):
@@ -35,7 +43,7 @@ def solution_tol(rtol):
 def test_golden_assembly_bitexact(gpu, name):
     G = load_golden(name)
     s = build(gpu, int(G["order"]), G["verts"], G["elems"], G["e2l"], G["bdry"], G["f"], G["g"],
-              G.get("kappa"), float(G.get("mass", 0.0)))
+              G.get("kappa"), float(G.get("mass", 0.0)), phg_geometry(name, G))
     ptr, cols, vals = s.get_matrix()
     assert np.array_equal(ptr, G["rows_ptr"])
     assert np.array_equal(cols, G["rows_cols"])
@@ -55,7 +63,7 @@ def test_golden_solve(gpu, name):
     PHG's default GMRES, FLGMRES_r)."""
     G = load_golden(name)
     s = build(gpu, int(G["order"]), G["verts"], G["elems"], G["e2l"], G["bdry"], G["f"], G["g"],
-              G.get("kappa"), float(G.get("mass", 0.0)))
+              G.get("kappa"), float(G.get("mass", 0.0)), phg_geometry(name, G))
     rtol = float(G["rtol"])
     solver = str(G["solver"]) if "solver" in G else "pcg"
     if solver in ("gmres_r", "flgmres_r"):
@@ -329,3 +337,24 @@ def test_rebuild_on_recorded_pattern(gpu, oracle):
                 assert abs(nits - no) <= 2
                 assert np.linalg.norm(x - xo) <= 1e-7 * np.linalg.norm(xo)
                 assert rm <= 1e-10 * np.linalg.norm(o["rhs"]) * (1 + 1e-9)
+
+
+@pytest.mark.parametrize("name", ["p2_m5_kappa", "p3_m3_mass"])
+def test_given_geometry_on_unrefined_mesh(gpu, name):
+    """On a mesh PHG did not refine, its stored geometry is the one the GPU
+    computes from the coordinates: the rows are the same bit for bit either
+    way, and a non-finite geometry is refused."""
+    G = load_golden(name)
+    args = (gpu, int(G["order"]), G["verts"], G["elems"], G["e2l"], G["bdry"], G["f"], G["g"],
+            G.get("kappa"), float(G.get("mass", 0.0)))
+    a, b = build(*args), build(*args, geom=G["geom"])
+    for x, y in zip(a.get_matrix() + (a.get_rhs(),), b.get_matrix() + (b.get_rhs(),)):
+        assert np.array_equal(x, y)
+    bad = G["geom"].copy()
+    bad[3, 16] = np.nan
+    with pytest.raises(gpu.PhgGpuError):
+        b.set_geometry(bad)
+    with pytest.raises(gpu.PhgGpuError):
+        b.set_geometry(G["geom"][:-1])
+    a.close()
+    b.close()

@@ -16,17 +16,49 @@ def test_quadrature_rules_bitexact(oracle):
         assert np.array_equal(wts, ref[:, 4]), order
 
 
+def refined(name):
+    """Meshes PHG refined by bisection: their elements' Jacobians and volumes
+    are interpolated from the parents (geom.c:460-565), not computed from
+    the coordinates, so the assembly takes PHG's stored geometry."""
+    return "refined" in name
+
+
 @pytest.mark.parametrize("name", golden_cases())
 def test_assembly_bitexact(oracle, name):
     G = load_golden(name)
     o = oracle.assemble(int(G["order"]), G["verts"], G["elems"], G["e2l"], G["bdry"], G["f"],
-                        G["g"], G.get("kappa"), float(G.get("mass", 0.0)))
+                        G["g"], G.get("kappa"), float(G.get("mass", 0.0)),
+                        geom=G["geom"] if refined(name) else None)
     for pre, op in (("rows_raw", "raw_"), ("rows", ""), ("bdry_rows", "b")):
         assert np.array_equal(G[pre + "_ptr"], o[op + "ptr"]), pre
         assert np.array_equal(G[pre + "_cols"], o[op + "cols"]), pre
         assert np.array_equal(G[pre + "_vals"], o[op + "vals"]), pre
     for k in ("rhs_raw", "rhs", "diag"):
         assert np.array_equal(G[k], o[k]), k
+
+
+@pytest.mark.parametrize("name", [n for n in golden_cases() if not refined(n)])
+def test_coordinate_geometry_is_phgs(oracle, name):
+    """On meshes PHG imported (no bisection) the geometry computed from the
+    coordinates (compute_jacobian, geom.c:103-169) is PHG's stored one, so
+    assembling with PHG's dumped geometry changes nothing."""
+    G = load_golden(name)
+    args = (int(G["order"]), G["verts"], G["elems"], G["e2l"], G["bdry"], G["f"], G["g"], G.get("kappa"),
+            float(G.get("mass", 0.0)))
+    a, b = oracle.assemble(*args), oracle.assemble(*args, geom=G["geom"])
+    for k in ("raw_ptr", "raw_cols", "raw_vals", "vals", "rhs"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_refined_geometry_differs_from_coordinates(oracle):
+    """On a bisected mesh PHG's interpolated Jacobians differ from the ones
+    the coordinates give in the last bits, and the assembled rows keep
+    entries the coordinates would turn into round-off (or the reverse)."""
+    G = load_golden("p1_corner_refined")
+    args = (1, G["verts"], G["elems"], G["e2l"], G["bdry"], G["f"], G["g"], G.get("kappa"))
+    a, b = oracle.assemble(*args), oracle.assemble(*args, geom=G["geom"])
+    assert not np.array_equal(a["raw_cols"], b["raw_cols"])
+    assert np.array_equal(b["raw_cols"], G["rows_raw_cols"])
 
 
 def solver_of(G):
