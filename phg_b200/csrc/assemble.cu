@@ -407,6 +407,148 @@ element_lanes_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo
     }
 }
 
+// Element matrices and vectors, N / 2 lanes per element (P1: 16 elements a
+// warp, P2: 6).  Lane j owns the columns j and N - 1 - j and evaluates the
+// entries (a, j) for a <= j and (a, N - 1 - j) for a <= N - 1 - j: N + 1
+// entries a lane, the N (N + 1) / 2 pairs of the element once each, as the
+// reference's loop over j <= i does; each value is stored at (a, b) and
+// (b, a).  Every operation is the one the lane-per-column kernel performs in
+// the same order (round-to-nearest, no contraction), so the matrices are the
+// same bits; the lanes evaluate half the entries and read half the
+// shared-memory words.
+template <int P>
+__global__ void __launch_bounds__(128)
+element_pairs_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, const int32_t *__restrict__ e2l,
+                     const double *__restrict__ kappa, const double mass, const double *__restrict__ f,
+                     const ElemWeights Wt, const double *__restrict__ gk, const double *__restrict__ br,
+                     const double *__restrict__ brt, double *__restrict__ Ke, double *__restrict__ Re, int *status) {
+    using D = ElemDims<P>;
+    constexpr int N = D::N, QK = D::QK, QR = D::QR, W = 4, H = N / 2;
+    constexpr int EPW = 32 / H;                  // elements per warp
+    constexpr int CS = QK * N;                   // component stride of the gk table
+    static_assert(N % 2 == 0, "columns are paired");
+    __shared__ double s_g[W][EPW][QK * 3][N];   // gradient component c at point q of basis b: [q * 3 + c][b]
+    __shared__ double s_f[W][EPW][N];
+    __shared__ double s_fq[W][EPW][QR];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int sub = lane / H, j = lane - sub * H;
+    const bool lane_ok = sub < EPW;
+    const int sl = lane_ok ? sub : 0;
+    const int b1 = j, b2 = N - 1 - j;
+    double(*G)[N] = s_g[w][sl];
+    double *fl = s_f[w][sl], *fq = s_fq[w][sl];
+
+    // gradient of basis b at the stiffness points (as the lane-per-column kernel)
+    auto grad = [&](const double *J, bool act, int b, double (&g)[QK][3]) {
+#pragma unroll
+        for (int q = 0; q < QK; q++) {
+            if (P == 1) {
+#pragma unroll
+                for (int c = 0; c < 3; c++) g[q][c] = act ? J[4 * b + c] : 0.0;
+            } else if (b < 4) {
+                const double d = gk[(b * QK + q) * N + b];
+#pragma unroll
+                for (int c = 0; c < 3; c++) g[q][c] = rn_mul(d, act ? J[4 * b + c] : 0.0);
+            } else {
+                const double *Gk = gk + q * N + b;
+                const double g0 = Gk[0], g1 = Gk[CS], g2 = Gk[2 * CS], g3 = Gk[3 * CS];
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const double j0 = act ? J[c] : 0.0, j1 = act ? J[4 + c] : 0.0;
+                    const double j2 = act ? J[8 + c] : 0.0, j3 = act ? J[12 + c] : 0.0;
+                    g[q][c] = rn_add(rn_add(rn_add(rn_mul(g0, j0), rn_mul(g1, j1)), rn_mul(g2, j2)), rn_mul(g3, j3));
+                }
+            }
+        }
+    };
+
+    for (int64_t e0 = ((int64_t)blockIdx.x * W + w) * EPW; e0 < nelem; e0 += (int64_t)gridDim.x * W * EPW) {
+        const int64_t e = e0 + sub;
+        const bool act = lane_ok && e < nelem;
+        const double *J = geo + (size_t)(act ? e : 0) * kGeo;
+        double kap = 0.0;
+        if (act && kappa != nullptr) {
+            kap = kappa[e];
+            if (j == 0 && !isfinite(kap)) atomicExch(status, PHGB_DEV_NONFINITE);
+        }
+        double g1[QK][3], g2[QK][3];
+        grad(J, act, b1, g1);
+        grad(J, act, b2, g2);
+        double fv1 = 0.0, fv2 = 0.0;
+        if (act && f != nullptr) {
+            const int32_t d1 = e2l[(size_t)e * N + b1], d2 = e2l[(size_t)e * N + b2];
+            if (d1 < 0 || d1 >= ndof || d2 < 0 || d2 >= ndof) atomicExch(status, PHGB_DEV_BAD_INDEX);
+            else {
+                fv1 = f[d1];
+                fv2 = f[d2];
+            }
+            if (!isfinite(fv1) || !isfinite(fv2)) atomicExch(status, PHGB_DEV_NONFINITE);
+        }
+        if (lane_ok) {
+#pragma unroll
+            for (int q = 0; q < QK; q++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    G[q * 3 + c][b1] = g1[q][c];
+                    G[q * 3 + c][b2] = g2[q][c];
+                }
+            fl[b1] = fv1;
+            fl[b2] = fv2;
+        }
+        __syncwarp();
+        // f_h at the RHS points (phgDofEval_: sum over the element's nodes)
+        if (lane_ok)
+            for (int q = j; q < QR; q += H) {
+                double v = 0.0;
+                for (int k = 0; k < N; k++) v = rn_add(v, rn_mul(brt[k * QR + q], fl[k]));
+                fq[q] = v;
+            }
+        __syncwarp();
+        const double vol = act ? J[16] : 0.0;
+        double *Ke_e = Ke + (size_t)(act ? e : 0) * N * N;
+        // the lane's N + 1 pairs: (a, b1) for a <= b1, then (a, b2) for a <= b2
+        for (int k = 0; k <= N; k++) {
+            const bool first = k <= b1;
+            const int a = first ? k : k - b1 - 1;
+            const int b = first ? b1 : b2;
+            double d = 0.;
+#pragma unroll
+            for (int q = 0; q < QK; q++) {
+                const double x0 = first ? g1[q][0] : g2[q][0];
+                const double x1 = first ? g1[q][1] : g2[q][1];
+                const double x2 = first ? g1[q][2] : g2[q][2];
+                const double d0 = rn_add(0., rn_add(rn_add(rn_mul(x0, G[q * 3][a]), rn_mul(x1, G[q * 3 + 1][a])),
+                                                    rn_mul(x2, G[q * 3 + 2][a])));
+                const double t = rn_mul(d0, Wt.wk[q]);
+                d = rn_add(d, kappa != nullptr ? rn_mul(t, kap) : t);
+            }
+            double v = rn_mul(d, vol);
+            if (mass != 0.0) {
+                double dm = 0.;
+                for (int q = 0; q < QR; q++) {
+                    const double d0 = rn_add(0., rn_mul(br[q * N + b], br[q * N + a]));
+                    dm = rn_add(dm, rn_mul(d0, Wt.wr[q]));
+                }
+                v = rn_add(v, rn_mul(mass, rn_mul(dm, vol)));
+            }
+            if (act) {
+                Ke_e[a * N + b] = v;
+                Ke_e[b * N + a] = v;
+            }
+        }
+        if (act) {
+            double r1 = 0.0, r2 = 0.0;
+            for (int q = 0; q < QR; q++) {
+                r1 = rn_add(r1, rn_mul(rn_mul(br[q * N + b1], Wt.wr[q]), fq[q]));
+                r2 = rn_add(r2, rn_mul(rn_mul(br[q * N + b2], Wt.wr[q]), fq[q]));
+            }
+            Re[(size_t)e * N + b1] = rn_mul(r1, vol);
+            Re[(size_t)e * N + b2] = rn_mul(r2, vol);
+        }
+        __syncwarp();
+    }
+}
+
 // ---------------------------------------------------------------------------
 // DOF -> (element, basis) incidence lists.
 
@@ -564,7 +706,7 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
                 int32_t *__restrict__ sc_cols, double *__restrict__ sc_vals,
                 double *__restrict__ rhs, double *__restrict__ diag, int *status,
                 int32_t *__restrict__ over_list, int *nover, uint16_t *__restrict__ slot,
-                uint16_t *__restrict__ tmap) {
+                uint16_t *__restrict__ tmap, int32_t *__restrict__ dpos) {
     constexpr int G = C::G, R = C::R, HS = C::HS, MAXROW = C::MAXROW, W = C::WARPS;
     __shared__ int32_t s_key[W][R][HS];
     __shared__ int16_t s_pos[W][R][HS];
@@ -741,6 +883,7 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
                 sc_cols[q] = c;
                 sc_vals[q] = val;
                 if (tmap != nullptr) tmap[rbase + t] = (uint16_t)k;
+                if (dpos != nullptr && c == d) dpos[d] = k;
             }
             if (valid && isbc) {
                 const int j = nb + __popc(bm & lt_mask);
@@ -793,24 +936,26 @@ __global__ void __launch_bounds__(C::WARPS * 32, C::LONG ? 1 : 8)
 value_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t *__restrict__ inc,
                   const uint8_t *__restrict__ bdry, const double *__restrict__ Ke, const double *__restrict__ Re,
                   const double *__restrict__ g, const uint16_t *__restrict__ slot, const uint16_t *__restrict__ tmap,
-                  const int32_t *__restrict__ ptr, const int32_t *__restrict__ cols, const int32_t *__restrict__ bptr,
-                  const int32_t *__restrict__ bcols, double *__restrict__ vals, double *__restrict__ bvals,
-                  double *__restrict__ rhs, double *__restrict__ diag, int *status,
+                  const int32_t *__restrict__ dpos, const int32_t *__restrict__ ptr,
+                  const int32_t *__restrict__ bptr, const int32_t *__restrict__ bcols, double *__restrict__ vals,
+                  double *__restrict__ bvals, double *__restrict__ rhs, double *__restrict__ diag, int *status,
                   const int32_t *__restrict__ over_list, const int *nover) {
     constexpr int G = C::G, R = C::R, MAXROW = C::MAXROW, W = C::WARPS;
+    static_assert(N % 2 == 0, "element rows are staged as 16-byte pairs");
     __shared__ double s_val[W][R][MAXROW];
-    __shared__ uint8_t s_isb[W][R][MAXROW];
+    __shared__ __align__(16) double s_ke[W][R][G][N];     // staged element rows of G incidences
+    __shared__ __align__(4) uint16_t s_sl[W][R][G][N];    // and their recorded slots
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int grp = lane / G, gl = lane % G;
+    const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (grp * G);
     double *sval = s_val[w][grp];
-    uint8_t *sisb = s_isb[w][grp];
 
     const int64_t nwarps = (int64_t)gridDim.x * W;
     const int64_t nrows = C::LONG ? (int64_t)*nover : ndof;
     for (int64_t wb = ((int64_t)blockIdx.x * W + w) * R; wb < nrows; wb += nwarps * R) {
         const int64_t d = C::LONG ? (wb + grp < nrows ? (int64_t)over_list[wb + grp] : ndof) : wb + grp;
         const bool active = d < ndof;
-        int32_t i0 = 0, i1 = 0, p0 = 0, nk = 0, b0 = 0, nb = 0;
+        int32_t i0 = 0, i1 = 0, p0 = 0, nk = 0, b0 = 0, nb = 0, dk = -1;
         bool isb = false;
         if (active) {
             i0 = inc_ptr[d];
@@ -820,6 +965,7 @@ value_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32
             nk = ptr[d + 1] - p0;
             b0 = bptr[d];
             nb = bptr[d + 1] - b0;
+            dk = dpos[d];
         }
         const int L = nk + nb;
         if (active && isb && gl == 0) {   // the Dirichlet row, as the walk makes it
@@ -842,22 +988,49 @@ value_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32
         if (maxwalk == 0) continue;   // warp-uniform
         const int Lw = walk ? L : 0;
         for (int t = gl; t < Lw; t += G) sval[t] = 0.0;
-        __syncwarp();
         bool changed = false;
-        for (int ii = 0; ii < maxwalk; ii++) {
-            if (ii < nwalk && gl < N) {
-                const int32_t kk = inc[i0 + ii];
+        for (int c0 = 0; c0 < maxwalk; c0 += G) {
+            // lane gl stages incidence c0 + gl: its element row (N / 2 16-byte
+            // loads) and its N recorded slots, so a group has G rows in flight
+            const int ii = c0 + gl;
+            if (ii < nwalk) {
+                const int32_t kk = __ldg(&inc[i0 + ii]);
                 const int32_t e = kk / N, a = kk - e * N;
-                const double v = Ke[((size_t)e * N + a) * N + gl];
-                const uint16_t t = slot[((int64_t)i0 + ii) * N + gl];
-                if ((v != 0.0) != (t != kSlotZero) || (t != kSlotZero && t >= L)) changed = true;
-                else if (t != kSlotZero) sval[t] = rn_add(sval[t], v);
+                const double2 *src = reinterpret_cast<const double2 *>(Ke + ((size_t)e * N + a) * N);
+                const uint32_t *ssrc = reinterpret_cast<const uint32_t *>(slot + ((int64_t)i0 + ii) * N);
+                double2 kv[N / 2];
+                uint32_t sv[N / 2];
+#pragma unroll
+                for (int q = 0; q < N / 2; q++) kv[q] = __ldcs(src + q);
+#pragma unroll
+                for (int q = 0; q < N / 2; q++) sv[q] = __ldcs(ssrc + q);
+                double2 *dst = reinterpret_cast<double2 *>(s_ke[w][grp][gl]);
+                uint32_t *sdst = reinterpret_cast<uint32_t *>(s_sl[w][grp][gl]);
+#pragma unroll
+                for (int q = 0; q < N / 2; q++) {
+                    dst[q] = kv[q];
+                    sdst[q] = sv[q];
+                }
             }
             __syncwarp();
+            // add them in element order (lane gl: column gl of each row)
+            const int nj = nwalk - c0 < G ? nwalk - c0 : G;
+            const int maxj = __reduce_max_sync(0xffffffffu, (unsigned)(nj > 0 ? nj : 0));
+            for (int j = 0; j < maxj; j++) {
+                if (j < nj && gl < N) {
+                    const double v = s_ke[w][grp][j][gl];
+                    const uint16_t t = s_sl[w][grp][j][gl];
+                    if ((v != 0.0) != (t != kSlotZero) || (t != kSlotZero && t >= L)) changed = true;
+                    else if (t != kSlotZero) sval[t] = rn_add(sval[t], v);
+                }
+                __syncwarp();
+            }
         }
         if (changed) atomicExch(status, PHGB_DEV_PATTERN_CHANGED);
-        // write the entries; boundary columns get their lift term in place
+        // write the entries; a boundary column's value is replaced in s_val by
+        // its lift term
         double dg = 0.0;
+        bool anyb = false;
         for (int t = gl; t < Lw; t += G) {
             const uint16_t tm = tmap[(int64_t)i0 * N + t];
             const double val = sval[t];
@@ -870,13 +1043,13 @@ value_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32
                 for (int m = 0; m < mult; m++) Dk = rn_add(Dk, 1.0);
                 const double rk = bdry_rhs(g, c, mult);
                 sval[t] = __ddiv_rn(rn_mul(rn_mul(1.0, rk), val), Dk);
-                sisb[t] = 1;
+                anyb = true;
             } else {
                 vals[p0 + tm] = val;
-                if (cols[p0 + tm] == d) dg = val;
-                sisb[t] = 0;
+                if (tm == dk) dg = val;
             }
         }
+        const bool lift = (__ballot_sync(0xffffffffu, anyb) & gmask) != 0;
 #pragma unroll
         for (int o = G / 2; o > 0; o >>= 1) dg += __shfl_xor_sync(0xffffffffu, dg, o, G);
         // element right-hand sides in element order, zeros skipped
@@ -892,8 +1065,10 @@ value_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32
         __syncwarp();
         if (walk && gl == 0) {
             diag[d] = dg;
-            for (int t = 0; t < L; t++)
-                if (sisb[t]) r = rn_sub(r, sval[t]);
+            // lift the boundary columns in first-touch order: r -= term
+            if (lift)
+                for (int t = 0; t < L; t++)
+                    if (tmap[(int64_t)i0 * N + t] & kTmapBdry) r = rn_sub(r, sval[t]);
             rhs[d] = r;
         }
         __syncwarp();
@@ -1079,10 +1254,10 @@ static void elem_launch(const ElemArgs &A, cudaStream_t s) {
     ElemWeights Wt{};
     for (int q = 0; q < ElemDims<P>::QK; q++) Wt.wk[q] = A.wk_host[q];
     for (int q = 0; q < ElemDims<P>::QR; q++) Wt.wr[q] = A.wr_host[q];
-    if constexpr (P <= 2) {   // a lane per basis function
-        constexpr int EPB = 4 * (32 / ElemDims<P>::N);   // elements per block
+    if constexpr (P <= 2) {   // two basis functions a lane
+        constexpr int EPB = 4 * (32 / (ElemDims<P>::N / 2));   // elements per block
         const int blocks = grid_for(A.nelem, EPB, 148 * 64);
-        element_lanes_kernel<P><<<blocks, 128, 0, s>>>(A.nelem, A.ndof, A.geo, A.e2l, A.kappa, A.mass, A.f, Wt,
+        element_pairs_kernel<P><<<blocks, 128, 0, s>>>(A.nelem, A.ndof, A.geo, A.e2l, A.kappa, A.mass, A.f, Wt,
                                                        A.gk, A.br, A.brt, A.Ke, A.Re, A.status);
     } else {          // P3: a warp per element
         const int blocks = grid_for(A.nelem, W, 148 * 64);
@@ -1137,12 +1312,12 @@ static cudaError_t walk(const WalkArgs &A, cudaStream_t s) {
     if (e != cudaSuccess) return e;
     row_walk_kernel<N, WalkCfg<N>><<<blocks, W * 32, 0, s>>>(
         A.ndof, A.inc_ptr, A.inc, A.e2l, A.bdry, A.Ke, A.Re, A.g, A.cnt_keep, A.cnt_bdry, A.sc_cols, A.sc_vals,
-        A.rhs, A.diag, A.status, A.over_list, A.nover, A.slot, A.tmap);
+        A.rhs, A.diag, A.status, A.over_list, A.nover, A.slot, A.tmap, A.dpos);
     // the rows the first pass listed (none in most meshes: the blocks return
     // after reading the count)
     row_walk_kernel<N, LongWalkCfg<N>><<<148 * 4, 32, 0, s>>>(
         A.ndof, A.inc_ptr, A.inc, A.e2l, A.bdry, A.Ke, A.Re, A.g, A.cnt_keep, A.cnt_bdry, A.sc_cols, A.sc_vals,
-        A.rhs, A.diag, A.status, A.over_list, A.nover, A.slot, A.tmap);
+        A.rhs, A.diag, A.status, A.over_list, A.nover, A.slot, A.tmap, A.dpos);
     return cudaGetLastError();
 }
 
@@ -1151,10 +1326,10 @@ static cudaError_t value_walk(const WalkArgs &A, cudaStream_t s) {
     constexpr int W = WalkCfg<N>::WARPS, R = WalkCfg<N>::R;
     const int blocks = grid_for(ceil_div(A.ndof, R), W, 148 * 32);
     value_walk_kernel<N, WalkCfg<N>><<<blocks, W * 32, 0, s>>>(
-        A.ndof, A.inc_ptr, A.inc, A.bdry, A.Ke, A.Re, A.g, A.slot, A.tmap, A.ptr, A.cols, A.bptr, A.bcols, A.vals,
+        A.ndof, A.inc_ptr, A.inc, A.bdry, A.Ke, A.Re, A.g, A.slot, A.tmap, A.dpos, A.ptr, A.bptr, A.bcols, A.vals,
         A.bvals, A.rhs, A.diag, A.status, A.over_list, A.nover);
     value_walk_kernel<N, LongWalkCfg<N>><<<148 * 4, 32, 0, s>>>(
-        A.ndof, A.inc_ptr, A.inc, A.bdry, A.Ke, A.Re, A.g, A.slot, A.tmap, A.ptr, A.cols, A.bptr, A.bcols, A.vals,
+        A.ndof, A.inc_ptr, A.inc, A.bdry, A.Ke, A.Re, A.g, A.slot, A.tmap, A.dpos, A.ptr, A.bptr, A.bcols, A.vals,
         A.bvals, A.rhs, A.diag, A.status, A.over_list, A.nover);
     return cudaGetLastError();
 }

@@ -47,6 +47,9 @@ struct WalkArgs {
     // the pattern: recorded by the walk when non-null (nelem * N * N
     // entries each, indexed like the scratch regions), read by the value walk
     uint16_t *slot, *tmap;
+    // per row, the index of its diagonal among its kept entries (recorded
+    // with the pattern; rows without one keep the caller's -1)
+    int32_t *dpos;
 };
 
 cudaError_t launch_element_kernel(int p, const ElemArgs &a, cudaStream_t s);

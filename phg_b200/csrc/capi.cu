@@ -185,6 +185,7 @@ struct phgGpuSystem_ {
     // next records the pattern), 2 recorded (builds use the value walk)
     int pattern_state = 0;
     DevBuf<uint16_t> slot, tmap;
+    DevBuf<int32_t> dpos;                  // per row, its diagonal's index among the kept entries
     // rows assembled from recorded row segments (phgGpuAssembleRows)
     DevBuf<int32_t> rec_row, rec_cols, rec_inc_ptr, rec_inc, rec_cnt, rec_cursor, rec_cap, rec_cap_ptr;
     DevBuf<int64_t> rec_ptr;
@@ -978,7 +979,7 @@ static int build_system(phgGpuSystem *s, const double *kappa, double mass, const
     wa.over_list = s->over_list.p; wa.nover = s->nover.p;
     if (s->pattern_state == 2 && s->assembled && s->have_bdry_cols) {
         // the recorded pattern: values only, written in place
-        wa.slot = s->slot.p; wa.tmap = s->tmap.p;
+        wa.slot = s->slot.p; wa.tmap = s->tmap.p; wa.dpos = s->dpos.p;
         wa.ptr = s->rp.p; wa.cols = s->ci.p; wa.vals = s->va.p;
         wa.bptr = s->brp.p; wa.bcols = s->bci.p; wa.bvals = s->bva.p;
         CK(launch_value_walk(s->order, wa, s->stream));
@@ -1001,11 +1002,15 @@ static int build_system(phgGpuSystem *s, const double *kappa, double mass, const
     if (record) {
         CHECK_RC(s->slot.ensure(nscratch));
         CHECK_RC(s->tmap.ensure(nscratch));
+        CHECK_RC(s->dpos.ensure((size_t)ndof));
+        CK(cudaMemsetAsync(s->dpos.p, 0xff, sizeof(int32_t) * (size_t)ndof, s->stream));   // -1: no diagonal
         wa.slot = s->slot.p;
         wa.tmap = s->tmap.p;
+        wa.dpos = s->dpos.p;
     } else {
         wa.slot = nullptr;
         wa.tmap = nullptr;
+        wa.dpos = nullptr;
     }
     CK(launch_row_walk(s->order, wa, s->stream));
     s->launches += 8;   // walk (two passes) + two scans
@@ -1319,7 +1324,7 @@ int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol,
     double tol = -1.0;
     int nits_total = 0, nupd = 0;
     double res_true = 0.0;
-    const GearBuffers B{n, s->x.p, s->r.p, s->r32.p, s->u32.p, s->Ap32.p, s->p32.p, s->s32.p, s->y32.p, s->D32.p,
+    const GearBuffers B{n, s->x.p, s->r.p, s->rhs.p, s->r32.p, s->u32.p, s->Ap32.p, s->p32.p, s->s32.p, s->y32.p, s->D32.p,
                         s->partials.p, s->gst.p};
     const GearLayouts L{s->kind32, s->unroll32, sell_view(s), sell2_view(s), Q};
     // the solve's graph, captured again when a buffer or the layout changed

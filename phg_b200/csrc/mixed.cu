@@ -16,10 +16,14 @@
 //   K2  the vector update above, no reduction
 // A reliable update (the FP32 residual has fallen tenfold since the last one,
 // or the iteration looks converged) runs inside a conditional graph node:
-//   R1  x += y (FP64), rtrue -= A y with the FP64 matrix values, r = (float)
-//       rtrue, u = D^-1 r, ||rtrue||^2 -> the stopping test on the FP64
-//       residual (the reference's rule, get_tol solver-phg.c:104)
+//   R1  rtrue = b - A (x + y) with the FP64 matrix values (the explicit
+//       residual of the FP64 iterate), r = (float) rtrue, u = D^-1 r,
+//       ||rtrue||^2 -> the stopping test on the FP64 residual (the
+//       reference's rule, get_tol solver-phg.c:104)
 //   R2  K1 again on the new u
+// and the next K2 folds y into x (x += y, FP64) before restarting y.  The
+// stopping test thus sees the residual of the iterate it returns, not a
+// recurrence that may have drifted from it.
 // The iterations run in a conditional WHILE loop of `chunk` iterations per
 // pass, so a solve is one graph launch and the host waits once.
 #include "common.cuh"
@@ -129,11 +133,9 @@ gear_reliable_kernel(const L64 lay, const GearBuffers B) {
     for (int64_t s = warp; s < nsl; s += nwarps) {
         const int64_t pos = s * 32 + lane;
         const int32_t row = lay.row(pos);
-        const double acc = lay.sum(s, lane, pos, B.y);
+        const double acc = lay.sum_xy(s, lane, pos, B.x, B.y);
         if (row >= 0) {
-            B.x[row] += (double)B.y[row];
-            const double rt = B.rtrue[row] - acc;
-            B.rtrue[row] = rt;
+            const double rt = B.b[row] - acc;
             const float rf = (float)rt;
             B.r[row] = rf;
             B.u[row] = rf / B.D[row];
@@ -156,7 +158,8 @@ gear_reliable_kernel(const L64 lay, const GearBuffers B) {
     }
 }
 
-// K2: the vector update, 16-byte vectors of four rows, no reduction.
+// K2: the vector update, 16-byte vectors of four rows, no reduction.  After
+// a reliable update it first folds y into x (x += y in FP64) and restarts y.
 __global__ void __launch_bounds__(kVecThreads)
 gear_update_kernel(const GearBuffers B) {
     const GearState *st = B.st;
@@ -164,12 +167,22 @@ gear_update_kernel(const GearBuffers B) {
     const float a = (float)st->alpha, b = (float)st->beta;
     const bool reset = st->y_reset != 0;
     const int64_t n = B.n;
-    const int nfull = aligned16(B.r, B.u, B.w, B.p, B.s, B.y, B.D) ? (int)(n / 4) : 0;   // n < 2^31
+    const int nfull = aligned16(B.r, B.u, B.w, B.p, B.s, B.y, B.D, B.x) ? (int)(n / 4) : 0;   // n < 2^31
     const int stride = gridDim.x * blockDim.x;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nfull; c += stride) {
         const int i = 4 * c;
         VArr<float> u = vload(B.u + i), p = vload(B.p + i), w = vload_ro(B.w + i), s = vload(B.s + i);
-        VArr<float> y = reset ? VArr<float>{{0.0f, 0.0f, 0.0f, 0.0f}} : vload(B.y + i);
+        VArr<float> y = vload(B.y + i);
+        if (reset) {
+            VArr<double> x0 = vload(B.x + i), x1 = vload(B.x + i + 2);
+            x0.v[0] += (double)y.v[0];
+            x0.v[1] += (double)y.v[1];
+            x1.v[0] += (double)y.v[2];
+            x1.v[1] += (double)y.v[3];
+            vstore(B.x + i, x0);
+            vstore(B.x + i + 2, x1);
+            y = VArr<float>{{0.0f, 0.0f, 0.0f, 0.0f}};
+        }
         VArr<float> r = vload(B.r + i);
         const VArr<float> d = vload_ro(B.D + i);
 #pragma unroll
@@ -191,6 +204,7 @@ gear_update_kernel(const GearBuffers B) {
         const float p = B.u[i] + b * B.p[i], s = B.w[i] + b * B.s[i];
         B.p[i] = p;
         B.s[i] = s;
+        if (reset) B.x[i] += (double)B.y[i];
         B.y[i] = (reset ? 0.0f : B.y[i]) + a * p;
         const float r = B.r[i] - a * s;
         B.r[i] = r;
@@ -240,8 +254,8 @@ gear_init_kernel(const GearBuffers B, const double *__restrict__ D64, unsigned *
     if (grid_sum2(rr, ru, B.partials, ticket)) { out[0] = rr; out[1] = ru; }
 }
 
+// The solve is over: x += y (y holds the steps since the last fold).
 __global__ void gear_fold_kernel(const GearBuffers B) {
-    if (B.st->y_reset) return;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < B.n; i += (int64_t)gridDim.x * blockDim.x)
         B.x[i] += (double)B.y[i];
 }

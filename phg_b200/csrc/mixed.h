@@ -17,11 +17,13 @@ struct GearState {
 
 enum { GEAR_PASS_LIMIT = kStatusPassLimit };   // status: the graph loop ran out of passes
 
-// Working vectors: x and rtrue FP64; r, u = r / D, w = A u, p, s = A p and
-// the correction y FP32.
+// Working vectors: x, the right-hand side b and the initial residual rtrue
+// FP64; r, u = r / D, w = A u, p, s = A p and the correction y (not yet
+// folded into x) FP32.
 struct GearBuffers {
     int64_t n;
     double *x, *rtrue;
+    const double *b;
     float *r, *u, *w, *p, *s, *y, *D;
     double *partials;   // red_partials3_doubles(kRedMaxBlocks)
     GearState *st;
@@ -52,7 +54,7 @@ cudaError_t launch_gear_init(const GearBuffers &B, const double *D64, unsigned *
 // state says done.  Graph construction uses `stream` for capture.
 cudaError_t build_gear_graph(const GearBuffers &B, const GearLayouts &L, int chunk, cudaStream_t stream,
                              cudaGraphExec_t *exec, int *kernels_per_iteration);
-// x += y unless the correction was already folded in.
+// x += y: the correction not yet folded into x.
 cudaError_t launch_gear_fold(const GearBuffers &B, cudaStream_t s);
 
 // A graph that repeats `body` (launches on `stream`, captured) in a
