@@ -407,148 +407,6 @@ element_lanes_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo
     }
 }
 
-// Element matrices and vectors, N / 2 lanes per element (P1: 16 elements a
-// warp, P2: 6).  Lane j owns the columns j and N - 1 - j and evaluates the
-// entries (a, j) for a <= j and (a, N - 1 - j) for a <= N - 1 - j: N + 1
-// entries a lane, the N (N + 1) / 2 pairs of the element once each, as the
-// reference's loop over j <= i does; each value is stored at (a, b) and
-// (b, a).  Every operation is the one the lane-per-column kernel performs in
-// the same order (round-to-nearest, no contraction), so the matrices are the
-// same bits; the lanes evaluate half the entries and read half the
-// shared-memory words.
-template <int P>
-__global__ void __launch_bounds__(128)
-element_pairs_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, const int32_t *__restrict__ e2l,
-                     const double *__restrict__ kappa, const double mass, const double *__restrict__ f,
-                     const ElemWeights Wt, const double *__restrict__ gk, const double *__restrict__ br,
-                     const double *__restrict__ brt, double *__restrict__ Ke, double *__restrict__ Re, int *status) {
-    using D = ElemDims<P>;
-    constexpr int N = D::N, QK = D::QK, QR = D::QR, W = 4, H = N / 2;
-    constexpr int EPW = 32 / H;                  // elements per warp
-    constexpr int CS = QK * N;                   // component stride of the gk table
-    static_assert(N % 2 == 0, "columns are paired");
-    __shared__ double s_g[W][EPW][QK * 3][N];   // gradient component c at point q of basis b: [q * 3 + c][b]
-    __shared__ double s_f[W][EPW][N];
-    __shared__ double s_fq[W][EPW][QR];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int sub = lane / H, j = lane - sub * H;
-    const bool lane_ok = sub < EPW;
-    const int sl = lane_ok ? sub : 0;
-    const int b1 = j, b2 = N - 1 - j;
-    double(*G)[N] = s_g[w][sl];
-    double *fl = s_f[w][sl], *fq = s_fq[w][sl];
-
-    // gradient of basis b at the stiffness points (as the lane-per-column kernel)
-    auto grad = [&](const double *J, bool act, int b, double (&g)[QK][3]) {
-#pragma unroll
-        for (int q = 0; q < QK; q++) {
-            if (P == 1) {
-#pragma unroll
-                for (int c = 0; c < 3; c++) g[q][c] = act ? J[4 * b + c] : 0.0;
-            } else if (b < 4) {
-                const double d = gk[(b * QK + q) * N + b];
-#pragma unroll
-                for (int c = 0; c < 3; c++) g[q][c] = rn_mul(d, act ? J[4 * b + c] : 0.0);
-            } else {
-                const double *Gk = gk + q * N + b;
-                const double g0 = Gk[0], g1 = Gk[CS], g2 = Gk[2 * CS], g3 = Gk[3 * CS];
-#pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    const double j0 = act ? J[c] : 0.0, j1 = act ? J[4 + c] : 0.0;
-                    const double j2 = act ? J[8 + c] : 0.0, j3 = act ? J[12 + c] : 0.0;
-                    g[q][c] = rn_add(rn_add(rn_add(rn_mul(g0, j0), rn_mul(g1, j1)), rn_mul(g2, j2)), rn_mul(g3, j3));
-                }
-            }
-        }
-    };
-
-    for (int64_t e0 = ((int64_t)blockIdx.x * W + w) * EPW; e0 < nelem; e0 += (int64_t)gridDim.x * W * EPW) {
-        const int64_t e = e0 + sub;
-        const bool act = lane_ok && e < nelem;
-        const double *J = geo + (size_t)(act ? e : 0) * kGeo;
-        double kap = 0.0;
-        if (act && kappa != nullptr) {
-            kap = kappa[e];
-            if (j == 0 && !isfinite(kap)) atomicExch(status, PHGB_DEV_NONFINITE);
-        }
-        double g1[QK][3], g2[QK][3];
-        grad(J, act, b1, g1);
-        grad(J, act, b2, g2);
-        double fv1 = 0.0, fv2 = 0.0;
-        if (act && f != nullptr) {
-            const int32_t d1 = e2l[(size_t)e * N + b1], d2 = e2l[(size_t)e * N + b2];
-            if (d1 < 0 || d1 >= ndof || d2 < 0 || d2 >= ndof) atomicExch(status, PHGB_DEV_BAD_INDEX);
-            else {
-                fv1 = f[d1];
-                fv2 = f[d2];
-            }
-            if (!isfinite(fv1) || !isfinite(fv2)) atomicExch(status, PHGB_DEV_NONFINITE);
-        }
-        if (lane_ok) {
-#pragma unroll
-            for (int q = 0; q < QK; q++)
-#pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    G[q * 3 + c][b1] = g1[q][c];
-                    G[q * 3 + c][b2] = g2[q][c];
-                }
-            fl[b1] = fv1;
-            fl[b2] = fv2;
-        }
-        __syncwarp();
-        // f_h at the RHS points (phgDofEval_: sum over the element's nodes)
-        if (lane_ok)
-            for (int q = j; q < QR; q += H) {
-                double v = 0.0;
-                for (int k = 0; k < N; k++) v = rn_add(v, rn_mul(brt[k * QR + q], fl[k]));
-                fq[q] = v;
-            }
-        __syncwarp();
-        const double vol = act ? J[16] : 0.0;
-        double *Ke_e = Ke + (size_t)(act ? e : 0) * N * N;
-        // the lane's N + 1 pairs: (a, b1) for a <= b1, then (a, b2) for a <= b2
-        for (int k = 0; k <= N; k++) {
-            const bool first = k <= b1;
-            const int a = first ? k : k - b1 - 1;
-            const int b = first ? b1 : b2;
-            double d = 0.;
-#pragma unroll
-            for (int q = 0; q < QK; q++) {
-                const double x0 = first ? g1[q][0] : g2[q][0];
-                const double x1 = first ? g1[q][1] : g2[q][1];
-                const double x2 = first ? g1[q][2] : g2[q][2];
-                const double d0 = rn_add(0., rn_add(rn_add(rn_mul(x0, G[q * 3][a]), rn_mul(x1, G[q * 3 + 1][a])),
-                                                    rn_mul(x2, G[q * 3 + 2][a])));
-                const double t = rn_mul(d0, Wt.wk[q]);
-                d = rn_add(d, kappa != nullptr ? rn_mul(t, kap) : t);
-            }
-            double v = rn_mul(d, vol);
-            if (mass != 0.0) {
-                double dm = 0.;
-                for (int q = 0; q < QR; q++) {
-                    const double d0 = rn_add(0., rn_mul(br[q * N + b], br[q * N + a]));
-                    dm = rn_add(dm, rn_mul(d0, Wt.wr[q]));
-                }
-                v = rn_add(v, rn_mul(mass, rn_mul(dm, vol)));
-            }
-            if (act) {
-                Ke_e[a * N + b] = v;
-                Ke_e[b * N + a] = v;
-            }
-        }
-        if (act) {
-            double r1 = 0.0, r2 = 0.0;
-            for (int q = 0; q < QR; q++) {
-                r1 = rn_add(r1, rn_mul(rn_mul(br[q * N + b1], Wt.wr[q]), fq[q]));
-                r2 = rn_add(r2, rn_mul(rn_mul(br[q * N + b2], Wt.wr[q]), fq[q]));
-            }
-            Re[(size_t)e * N + b1] = rn_mul(r1, vol);
-            Re[(size_t)e * N + b2] = rn_mul(r2, vol);
-        }
-        __syncwarp();
-    }
-}
-
 // ---------------------------------------------------------------------------
 // DOF -> (element, basis) incidence lists.
 
@@ -1254,10 +1112,10 @@ static void elem_launch(const ElemArgs &A, cudaStream_t s) {
     ElemWeights Wt{};
     for (int q = 0; q < ElemDims<P>::QK; q++) Wt.wk[q] = A.wk_host[q];
     for (int q = 0; q < ElemDims<P>::QR; q++) Wt.wr[q] = A.wr_host[q];
-    if constexpr (P <= 2) {   // two basis functions a lane
-        constexpr int EPB = 4 * (32 / (ElemDims<P>::N / 2));   // elements per block
+    if constexpr (P <= 2) {   // a lane per basis function
+        constexpr int EPB = 4 * (32 / ElemDims<P>::N);   // elements per block
         const int blocks = grid_for(A.nelem, EPB, 148 * 64);
-        element_pairs_kernel<P><<<blocks, 128, 0, s>>>(A.nelem, A.ndof, A.geo, A.e2l, A.kappa, A.mass, A.f, Wt,
+        element_lanes_kernel<P><<<blocks, 128, 0, s>>>(A.nelem, A.ndof, A.geo, A.e2l, A.kappa, A.mass, A.f, Wt,
                                                        A.gk, A.br, A.brt, A.Ke, A.Re, A.status);
     } else {          // P3: a warp per element
         const int blocks = grid_for(A.nelem, W, 148 * 64);

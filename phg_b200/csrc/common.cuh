@@ -25,6 +25,10 @@ __device__ __forceinline__ double rn_mul(double a, double b) { return __dmul_rn(
 __device__ __forceinline__ double rn_add(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double rn_sub(double a, double b) { return __dsub_rn(a, b); }
 
+// acc + a x in FP32 with the product and the sum rounded on their own (no
+// fused multiply-add): the row sums of the mixed solver's FP32 products.
+__device__ __forceinline__ float fma_free(float acc, float a, float x) { return __fadd_rn(acc, __fmul_rn(a, x)); }
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -42,3 +46,19 @@ __device__ __forceinline__ int warp_sumi(int v) {
 }
 
 static inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// Asynchronous global -> shared copies (cp.async; both addresses aligned to
+// the size) and the wait for all of the calling thread's copies.
+__device__ __forceinline__ void copy_async16(void *smem, const void *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void copy_async8(void *smem, const void *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void copy_async4(void *smem, const void *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void copy_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }

@@ -87,10 +87,12 @@ __device__ __forceinline__ bool gear_final(GearState *st, double gamma, double d
 }
 
 // ---------------------------------------------------------------------------
-// K1 / R2: w = A u with the three dot products.  Grid-stride over slices,
-// at most 8 blocks of 256 threads per SM.
+// K1 / R2: w = A u with the three dot products.  Grid-stride over slices on
+// a grid of kGearBlocksPerSM blocks of 256 threads per SM.
+constexpr int kGearBlocksPerSM = 8;
+
 template <class L, bool AFTER_RU>
-__global__ void __launch_bounds__(kVecThreads, kResidentBlocks)
+__global__ void __launch_bounds__(kVecThreads, kGearBlocksPerSM)
 gear_spmv_kernel(const L lay, const GearBuffers B, cudaGraphConditionalHandle hif) {
     GearState *st = B.st;
     if (st->done) return;
@@ -322,7 +324,8 @@ static cudaError_t add_conditional(cudaGraph_t g, cudaGraphNode_t dep, cudaGraph
 template <class L32, class L64>
 static cudaError_t build_body(const GearBuffers &B, const L32 &l32, const L64 &l64, int chunk, cudaStream_t stream,
                               cudaGraph_t body, cudaGraphConditionalHandle hwhile) {
-    const int sb = vec_blocks(l32.nslices_host * 32);
+    int sb = vec_blocks(l32.nslices_host * 32);
+    if (sb > 148 * kGearBlocksPerSM) sb = 148 * kGearBlocksPerSM;
     const int rb = sb < 148 * 6 ? sb : 148 * 6;   // the reliable kernel holds 6 blocks per SM
     const int ub = update_blocks(B.n);
     cudaGraphNode_t prev = nullptr;

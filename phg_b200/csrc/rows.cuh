@@ -12,6 +12,12 @@
 
 namespace phgb {
 
+// The FP32 products of the mixed solver round each product a_ij x_j and each
+// partial sum to FP32 on its own (__fmul_rn, __fadd_rn): contracted into
+// fused multiply-adds, the sums perturb the single-reduction recurrence
+// enough to cost it a fifth more iterations at 2 million rows (264 against
+// 219 on P2 64^3; 216 with exact products summed in FP64, whose conversions
+// cost more time than the three iterations they save).
 // FP32 values of the q16 layout, four entries per lane per step, U steps in flight.
 template <int U>
 struct Q16Rows32 {
@@ -38,10 +44,10 @@ struct Q16Rows32 {
 #pragma unroll
             for (int u = 0; u < U; u++) {
                 const int j = 4 * (jq + u);
-                if (j < l) acc += v[u].x * __ldg(&x[q16_col(j, sp, b0, b1, c[u].x & 0xffffu)]);
-                if (j + 1 < l) acc += v[u].y * __ldg(&x[q16_col(j + 1, sp, b0, b1, c[u].x >> 16)]);
-                if (j + 2 < l) acc += v[u].z * __ldg(&x[q16_col(j + 2, sp, b0, b1, c[u].y & 0xffffu)]);
-                if (j + 3 < l) acc += v[u].w * __ldg(&x[q16_col(j + 3, sp, b0, b1, c[u].y >> 16)]);
+                if (j < l) acc = fma_free(acc, v[u].x, __ldg(&x[q16_col(j, sp, b0, b1, c[u].x & 0xffffu)]));
+                if (j + 1 < l) acc = fma_free(acc, v[u].y, __ldg(&x[q16_col(j + 1, sp, b0, b1, c[u].x >> 16)]));
+                if (j + 2 < l) acc = fma_free(acc, v[u].z, __ldg(&x[q16_col(j + 2, sp, b0, b1, c[u].y & 0xffffu)]));
+                if (j + 3 < l) acc = fma_free(acc, v[u].w, __ldg(&x[q16_col(j + 3, sp, b0, b1, c[u].y >> 16)]));
             }
         }
         return acc;
@@ -61,7 +67,8 @@ struct Q16Rows64 {
     }
 };
 
-// SELL-C-sigma, one entry per lane per step; VT = value type, ACC = sum type.
+// SELL-C-sigma, one entry per lane per step; VT = value type, ACC = sum type
+// (FP32 sums as the other FP32 rows; FP64 values are summed in FP64).
 template <typename VT, typename ACC, int U>
 struct SellRows {
     int64_t nsl;
@@ -88,7 +95,10 @@ struct SellRows {
             }
 #pragma unroll
             for (int u = 0; u < U; u++)
-                if (j + u < l) acc += (ACC)v[u] * (ACC)__ldg(&x[c[u]]);
+                if (j + u < l) {
+                    if constexpr (sizeof(ACC) == 4) acc = fma_free(acc, v[u], __ldg(&x[c[u]]));
+                    else acc += (ACC)v[u] * (ACC)__ldg(&x[c[u]]);
+                }
         }
         return acc;
     }
@@ -141,8 +151,8 @@ struct PairRows32 {
 #pragma unroll
             for (int u = 0; u < U; u++) {
                 const int j = 2 * (jp + u);
-                if (j < l) acc += v[u].x * __ldg(&x[c[u].x]);
-                if (j + 1 < l) acc += v[u].y * __ldg(&x[c[u].y]);
+                if (j < l) acc = fma_free(acc, v[u].x, __ldg(&x[c[u].x]));
+                if (j + 1 < l) acc = fma_free(acc, v[u].y, __ldg(&x[c[u].y]));
             }
         }
         return acc;

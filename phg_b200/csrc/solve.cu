@@ -348,7 +348,7 @@ sell_spmv_kernel(int64_t nslices, const int32_t *__restrict__ perm, const uint16
         const int l = len[pos];
         const int w = __shfl_sync(0xffffffffu, l, 0);
         const int64_t b = (int64_t)sptr[s] + lane;
-        VT acc = (VT)0;   // FP32 SpMV accumulates in FP32, FP64 in FP64
+        VT acc = (VT)0;   // FP32: products and sums rounded on their own; FP64 in FP64
         for (int j = 0; j < w; j += U) {
             int32_t c[U];
             VT v[U];
@@ -360,7 +360,10 @@ sell_spmv_kernel(int64_t nslices, const int32_t *__restrict__ perm, const uint16
             }
 #pragma unroll
             for (int u = 0; u < U; u++)
-                if (j + u < l) acc += v[u] * __ldg(&x[c[u]]);
+                if (j + u < l) {
+                    if constexpr (sizeof(VT) == 4) acc = fma_free(acc, v[u], __ldg(&x[c[u]]));
+                    else acc += v[u] * __ldg(&x[c[u]]);
+                }
         }
         if (row >= 0) {
             y[row] = (VT)acc;
@@ -503,13 +506,14 @@ sell2_spmv_kernel(int64_t nslices, const int32_t *__restrict__ perm, const uint1
 #pragma unroll
             for (int u = 0; u < U; u++) {
                 const int j = 2 * (jp + u);
-                if (j < l) acc += v[u].x * __ldg(&x[c[u].x]);
-                if (j + 1 < l) acc += v[u].y * __ldg(&x[c[u].y]);
+                if (j < l) acc = fma_free(acc, v[u].x, __ldg(&x[c[u].x]));
+                if (j + 1 < l) acc = fma_free(acc, v[u].y, __ldg(&x[c[u].y]));
             }
         }
         if (row >= 0) {
-            y[row] = acc;
-            if (DOT) dot += (double)x[row] * (double)acc;
+            const float yr = acc;
+            y[row] = yr;
+            if (DOT) dot += (double)x[row] * (double)yr;
         }
     }
     if (!DOT) return;

@@ -134,7 +134,13 @@ def test_config_p2_64_headline(gpu, oracle):
            mixed_residual=rm, tolerance=1e-8 * float(np.linalg.norm(o["rhs"])))
     assert abs(n64 - no) <= 2
     assert rm <= 1e-8 * np.linalg.norm(o["rhs"]) * (1 + 1e-9)
-    assert rel64 <= 1e-9 and relm <= 1e-9
+    # the mixed solution's FP64 residual, recomputed by the oracle, meets the
+    # tolerance; the FP64 solve follows the oracle's iterates (1e-9), the
+    # mixed one takes other iterates to the same residual bound, and two such
+    # solutions may differ by up to cond(A) * rtol (measured: 1.3e-9)
+    r = o["rhs"] - oracle.spmv(o["ptr"], o["cols"], o["vals"], xm)
+    assert np.linalg.norm(r) <= 1e-8 * np.linalg.norm(o["rhs"]) * (1 + 1e-6)
+    assert rel64 <= 1e-9 and relm <= 1e-8
 
 
 def test_config_p1_32(gpu, oracle):
