@@ -303,7 +303,7 @@ element_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, cons
 // words an element instead of hundreds, and the element matrix goes straight
 // to global memory.
 template <int P>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 6)   // 80 registers: 24 warps an SM (96 without the bound: 20)
 element_lanes_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, const int32_t *__restrict__ e2l,
                      const double *__restrict__ kappa, const double mass, const double *__restrict__ f,
                      const ElemWeights Wt, const double *__restrict__ gk, const double *__restrict__ br,
@@ -312,14 +312,22 @@ element_lanes_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo
     constexpr int N = D::N, QK = D::QK, QR = D::QR, W = 4;
     constexpr int EPW = 32 / N;                  // elements per warp
     constexpr int CS = QK * N;                   // component stride of the gk table
-    __shared__ double s_g[W][EPW][QK * 3][N];   // gradient component c at point q of basis b: [q * 3 + c][b]
+    // gradient component c at point q of basis b at [q * 3 + c][b]; each
+    // element's table is padded so that the EPW elements of a warp start in
+    // different banks (a lane reads its element's entry while the other
+    // elements' lanes read theirs: unpadded, elements 0 and 2 of a P2 warp
+    // shared banks and every read took two wavefronts)
+    constexpr int GW = QK * 3 * N;                      // doubles of one element's table
+    constexpr int WANT = (32 / EPW) & ~1;               // bank offset (words) between elements
+    constexpr int GPAD = (((WANT - 2 * GW) % 32 + 32) % 32) / 2;
+    __shared__ double s_g[W][EPW][GW + GPAD];
     __shared__ double s_f[W][EPW][N];
     __shared__ double s_fq[W][EPW][QR];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int sub = lane / N, b = lane - sub * N;
     const bool lane_ok = sub < EPW;
     const int sl = lane_ok ? sub : 0;
-    double(*G)[N] = s_g[w][sl];
+    double(*G)[N] = reinterpret_cast<double(*)[N]>(s_g[w][sl]);
     double *fl = s_f[w][sl], *fq = s_fq[w][sl];
 
     for (int64_t e0 = ((int64_t)blockIdx.x * W + w) * EPW; e0 < nelem; e0 += (int64_t)gridDim.x * W * EPW) {
@@ -630,6 +638,10 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
         // inspected when they are used, so the loads stay in flight.
         auto inc_at = [&](int j) -> int32_t { return j < nwalk ? __ldg(&inc[i0 + j]) : 0; };
         int32_t incA = inc_at(gl), incB = inc_at(G + gl);
+        // the element RHS entries of the first two chunks, loaded now and
+        // summed after the walk (their loads complete behind it)
+        const double reA = gl < nwalk ? __ldg(&Re[incA]) : 0.0;
+        const double reB = G + gl < nwalk ? __ldg(&Re[incB]) : 0.0;
         struct Pf {
             int32_t c;
             double v;
@@ -758,8 +770,16 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
         // element right-hand sides of this row, loaded by the lanes in parallel
         // and added by the group's first lane in element order (zeros skipped)
         double r = 0.0;
+        for (int t = 0; t < G; t++) {
+            const double ba = __shfl_sync(0xffffffffu, reA, t, G);
+            if (gl == 0 && t < nwalk && ba != 0.0) r = rn_add(r, ba);
+        }
+        for (int t = 0; t < G; t++) {
+            const double bb = __shfl_sync(0xffffffffu, reB, t, G);
+            if (gl == 0 && G + t < nwalk && bb != 0.0) r = rn_add(r, bb);
+        }
         const int maxinc = __reduce_max_sync(0xffffffffu, (unsigned)(emit ? i1 - i0 : 0));
-        for (int base = 0; base < maxinc; base += G) {
+        for (int base = 2 * G; base < maxinc; base += G) {
             const int ii = base + gl;
             const double bb = (emit && ii < i1 - i0) ? Re[inc[i0 + ii]] : 0.0;
             for (int t = 0; t < G; t++) {
@@ -799,14 +819,17 @@ value_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32
                   double *__restrict__ bvals, double *__restrict__ rhs, double *__restrict__ diag, int *status,
                   const int32_t *__restrict__ over_list, const int *nover) {
     constexpr int G = C::G, R = C::R, MAXROW = C::MAXROW, W = C::WARPS;
+    constexpr int TPL = C::LONG ? 1 : MAXROW / G;   // first-touch places a lane prefetches
     static_assert(N % 2 == 0, "element rows are staged as 16-byte pairs");
     __shared__ double s_val[W][R][MAXROW];
+    __shared__ uint8_t s_isb[W][R][MAXROW];
     __shared__ __align__(16) double s_ke[W][R][G][N];     // staged element rows of G incidences
     __shared__ __align__(4) uint16_t s_sl[W][R][G][N];    // and their recorded slots
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int grp = lane / G, gl = lane % G;
     const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (grp * G);
     double *sval = s_val[w][grp];
+    uint8_t *sisb = s_isb[w][grp];
 
     const int64_t nwarps = (int64_t)gridDim.x * W;
     const int64_t nrows = C::LONG ? (int64_t)*nover : ndof;
@@ -845,12 +868,25 @@ value_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32
         const int maxwalk = __reduce_max_sync(0xffffffffu, (unsigned)nwalk);
         if (maxwalk == 0) continue;   // warp-uniform
         const int Lw = walk ? L : 0;
+        // the row's first-touch map, fetched now so that it is here when the
+        // values are (first pass: each lane's places gl, gl + G, ...)
+        uint16_t tm[TPL];
+        if (!C::LONG) {
+#pragma unroll
+            for (int k = 0; k < TPL; k++) {
+                const int t = gl + k * G;
+                tm[k] = t < Lw ? __ldg(&tmap[(int64_t)i0 * N + t]) : (uint16_t)0;
+            }
+        }
         for (int t = gl; t < Lw; t += G) sval[t] = 0.0;
         bool changed = false;
+        double r = 0.0;   // the row's RHS: element contributions in element order
         for (int c0 = 0; c0 < maxwalk; c0 += G) {
             // lane gl stages incidence c0 + gl: its element row (N / 2 16-byte
-            // loads) and its N recorded slots, so a group has G rows in flight
+            // loads), its N recorded slots and its element RHS entry, so a
+            // group has G rows in flight
             const int ii = c0 + gl;
+            double reb = 0.0;
             if (ii < nwalk) {
                 const int32_t kk = __ldg(&inc[i0 + ii]);
                 const int32_t e = kk / N, a = kk - e * N;
@@ -862,6 +898,7 @@ value_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32
                 for (int q = 0; q < N / 2; q++) kv[q] = __ldcs(src + q);
 #pragma unroll
                 for (int q = 0; q < N / 2; q++) sv[q] = __ldcs(ssrc + q);
+                reb = __ldg(&Re[kk]);
                 double2 *dst = reinterpret_cast<double2 *>(s_ke[w][grp][gl]);
                 uint32_t *sdst = reinterpret_cast<uint32_t *>(s_sl[w][grp][gl]);
 #pragma unroll
@@ -883,17 +920,25 @@ value_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32
                 }
                 __syncwarp();
             }
+            // the chunk's element RHS entries, zeros skipped
+            for (int t = 0; t < G; t++) {
+                const double bt = __shfl_sync(0xffffffffu, reb, t, G);
+                if (gl == 0 && c0 + t < nwalk && bt != 0.0) r = rn_add(r, bt);
+            }
         }
         if (changed) atomicExch(status, PHGB_DEV_PATTERN_CHANGED);
         // write the entries; a boundary column's value is replaced in s_val by
         // its lift term
         double dg = 0.0;
         bool anyb = false;
-        for (int t = gl; t < Lw; t += G) {
-            const uint16_t tm = tmap[(int64_t)i0 * N + t];
+#pragma unroll
+        for (int k = 0; k < (C::LONG ? MAXROW / G : TPL); k++) {
+            const int t = gl + k * G;
+            if (t >= Lw) break;
+            const uint16_t tmk = C::LONG ? __ldg(&tmap[(int64_t)i0 * N + t]) : tm[C::LONG ? 0 : k];
             const double val = sval[t];
-            if (tm & kTmapBdry) {
-                const int j = tm & ~kTmapBdry;
+            if (tmk & kTmapBdry) {
+                const int j = tmk & ~kTmapBdry;
                 const int32_t c = bcols[b0 + j];
                 bvals[b0 + j] = val;
                 const int mult = inc_ptr[c + 1] - inc_ptr[c];
@@ -901,32 +946,24 @@ value_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32
                 for (int m = 0; m < mult; m++) Dk = rn_add(Dk, 1.0);
                 const double rk = bdry_rhs(g, c, mult);
                 sval[t] = __ddiv_rn(rn_mul(rn_mul(1.0, rk), val), Dk);
+                sisb[t] = 1;
                 anyb = true;
             } else {
-                vals[p0 + tm] = val;
-                if (tm == dk) dg = val;
+                vals[p0 + tmk] = val;
+                if (tmk == dk) dg = val;
+                sisb[t] = 0;
             }
         }
         const bool lift = (__ballot_sync(0xffffffffu, anyb) & gmask) != 0;
 #pragma unroll
         for (int o = G / 2; o > 0; o >>= 1) dg += __shfl_xor_sync(0xffffffffu, dg, o, G);
-        // element right-hand sides in element order, zeros skipped
-        double r = 0.0;
-        for (int base = 0; base < maxwalk; base += G) {
-            const int ii = base + gl;
-            const double bb = (walk && ii < nwalk) ? Re[inc[i0 + ii]] : 0.0;
-            for (int t = 0; t < G; t++) {
-                const double bt = __shfl_sync(0xffffffffu, bb, t, G);
-                if (gl == 0 && base + t < nwalk && bt != 0.0) r = rn_add(r, bt);
-            }
-        }
         __syncwarp();
         if (walk && gl == 0) {
             diag[d] = dg;
             // lift the boundary columns in first-touch order: r -= term
             if (lift)
                 for (int t = 0; t < L; t++)
-                    if (tmap[(int64_t)i0 * N + t] & kTmapBdry) r = rn_sub(r, sval[t]);
+                    if (sisb[t]) r = rn_sub(r, sval[t]);
             rhs[d] = r;
         }
         __syncwarp();

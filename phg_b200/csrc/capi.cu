@@ -374,7 +374,7 @@ int solver_buffers(phgGpuSystem *s) {
     CHECK_RC(s->Ap.ensure(n));
     // grid sums of two or three values over at most kRedMaxBlocks blocks
     CHECK_RC(s->partials.ensure((size_t)red_partials3_doubles(kRedMaxBlocks) + 64));
-    CHECK_RC(s->sums.ensure(2));
+    CHECK_RC(s->sums.ensure(4));
     CHECK_RC(s->st.ensure(1));
     CHECK_RC(s->ticket.ensure(kRedTickets));
     return PHG_GPU_OK;
@@ -757,7 +757,7 @@ int phgGpuCreate(int device, void *stream, phgGpuSystem **out) {
     }
     if (rc == PHG_GPU_OK) {
         cudaError_t e1 = cudaMallocHost((void **)&s->h_st, sizeof(PcgState));
-        cudaError_t e2 = cudaMallocHost((void **)&s->h_sums, 2 * sizeof(double));
+        cudaError_t e2 = cudaMallocHost((void **)&s->h_sums, 4 * sizeof(double));
         cudaError_t e3 = cudaMallocHost((void **)&s->h_status, sizeof(int));
         if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess)
             rc = fail(PHG_GPU_ERR_CUDA, "cudaMallocHost failed");
@@ -1359,7 +1359,7 @@ int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol,
         }
         CK(launch_gear_init(B, s->diag.p, s->ticket.p, s->sums.p, s->stream));
         s->launches += 1;
-        CK(cudaMemcpyAsync(s->h_sums, s->sums.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+        CK(cudaMemcpyAsync(s->h_sums, s->sums.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
         CK(cudaStreamSynchronize(s->stream));
         const double r0 = sqrt(s->h_sums[0]), ru0 = s->h_sums[1];
         if (!isfinite(ru0)) return fail(PHG_GPU_ERR_NAN, "phgGpuSolverPCGMixed: zero or non-finite diagonal");
@@ -1374,6 +1374,8 @@ int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol,
         g.maxr = r0;
         g.delta = 0.1;
         g.residual = r0;
+        g.gamma_cur = ru0;
+        g.rr_cur = s->h_sums[2];
         g.first = 1;
         g.y_reset = 1;
         g.done = !(r0 > tol && nits_total < maxit);
@@ -1385,7 +1387,7 @@ int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol,
         CK(launch_gear_fold(B, s->stream));
         CK(cudaStreamSynchronize(s->stream));
         const GearState &hg = *s->h_gst_mixed;
-        s->launches += 2 * (int64_t)hg.nits + 2 * (int64_t)hg.nupdates + hg.passes + 1;
+        s->launches += 2 * (int64_t)hg.nits + 3 * (int64_t)hg.nupdates + hg.passes + 1;
         nits_total += hg.nits;
         nupd += hg.nupdates;
         if (hg.status == PCG_NONFINITE) return fail(PHG_GPU_ERR_NAN, "mixed PCG: non-finite residual");

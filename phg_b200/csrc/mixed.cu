@@ -7,23 +7,23 @@
 //   beta  = gamma / gamma_prev,  alpha = gamma / (delta - beta gamma / alpha_prev)
 //   p = u + beta p,  s = w + beta s,  y += alpha p,  r -= alpha s,  u = D^-1 r
 // In exact arithmetic it produces the iterates of solver_pcg
-// (solver-phg.c:485-604); its three dot products (gamma, delta and ||r||^2)
-// are summed in the epilogue of the one matrix-vector product of the
-// iteration, so an iteration is two kernels:
-//   K1  w = A u (FP32 values and vectors), then gamma, delta, ||r||^2 in FP64
-//       (one grid sum); the last block decides the step's alpha and beta,
-//       or that a reliable update is due
-//   K2  the vector update above, no reduction
+// (solver-phg.c:485-604).  An iteration is two kernels, each with one grid
+// sum in its epilogue:
+//   K1  w = A u (FP32 values and vectors) and delta = w.u in FP64; the last
+//       block decides the step's alpha and beta from delta and the gamma
+//       K2 left, or that a reliable update is due (on the r.r K2 left)
+//   K2  the vector update above, and the next gamma = r.u and r.r in FP64
+//       from the new r and u while they are in registers
 // A reliable update (the FP32 residual has fallen tenfold since the last one,
 // or the iteration looks converged) runs inside a conditional graph node:
-//   R1  rtrue = b - A (x + y) with the FP64 matrix values (the explicit
-//       residual of the FP64 iterate), r = (float) rtrue, u = D^-1 r,
-//       ||rtrue||^2 -> the stopping test on the FP64 residual (the
-//       reference's rule, get_tol solver-phg.c:104)
+//   R0  x += y (FP64)
+//   R1  rtrue = b - A x with the FP64 matrix values (the explicit residual of
+//       the FP64 iterate), r = (float) rtrue, u = D^-1 r, ||rtrue||^2 -> the
+//       stopping test (the reference's rule, get_tol solver-phg.c:104), and
+//       r.u, r.r for the next step
 //   R2  K1 again on the new u
-// and the next K2 folds y into x (x += y, FP64) before restarting y.  The
-// stopping test thus sees the residual of the iterate it returns, not a
-// recurrence that may have drifted from it.
+// and the next K2 restarts y.  The stopping test thus sees the residual of
+// the iterate it returns, not a recurrence that may have drifted from it.
 // The iterations run in a conditional WHILE loop of `chunk` iterations per
 // pass, so a solve is one graph launch and the host waits once.
 #include "common.cuh"
@@ -87,8 +87,8 @@ __device__ __forceinline__ bool gear_final(GearState *st, double gamma, double d
 }
 
 // ---------------------------------------------------------------------------
-// K1 / R2: w = A u with the three dot products.  Grid-stride over slices on
-// a grid of kGearBlocksPerSM blocks of 256 threads per SM.
+// K1 / R2: w = A u and delta = w.u.  Grid-stride over slices on a grid of
+// kGearBlocksPerSM blocks of 256 threads per SM.
 constexpr int kGearBlocksPerSM = 8;
 
 template <class L, bool AFTER_RU>
@@ -96,28 +96,37 @@ __global__ void __launch_bounds__(kVecThreads, kGearBlocksPerSM)
 gear_spmv_kernel(const L lay, const GearBuffers B, cudaGraphConditionalHandle hif) {
     GearState *st = B.st;
     if (st->done) return;
-    grid_sum3_init();
+    grid_sum_init();
     const int lane = threadIdx.x & 31;
-    const int64_t warp = ((int64_t)blockIdx.x * kVecThreads + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * kVecThreads) >> 5;
-    double v[3] = {0.0, 0.0, 0.0};
-    const int64_t nsl = lay.nslices();
-    for (int64_t s = warp; s < nsl; s += nwarps) {
-        const int64_t pos = s * 32 + lane;
+    const int warp = (int)((blockIdx.x * kVecThreads + threadIdx.x) >> 5);
+    const int nwarps = (int)((gridDim.x * kVecThreads) >> 5);
+    double delta = 0.0, dummy = 0.0;
+    const int nsl = (int)lay.nslices();   // < 2^26 (rows < 2^31)
+    for (int s = warp; s < nsl; s += nwarps) {
+        const int64_t pos = (int64_t)s * 32 + lane;
         const int32_t row = lay.row(pos);
+        // the row's own u, loaded before the row sum so that it arrives
+        // behind it (after it, it would add a memory round trip to every
+        // slice a warp takes)
+        const float uf = row >= 0 ? __ldg(&B.u[row]) : 0.0f;
         const float acc = lay.sum(s, lane, pos, B.u);
         if (row >= 0) {
             B.w[row] = acc;
-            const double ri = (double)B.r[row], ui = (double)B.u[row];
-            v[0] += ri * ui;
-            v[1] += (double)acc * ui;
-            v[2] += ri * ri;
+            delta += (double)acc * (double)uf;
         }
     }
-    if (grid_sum3(v, B.partials, st->ticket)) {
-        const bool ru = gear_final<AFTER_RU>(st, v[0], v[1], v[2]);
+    if (grid_sum2(delta, dummy, B.partials, st->ticket)) {
+        const bool ru = gear_final<AFTER_RU>(st, st->gamma_cur, delta, st->rr_cur);
         if (!AFTER_RU) cudaGraphSetConditional(hif, ru ? 1u : 0u);
     }
+}
+
+// R0: x += y before the explicit residual.
+__global__ void __launch_bounds__(kVecThreads)
+gear_fold_ru_kernel(const GearBuffers B) {
+    if (B.st->done) return;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < B.n; i += (int64_t)gridDim.x * blockDim.x)
+        B.x[i] += (double)B.y[i];
 }
 
 // R1: the reliable update with the FP64 matrix values.
@@ -126,28 +135,38 @@ __global__ void __launch_bounds__(kVecThreads, 6)
 gear_reliable_kernel(const L64 lay, const GearBuffers B) {
     GearState *st = B.st;
     if (st->done) return;
-    grid_sum_init();
+    grid_sum3_init();
     const int lane = threadIdx.x & 31;
-    const int64_t warp = ((int64_t)blockIdx.x * kVecThreads + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * kVecThreads) >> 5;
-    double rr = 0.0, dummy = 0.0;
-    const int64_t nsl = lay.nslices();
-    for (int64_t s = warp; s < nsl; s += nwarps) {
-        const int64_t pos = s * 32 + lane;
+    const int warp = (int)((blockIdx.x * kVecThreads + threadIdx.x) >> 5);
+    const int nwarps = (int)((gridDim.x * kVecThreads) >> 5);
+    double v[3] = {0.0, 0.0, 0.0};   // ||rtrue||^2, r.u, r.r
+    const int nsl = (int)lay.nslices();
+    for (int s = warp; s < nsl; s += nwarps) {
+        const int64_t pos = (int64_t)s * 32 + lane;
         const int32_t row = lay.row(pos);
-        const double acc = lay.sum_xy(s, lane, pos, B.x, B.y);
+        double bi = 0.0;
+        float di = 1.0f;
+        if (row >= 0) {   // loaded before the row sum, as in K1
+            bi = __ldg(&B.b[row]);
+            di = __ldg(&B.D[row]);
+        }
+        const double acc = lay.sum_x(s, lane, pos, B.x);
         if (row >= 0) {
-            const double rt = B.b[row] - acc;
-            const float rf = (float)rt;
+            const double rt = bi - acc;
+            const float rf = (float)rt, uf = rf / di;
             B.r[row] = rf;
-            B.u[row] = rf / B.D[row];
-            rr += rt * rt;
+            B.u[row] = uf;
+            v[0] += rt * rt;
+            v[1] += (double)rf * (double)uf;
+            v[2] += (double)rf * (double)rf;
         }
     }
-    if (grid_sum2(rr, dummy, B.partials, st->ticket)) {
-        const double res = sqrt(rr);
+    if (grid_sum3(v, B.partials, st->ticket)) {
+        const double res = sqrt(v[0]);
         st->residual = res;
         st->maxr = res;
+        st->gamma_cur = v[1];
+        st->rr_cur = v[2];
         st->y_reset = 1;
         st->nupdates += 1;
         st->final_check = 0;
@@ -160,31 +179,24 @@ gear_reliable_kernel(const L64 lay, const GearBuffers B) {
     }
 }
 
-// K2: the vector update, 16-byte vectors of four rows, no reduction.  After
-// a reliable update it first folds y into x (x += y in FP64) and restarts y.
+// K2: the vector update, 16-byte vectors of four rows, with the next
+// gamma = r.u and r.r summed from the new r and u.  After a reliable update
+// (whose R0 folded y into x) it restarts y.
 __global__ void __launch_bounds__(kVecThreads)
 gear_update_kernel(const GearBuffers B) {
-    const GearState *st = B.st;
+    GearState *st = B.st;
     if (st->done) return;
+    grid_sum_init();
     const float a = (float)st->alpha, b = (float)st->beta;
     const bool reset = st->y_reset != 0;
     const int64_t n = B.n;
-    const int nfull = aligned16(B.r, B.u, B.w, B.p, B.s, B.y, B.D, B.x) ? (int)(n / 4) : 0;   // n < 2^31
+    const int nfull = aligned16(B.r, B.u, B.w, B.p, B.s, B.y, B.D) ? (int)(n / 4) : 0;   // n < 2^31
     const int stride = gridDim.x * blockDim.x;
+    double ru = 0.0, rr = 0.0;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nfull; c += stride) {
         const int i = 4 * c;
         VArr<float> u = vload(B.u + i), p = vload(B.p + i), w = vload_ro(B.w + i), s = vload(B.s + i);
-        VArr<float> y = vload(B.y + i);
-        if (reset) {
-            VArr<double> x0 = vload(B.x + i), x1 = vload(B.x + i + 2);
-            x0.v[0] += (double)y.v[0];
-            x0.v[1] += (double)y.v[1];
-            x1.v[0] += (double)y.v[2];
-            x1.v[1] += (double)y.v[3];
-            vstore(B.x + i, x0);
-            vstore(B.x + i + 2, x1);
-            y = VArr<float>{{0.0f, 0.0f, 0.0f, 0.0f}};
-        }
+        VArr<float> y = reset ? VArr<float>{{0.0f, 0.0f, 0.0f, 0.0f}} : vload(B.y + i);
         VArr<float> r = vload(B.r + i);
         const VArr<float> d = vload_ro(B.D + i);
 #pragma unroll
@@ -194,6 +206,8 @@ gear_update_kernel(const GearBuffers B) {
             y.v[q] = y.v[q] + a * p.v[q];
             r.v[q] = r.v[q] - a * s.v[q];
             u.v[q] = r.v[q] / d.v[q];
+            ru += (double)r.v[q] * (double)u.v[q];
+            rr += (double)r.v[q] * (double)r.v[q];
         }
         vstore(B.p + i, p);
         vstore(B.s + i, s);
@@ -206,11 +220,16 @@ gear_update_kernel(const GearBuffers B) {
         const float p = B.u[i] + b * B.p[i], s = B.w[i] + b * B.s[i];
         B.p[i] = p;
         B.s[i] = s;
-        if (reset) B.x[i] += (double)B.y[i];
         B.y[i] = (reset ? 0.0f : B.y[i]) + a * p;
-        const float r = B.r[i] - a * s;
+        const float r = B.r[i] - a * s, u = r / B.D[i];
         B.r[i] = r;
-        B.u[i] = r / B.D[i];
+        B.u[i] = u;
+        ru += (double)r * (double)u;
+        rr += (double)r * (double)r;
+    }
+    if (grid_sum2(ru, rr, B.partials, st->ticket)) {
+        st->gamma_cur = ru;
+        st->rr_cur = rr;
     }
 }
 
@@ -238,8 +257,8 @@ __global__ void pcg_loop_kernel(PcgState *st, cudaGraphConditionalHandle hwhile)
 
 __global__ void __launch_bounds__(kVecThreads)
 gear_init_kernel(const GearBuffers B, const double *__restrict__ D64, unsigned *ticket, double *out) {
-    grid_sum_init();
-    double rr = 0.0, ru = 0.0;
+    grid_sum3_init();
+    double v[3] = {0.0, 0.0, 0.0};
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < B.n; i += (int64_t)gridDim.x * blockDim.x) {
         const double rt = B.rtrue[i];
         const float rf = (float)rt, df = (float)D64[i];
@@ -250,14 +269,20 @@ gear_init_kernel(const GearBuffers B, const double *__restrict__ D64, unsigned *
         B.y[i] = 0.0f;
         B.p[i] = 0.0f;
         B.s[i] = 0.0f;
-        rr += rt * rt;
-        ru += (double)rf * (double)uf;
+        v[0] += rt * rt;
+        v[1] += (double)rf * (double)uf;
+        v[2] += (double)rf * (double)rf;
     }
-    if (grid_sum2(rr, ru, B.partials, ticket)) { out[0] = rr; out[1] = ru; }
+    if (grid_sum3(v, B.partials, ticket)) {
+        out[0] = v[0];
+        out[1] = v[1];
+        out[2] = v[2];
+    }
 }
 
-// The solve is over: x += y (y holds the steps since the last fold).
+// The solve is over: x += y, unless a reliable update (R0) folded y last.
 __global__ void gear_fold_kernel(const GearBuffers B) {
+    if (B.st->y_reset) return;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < B.n; i += (int64_t)gridDim.x * blockDim.x)
         B.x[i] += (double)B.y[i];
 }
@@ -343,6 +368,7 @@ static cudaError_t build_body(const GearBuffers &B, const L32 &l32, const L64 &l
         if (e != cudaSuccess) return e;
         cudaGraphNode_t r2;
         e = capture_into(stream, ifbody, nullptr, [&] {
+            gear_fold_ru_kernel<<<vec_blocks(B.n), kVecThreads, 0, stream>>>(B);
             gear_reliable_kernel<L64><<<rb, kVecThreads, 0, stream>>>(l64, B);
             gear_spmv_kernel<typename L32::Dev, true><<<sb, kVecThreads, 0, stream>>>(l32.dev, B, hif);
         }, &r2);

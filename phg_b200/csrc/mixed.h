@@ -10,6 +10,7 @@ namespace phgb {
 struct GearState {
     double alpha, beta;             // scalars of the step the update kernel takes next
     double gamma_prev, alpha_prev;  // r.u and alpha of the previous step
+    double gamma_cur, rr_cur;       // r.u and r.r of the current FP32 r and u (the update kernel's sums)
     double tol, maxr, delta, residual;
     int nits, maxit, done, status, first, y_reset, final_check, nupdates, passes, max_passes;
     unsigned ticket[kRedTickets];
@@ -45,7 +46,7 @@ constexpr int64_t red_partials3_doubles(int64_t blocks) {
 }
 
 // r = (float) rtrue, u = r / D, D32 = (float) D64, y = p = s = 0, and
-// (||rtrue||^2, r.u) into out[0..1].
+// (||rtrue||^2, r.u, r.r) into out[0..2].
 cudaError_t launch_gear_init(const GearBuffers &B, const double *D64, unsigned *ticket, double *out,
                              cudaStream_t s);
 // Builds the executable graph of a whole solve: a loop (conditional WHILE
@@ -54,7 +55,7 @@ cudaError_t launch_gear_init(const GearBuffers &B, const double *D64, unsigned *
 // state says done.  Graph construction uses `stream` for capture.
 cudaError_t build_gear_graph(const GearBuffers &B, const GearLayouts &L, int chunk, cudaStream_t stream,
                              cudaGraphExec_t *exec, int *kernels_per_iteration);
-// x += y: the correction not yet folded into x.
+// x += y at the end of a solve, unless a reliable update folded y last.
 cudaError_t launch_gear_fold(const GearBuffers &B, cudaStream_t s);
 
 // A graph that repeats `body` (launches on `stream`, captured) in a

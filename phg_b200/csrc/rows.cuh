@@ -54,16 +54,13 @@ struct Q16Rows32 {
     }
 };
 
-// FP64 values of the q16 layout against x + y, x FP64 and y FP32, each
-// column's x_j + y_j rounded to FP64 first (what folding y into x gives).
+// FP64 values of the q16 layout against an FP64 vector.
 struct Q16Rows64 {
     Q16View Q;
     __device__ __forceinline__ int64_t nslices() const { return Q.nslices; }
     __device__ __forceinline__ int32_t row(int64_t pos) const { return Q.perm[pos]; }
-    __device__ __forceinline__ double sum_xy(int64_t s, int lane, int64_t pos, const double *__restrict__ x,
-                                             const float *__restrict__ y) const {
-        return q16_row64_with(Q, s, lane, Q.len[pos], Q.split[pos], Q.base0[pos], Q.base1[pos],
-                              [x, y](int32_t c) { return __ldg(&x[c]) + (double)__ldg(&y[c]); });
+    __device__ __forceinline__ double sum_x(int64_t s, int lane, int64_t pos, const double *__restrict__ x) const {
+        return q16_row64(Q, s, lane, Q.len[pos], Q.split[pos], Q.base0[pos], Q.base1[pos], x);
     }
 };
 
@@ -102,9 +99,8 @@ struct SellRows {
         }
         return acc;
     }
-    // against x + y (FP64 x, FP32 y), x_j + y_j rounded to FP64 first
-    __device__ __forceinline__ double sum_xy(int64_t s, int lane, int64_t pos, const double *__restrict__ x,
-                                             const float *__restrict__ y) const {
+    // against an FP64 vector
+    __device__ __forceinline__ double sum_x(int64_t s, int lane, int64_t pos, const double *__restrict__ x) const {
         const int l = len[pos];
         const int w = __shfl_sync(0xffffffffu, l, 0);
         const int64_t b = (int64_t)sptr[s] + lane;
@@ -120,7 +116,7 @@ struct SellRows {
             }
 #pragma unroll
             for (int u = 0; u < U; u++)
-                if (j + u < l) acc += (double)v[u] * (__ldg(&x[c[u]]) + (double)__ldg(&y[c[u]]));
+                if (j + u < l) acc += (double)v[u] * __ldg(&x[c[u]]);
         }
         return acc;
     }
