@@ -282,14 +282,29 @@ def impl_ours(args):
         s.set_dof_map(p, inp["e2l"], inp["bdry"])
         s.build_linear_system(f=inp["f"])
 
-    def step(inp, x, mixed):
-        assemble(inp)
+    phase_ev = []   # per timed mixed step: events between its phases
+
+    def step(inp, x, mixed, record=False):
+        if record:
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+            ev[0].record(stream)
+            s.set_mesh(inp["verts"], inp["elems"])
+            ev[1].record(stream)
+            s.set_dof_map(p, inp["e2l"], inp["bdry"])
+            ev[2].record(stream)
+            s.build_linear_system(f=inp["f"])
+            ev[3].record(stream)
+            phase_ev.append(ev)
+        else:
+            assemble(inp)
         x.zero_()
         if mixed:
             _, nits, res, nupd = s.solve_pcg_mixed(out=x, rtol=rtol, btol=0.0, atol=0.0)
         else:
             _, nits, res = s.solve_pcg(out=x, rtol=rtol, btol=0.0, atol=0.0)
             nupd = 0
+        if record:
+            ev[4].record(stream)
         return nits, res, nupd
 
     def barrier():
@@ -298,7 +313,7 @@ def impl_ours(args):
     def max_over_ranks(val):
         return replica_max(val, dist, dev)
 
-    def timed(inp, x, k, mixed):
+    def timed(inp, x, k, mixed, record=False):
         barrier()
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -306,7 +321,7 @@ def impl_ours(args):
         with torch.cuda.stream(stream):
             a.record(stream)
             for _ in range(k):
-                out = step(inp, x, mixed)
+                out = step(inp, x, mixed, record)
             b.record(stream)
         torch.cuda.synchronize()
         barrier()
@@ -327,7 +342,7 @@ def impl_ours(args):
             step(d, x_fp64, False)
     clocks = ClockSampler(local)
     clocks.start()
-    ms, (nits, res, nupd), launches = timed(d, x_mixed, args.steps, True)
+    ms, (nits, res, nupd), launches = timed(d, x_mixed, args.steps, True, record=True)
     ms64, (nits64, res64, _), _ = timed(d, x_fp64, args.steps, False)
     clock_info = clocks.stop()
 
@@ -345,21 +360,10 @@ def impl_ours(args):
     u = np.sin(np.pi * nodes[:, 0]) * np.sin(np.pi * nodes[:, 1]) * np.sin(np.pi * nodes[:, 2])
     rel_l2_vs_fp64 = float(np.linalg.norm(xm - x64) / np.linalg.norm(x64))
 
-    # phase breakdown of one mixed step
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
-    with torch.cuda.stream(stream):
-        ev[0].record(stream)
-        s.set_mesh(d["verts"], d["elems"])
-        ev[1].record(stream)
-        s.set_dof_map(p, d["e2l"], d["bdry"])
-        ev[2].record(stream)
-        s.build_linear_system(f=d["f"])
-        ev[3].record(stream)
-        x_mixed.zero_()
-        s.solve_pcg_mixed(out=x_mixed, rtol=rtol, btol=0.0, atol=0.0)
-        ev[4].record(stream)
-    torch.cuda.synchronize()
-    phases = [ev[i].elapsed_time(ev[i + 1]) for i in range(4)]
+    # phase breakdown: the mean over the timed mixed steps (events between
+    # the phases of each step; the phases add up to the step but for the
+    # host's gaps between calls)
+    phases = [float(np.mean([e[i].elapsed_time(e[i + 1]) for e in phase_ev])) for i in range(4)]
     # a rebuild on the same mesh and DOF map (new coefficient values): the
     # build after the one that recorded the pattern adds the contributions at
     # their recorded places; timed over 5 builds with kappa = 1 + 0.5 (elem % 3)

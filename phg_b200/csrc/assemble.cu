@@ -793,8 +793,10 @@ row_walk_kernel(int64_t ndof, const int32_t *__restrict__ inc_ptr, const int32_t
             cnt_bdry[d] = nb;
             diag[d] = dg;
             // lift the boundary columns in first-touch order: r -= term
-            for (int t = 0; t < L; t++)
-                if (scol[t] >= 0) r = rn_sub(r, sval[t]);
+            // (rows without boundary columns, most of them, skip the scan)
+            if (nb > 0)
+                for (int t = 0; t < L; t++)
+                    if (scol[t] >= 0) r = rn_sub(r, sval[t]);
             rhs[d] = r;
         }
         __syncwarp();
