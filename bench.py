@@ -28,6 +28,7 @@ the reference's own CPU build (oracle/_ref/phg_dump_omp, all host threads)
 on the same workload.
 """
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -315,6 +316,8 @@ def impl_ours(args):
 
     def timed(inp, x, k, mixed, record=False):
         barrier()
+        gc.collect()
+        gc.disable()   # no collector pause inside the timed region
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         l0 = s.launch_count()
@@ -324,6 +327,7 @@ def impl_ours(args):
                 out = step(inp, x, mixed, record)
             b.record(stream)
         torch.cuda.synchronize()
+        gc.enable()
         barrier()
         return max_over_ranks(a.elapsed_time(b) / k), out, s.launch_count() - l0
 

@@ -151,6 +151,10 @@ struct phgGpuSystem_ {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    // solver graphs without conditional nodes, relaunched by the host per
+    // chunk ($PHG_GPU_PLAIN_GRAPHS=1 at creation): profilers do not see the
+    // kernels inside conditional nodes
+    bool plain_graphs = false;
 
     // mesh
     int64_t nvert = 0, nelem = 0;
@@ -522,8 +526,8 @@ int ensure_q16(phgGpuSystem *s) {
         const int64_t extra = grow(e, s->q16_cols.cap, 2) + grow(e, s->q16_v32.cap, 4) + grow(e, s->q16_v64.cap, 8) +
                               grow(npos, s->q16_perm.cap, 16);
         size_t free_b = 0, total_b = 0;
-        CK(cudaMemGetInfo(&free_b, &total_b));
-        if (e >= (int64_t)INT32_MAX || extra > (int64_t)(0.9 * (double)free_b)) {
+        if (extra > 0) CK(cudaMemGetInfo(&free_b, &total_b));   // only when the buffers must grow
+        if (e >= (int64_t)INT32_MAX || (extra > 0 && extra > (int64_t)(0.9 * (double)free_b))) {
             s->q16_valid = true;
             s->q16_fits = false;
             return PHG_GPU_OK;
@@ -745,6 +749,10 @@ int phgGpuCreate(int device, void *stream, phgGpuSystem **out) {
     if (device < 0 || device >= ndev) return fail(PHG_GPU_ERR_ARG, "phgGpuCreate: no CUDA device %d", device);
     phgGpuSystem *s = new phgGpuSystem();
     s->device = device;
+    {
+        const char *pg = getenv("PHG_GPU_PLAIN_GRAPHS");
+        s->plain_graphs = pg != nullptr && pg[0] != '\0' && pg[0] != '0';
+    }
     int rc = set_device(s);
     if (rc == PHG_GPU_OK) {
         if (stream != nullptr) {
@@ -1344,7 +1352,7 @@ int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol,
     }
     if (s->graph_mixed == nullptr || !(s->gkey_mixed == key)) {
         if (s->graph_mixed != nullptr) { cudaGraphExecDestroy(s->graph_mixed); s->graph_mixed = nullptr; }
-        CK(build_gear_graph(B, L, kGraphChunk, s->stream, &s->graph_mixed, nullptr));
+        CK(build_gear_graph(B, L, kGraphChunk, s->plain_graphs, s->stream, &s->graph_mixed, nullptr));
         s->gkey_mixed = key;
     }
     // the explicit FP64 residual b - A x is checked at the end; a recurrence
@@ -1382,12 +1390,26 @@ int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol,
         g.max_passes = g.maxit / kGraphChunk + 3;
         *s->h_gst_mixed = g;
         CK(cudaMemcpyAsync(s->gst.p, s->h_gst_mixed, sizeof(GearState), cudaMemcpyHostToDevice, s->stream));
-        if (!g.done) CK(cudaGraphLaunch(s->graph_mixed, s->stream));
+        int plain_passes = 0;
+        bool plain_limit = false;
+        if (!g.done && !s->plain_graphs) CK(cudaGraphLaunch(s->graph_mixed, s->stream));
+        if (!g.done && s->plain_graphs) {
+            for (;;) {
+                if (plain_passes >= g.max_passes) { plain_limit = true; break; }
+                CK(cudaGraphLaunch(s->graph_mixed, s->stream));
+                plain_passes++;
+                CK(cudaMemcpyAsync(s->h_gst_mixed, s->gst.p, sizeof(GearState), cudaMemcpyDeviceToHost, s->stream));
+                CK(cudaStreamSynchronize(s->stream));
+                if (s->h_gst_mixed->done) break;
+            }
+        }
         CK(cudaMemcpyAsync(s->h_gst_mixed, s->gst.p, sizeof(GearState), cudaMemcpyDeviceToHost, s->stream));
         CK(launch_gear_fold(B, s->stream));
         CK(cudaStreamSynchronize(s->stream));
-        const GearState &hg = *s->h_gst_mixed;
-        s->launches += 2 * (int64_t)hg.nits + 3 * (int64_t)hg.nupdates + hg.passes + 1;
+        GearState &hg = *s->h_gst_mixed;
+        if (plain_limit) hg.status = GEAR_PASS_LIMIT;
+        if (s->plain_graphs) s->launches += 5 * (int64_t)kGraphChunk * plain_passes + 1;
+        else s->launches += 2 * (int64_t)hg.nits + 3 * (int64_t)hg.nupdates + hg.passes + 1;
         nits_total += hg.nits;
         nupd += hg.nupdates;
         if (hg.status == PCG_NONFINITE) return fail(PHG_GPU_ERR_NAN, "mixed PCG: non-finite residual");
@@ -1601,13 +1623,27 @@ int pcg_core(phgGpuSystem *s, const double *drhs, double rtol, double btol, doub
             const Ctx *x = (const Ctx *)c;
             for (int i = 0; i < kGraphChunk; i++) launch_pcg_iteration_plan(x->B, x->P, st);
         };
-        CK(build_pcg_loop_graph(s->stream, body, &ctx, s->st.p, &s->graph));
+        CK(build_pcg_loop_graph(s->stream, body, &ctx, s->st.p, s->plain_graphs, &s->graph));
         s->gkey = key;
     }
-    if (!init.done) CK(cudaGraphLaunch(s->graph, s->stream));
+    if (!init.done && !s->plain_graphs) CK(cudaGraphLaunch(s->graph, s->stream));
+    int plain_passes = 0;
+    bool plain_limit = false;
+    if (!init.done && s->plain_graphs) {
+        for (;;) {
+            if (plain_passes >= init.max_passes) { plain_limit = true; break; }
+            CK(cudaGraphLaunch(s->graph, s->stream));
+            plain_passes++;
+            CK(cudaMemcpyAsync(s->h_st, s->st.p, sizeof(PcgState), cudaMemcpyDeviceToHost, s->stream));
+            CK(cudaStreamSynchronize(s->stream));
+            if (s->h_st->done) break;
+        }
+    }
     CK(cudaMemcpyAsync(s->h_st, s->st.p, sizeof(PcgState), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
-    s->launches += 3 * (int64_t)kGraphChunk * s->h_st->passes + s->h_st->passes;
+    if (plain_limit) s->h_st->status = kStatusPassLimit;
+    if (s->plain_graphs) s->launches += 3 * (int64_t)kGraphChunk * plain_passes;
+    else s->launches += 3 * (int64_t)kGraphChunk * s->h_st->passes + s->h_st->passes;
     const int nits = s->h_st->nits;
     if (residual) *residual = s->h_st->residual;
     if (s->h_st->status == kStatusPassLimit)

@@ -95,7 +95,7 @@ template <class L, bool AFTER_RU>
 __global__ void __launch_bounds__(kVecThreads, kGearBlocksPerSM)
 gear_spmv_kernel(const L lay, const GearBuffers B, cudaGraphConditionalHandle hif) {
     GearState *st = B.st;
-    if (st->done) return;
+    if (st->done || (AFTER_RU && !st->ru_due)) return;
     grid_sum_init();
     const int lane = threadIdx.x & 31;
     const int warp = (int)((blockIdx.x * kVecThreads + threadIdx.x) >> 5);
@@ -117,14 +117,17 @@ gear_spmv_kernel(const L lay, const GearBuffers B, cudaGraphConditionalHandle hi
     }
     if (grid_sum2(delta, dummy, B.partials, st->ticket)) {
         const bool ru = gear_final<AFTER_RU>(st, st->gamma_cur, delta, st->rr_cur);
-        if (!AFTER_RU) cudaGraphSetConditional(hif, ru ? 1u : 0u);
+        if (!AFTER_RU) {
+            st->ru_due = ru ? 1 : 0;
+            if (hif != 0) cudaGraphSetConditional(hif, ru ? 1u : 0u);
+        }
     }
 }
 
 // R0: x += y before the explicit residual.
 __global__ void __launch_bounds__(kVecThreads)
 gear_fold_ru_kernel(const GearBuffers B) {
-    if (B.st->done) return;
+    if (B.st->done || !B.st->ru_due) return;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < B.n; i += (int64_t)gridDim.x * blockDim.x)
         B.x[i] += (double)B.y[i];
 }
@@ -134,7 +137,7 @@ template <class L64>
 __global__ void __launch_bounds__(kVecThreads, 6)
 gear_reliable_kernel(const L64 lay, const GearBuffers B) {
     GearState *st = B.st;
-    if (st->done) return;
+    if (st->done || !st->ru_due) return;
     grid_sum3_init();
     const int lane = threadIdx.x & 31;
     const int warp = (int)((blockIdx.x * kVecThreads + threadIdx.x) >> 5);
@@ -179,10 +182,36 @@ gear_reliable_kernel(const L64 lay, const GearBuffers B) {
     }
 }
 
-// K2: the vector update, 16-byte vectors of four rows, with the next
-// gamma = r.u and r.r summed from the new r and u.  After a reliable update
-// (whose R0 folded y into x) it restarts y.
-__global__ void __launch_bounds__(kVecThreads)
+// K2: the vector update, V rows a thread and step (16-byte vectors: 2.5% to
+// 7% faster solves at P2 64^3 than 8-byte ones at 5 blocks an SM), with the
+// next gamma = r.u and r.r summed from the new r and u.  After a reliable
+// update (whose R0 folded y into x) it restarts y.
+template <int V> struct FVec;
+template <> struct FVec<2> { using T = float2; };
+template <> struct FVec<4> { using T = float4; };
+
+template <int V>
+struct FArr {
+    float v[V];
+};
+template <int V> __device__ __forceinline__ FArr<V> fload(const float *p) {
+    FArr<V> a;
+    *reinterpret_cast<typename FVec<V>::T *>(a.v) = *reinterpret_cast<const typename FVec<V>::T *>(p);
+    return a;
+}
+template <int V> __device__ __forceinline__ FArr<V> fload_ro(const float *p) {
+    FArr<V> a;
+    *reinterpret_cast<typename FVec<V>::T *>(a.v) = __ldg(reinterpret_cast<const typename FVec<V>::T *>(p));
+    return a;
+}
+template <int V> __device__ __forceinline__ void fstore(float *p, const FArr<V> &a) {
+    *reinterpret_cast<typename FVec<V>::T *>(p) = *reinterpret_cast<const typename FVec<V>::T *>(a.v);
+}
+
+constexpr int kUpdateV = 4;
+
+template <int V>
+__global__ void __launch_bounds__(kVecThreads, V == 2 ? 5 : 4)
 gear_update_kernel(const GearBuffers B) {
     GearState *st = B.st;
     if (st->done) return;
@@ -190,17 +219,23 @@ gear_update_kernel(const GearBuffers B) {
     const float a = (float)st->alpha, b = (float)st->beta;
     const bool reset = st->y_reset != 0;
     const int64_t n = B.n;
-    const int nfull = aligned16(B.r, B.u, B.w, B.p, B.s, B.y, B.D) ? (int)(n / 4) : 0;   // n < 2^31
+    const int nfull = aligned16(B.r, B.u, B.w, B.p, B.s, B.y, B.D) ? (int)(n / V) : 0;   // n < 2^31
     const int stride = gridDim.x * blockDim.x;
     double ru = 0.0, rr = 0.0;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nfull; c += stride) {
-        const int i = 4 * c;
-        VArr<float> u = vload(B.u + i), p = vload(B.p + i), w = vload_ro(B.w + i), s = vload(B.s + i);
-        VArr<float> y = reset ? VArr<float>{{0.0f, 0.0f, 0.0f, 0.0f}} : vload(B.y + i);
-        VArr<float> r = vload(B.r + i);
-        const VArr<float> d = vload_ro(B.D + i);
+        const int i = V * c;
+        FArr<V> u = fload<V>(B.u + i), p = fload<V>(B.p + i), w = fload_ro<V>(B.w + i), s = fload<V>(B.s + i);
+        FArr<V> y;
+        if (reset) {
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
+            for (int q = 0; q < V; q++) y.v[q] = 0.0f;
+        } else {
+            y = fload<V>(B.y + i);
+        }
+        FArr<V> r = fload<V>(B.r + i);
+        const FArr<V> d = fload_ro<V>(B.D + i);
+#pragma unroll
+        for (int q = 0; q < V; q++) {
             p.v[q] = u.v[q] + b * p.v[q];
             s.v[q] = w.v[q] + b * s.v[q];
             y.v[q] = y.v[q] + a * p.v[q];
@@ -209,13 +244,13 @@ gear_update_kernel(const GearBuffers B) {
             ru += (double)r.v[q] * (double)u.v[q];
             rr += (double)r.v[q] * (double)r.v[q];
         }
-        vstore(B.p + i, p);
-        vstore(B.s + i, s);
-        vstore(B.y + i, y);
-        vstore(B.r + i, r);
-        vstore(B.u + i, u);
+        fstore<V>(B.p + i, p);
+        fstore<V>(B.s + i, s);
+        fstore<V>(B.y + i, y);
+        fstore<V>(B.r + i, r);
+        fstore<V>(B.u + i, u);
     }
-    for (int64_t i = (int64_t)nfull * 4 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+    for (int64_t i = (int64_t)nfull * V + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         const float p = B.u[i] + b * B.p[i], s = B.w[i] + b * B.s[i];
         B.p[i] = p;
@@ -291,8 +326,9 @@ __global__ void gear_fold_kernel(const GearBuffers B) {
 // Host side.
 
 static int update_blocks(int64_t n) {
-    int64_t b = ceil_div(ceil_div(n, 4), kVecThreads);
-    if (b > 148 * 4) b = 148 * 4;
+    constexpr int per_sm = kUpdateV == 2 ? 5 : 4;
+    int64_t b = ceil_div(ceil_div(n, kUpdateV), kVecThreads);
+    if (b > 148 * per_sm) b = 148 * per_sm;
     return b < 1 ? 1 : (int)b;
 }
 
@@ -348,12 +384,28 @@ static cudaError_t add_conditional(cudaGraph_t g, cudaGraphNode_t dep, cudaGraph
 // The iteration's kernels for FP32 layout L32 and FP64 layout L64.
 template <class L32, class L64>
 static cudaError_t build_body(const GearBuffers &B, const L32 &l32, const L64 &l64, int chunk, cudaStream_t stream,
-                              cudaGraph_t body, cudaGraphConditionalHandle hwhile) {
+                              cudaGraph_t body, cudaGraphConditionalHandle hwhile, bool plain) {
     int sb = vec_blocks(l32.nslices_host * 32);
     if (sb > 148 * kGearBlocksPerSM) sb = 148 * kGearBlocksPerSM;
     const int rb = sb < 148 * 6 ? sb : 148 * 6;   // the reliable kernel holds 6 blocks per SM
     const int ub = update_blocks(B.n);
     cudaGraphNode_t prev = nullptr;
+    if (plain) {   // every kernel every iteration; R0-R2 return unless K1 asked for them
+        for (int i = 0; i < chunk; i++) {
+            cudaGraphNode_t k2;
+            const cudaGraphConditionalHandle none{};
+            cudaError_t e = capture_into(stream, body, prev, [&] {
+                gear_spmv_kernel<typename L32::Dev, false><<<sb, kVecThreads, 0, stream>>>(l32.dev, B, none);
+                gear_fold_ru_kernel<<<vec_blocks(B.n), kVecThreads, 0, stream>>>(B);
+                gear_reliable_kernel<L64><<<rb, kVecThreads, 0, stream>>>(l64, B);
+                gear_spmv_kernel<typename L32::Dev, true><<<sb, kVecThreads, 0, stream>>>(l32.dev, B, none);
+                gear_update_kernel<kUpdateV><<<ub, kVecThreads, 0, stream>>>(B);
+            }, &k2);
+            if (e != cudaSuccess) return e;
+            prev = k2;
+        }
+        return cudaSuccess;
+    }
     for (int i = 0; i < chunk; i++) {
         cudaGraphConditionalHandle hif;
         cudaError_t e = cudaGraphConditionalHandleCreate(&hif, body, 0, 0);
@@ -374,7 +426,7 @@ static cudaError_t build_body(const GearBuffers &B, const L32 &l32, const L64 &l
         }, &r2);
         if (e != cudaSuccess) return e;
         e = capture_into(stream, body, ifn, [&] {
-            gear_update_kernel<<<ub, kVecThreads, 0, stream>>>(B);
+            gear_update_kernel<kUpdateV><<<ub, kVecThreads, 0, stream>>>(B);
         }, &k2);
         if (e != cudaSuccess) return e;
         prev = k2;
@@ -391,39 +443,41 @@ struct HostLayout {
     int64_t nslices_host;
 };
 
-cudaError_t build_gear_graph(const GearBuffers &B, const GearLayouts &L, int chunk, cudaStream_t stream,
+cudaError_t build_gear_graph(const GearBuffers &B, const GearLayouts &L, int chunk, bool plain, cudaStream_t stream,
                              cudaGraphExec_t *exec, int *kernels_per_iteration) {
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaGraphCreate(&g, 0);
     if (e != cudaSuccess) return e;
-    cudaGraphConditionalHandle hw;
-    cudaGraphNode_t wnode;
-    cudaGraph_t body = nullptr;
-    e = cudaGraphConditionalHandleCreate(&hw, g, 1, cudaGraphCondAssignDefault);
-    if (e == cudaSuccess) e = add_conditional(g, nullptr, hw, cudaGraphCondTypeWhile, &wnode, &body);
+    cudaGraphConditionalHandle hw{};
+    cudaGraph_t body = g;
+    if (!plain) {
+        cudaGraphNode_t wnode;
+        e = cudaGraphConditionalHandleCreate(&hw, g, 1, cudaGraphCondAssignDefault);
+        if (e == cudaSuccess) e = add_conditional(g, nullptr, hw, cudaGraphCondTypeWhile, &wnode, &body);
+    }
     if (e == cudaSuccess) {
         const int64_t nsl = L.S.nslices;
         const SellRows<double, double, 4> sell64{nsl, L.S.perm, L.S.len, L.S.sptr, L.S.cols, L.S.vals};
         if (L.kind == 2) {
             const Q16Rows64 q64{L.Q};
             if (L.unroll == 2)
-                e = build_body(B, HostLayout<Q16Rows32<2>>{{L.Q}, L.Q.nslices}, q64, chunk, stream, body, hw);
+                e = build_body(B, HostLayout<Q16Rows32<2>>{{L.Q}, L.Q.nslices}, q64, chunk, stream, body, hw, plain);
             else
-                e = build_body(B, HostLayout<Q16Rows32<1>>{{L.Q}, L.Q.nslices}, q64, chunk, stream, body, hw);
+                e = build_body(B, HostLayout<Q16Rows32<1>>{{L.Q}, L.Q.nslices}, q64, chunk, stream, body, hw, plain);
         } else if (L.kind == 1) {
             switch (L.unroll) {
-            case 2: e = build_body(B, HostLayout<PairRows32<2>>{{nsl, L.S2}, nsl}, sell64, chunk, stream, body, hw); break;
-            case 8: e = build_body(B, HostLayout<PairRows32<8>>{{nsl, L.S2}, nsl}, sell64, chunk, stream, body, hw); break;
-            default: e = build_body(B, HostLayout<PairRows32<4>>{{nsl, L.S2}, nsl}, sell64, chunk, stream, body, hw); break;
+            case 2: e = build_body(B, HostLayout<PairRows32<2>>{{nsl, L.S2}, nsl}, sell64, chunk, stream, body, hw, plain); break;
+            case 8: e = build_body(B, HostLayout<PairRows32<8>>{{nsl, L.S2}, nsl}, sell64, chunk, stream, body, hw, plain); break;
+            default: e = build_body(B, HostLayout<PairRows32<4>>{{nsl, L.S2}, nsl}, sell64, chunk, stream, body, hw, plain); break;
             }
         } else {
             using S32_4 = SellRows<float, float, 4>;
             using S32_8 = SellRows<float, float, 8>;
             using S32_16 = SellRows<float, float, 16>;
             switch (L.unroll) {
-            case 8: e = build_body(B, HostLayout<S32_8>{{nsl, L.S.perm, L.S.len, L.S.sptr, L.S.cols, L.S.vals32}, nsl}, sell64, chunk, stream, body, hw); break;
-            case 16: e = build_body(B, HostLayout<S32_16>{{nsl, L.S.perm, L.S.len, L.S.sptr, L.S.cols, L.S.vals32}, nsl}, sell64, chunk, stream, body, hw); break;
-            default: e = build_body(B, HostLayout<S32_4>{{nsl, L.S.perm, L.S.len, L.S.sptr, L.S.cols, L.S.vals32}, nsl}, sell64, chunk, stream, body, hw); break;
+            case 8: e = build_body(B, HostLayout<S32_8>{{nsl, L.S.perm, L.S.len, L.S.sptr, L.S.cols, L.S.vals32}, nsl}, sell64, chunk, stream, body, hw, plain); break;
+            case 16: e = build_body(B, HostLayout<S32_16>{{nsl, L.S.perm, L.S.len, L.S.sptr, L.S.cols, L.S.vals32}, nsl}, sell64, chunk, stream, body, hw, plain); break;
+            default: e = build_body(B, HostLayout<S32_4>{{nsl, L.S.perm, L.S.len, L.S.sptr, L.S.cols, L.S.vals32}, nsl}, sell64, chunk, stream, body, hw, plain); break;
             }
         }
     }
@@ -434,10 +488,17 @@ cudaError_t build_gear_graph(const GearBuffers &B, const GearLayouts &L, int chu
 }
 
 cudaError_t build_pcg_loop_graph(cudaStream_t stream, void (*body)(void *ctx, cudaStream_t s), void *ctx,
-                                 PcgState *st, cudaGraphExec_t *exec) {
+                                 PcgState *st, bool plain, cudaGraphExec_t *exec) {
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaGraphCreate(&g, 0);
     if (e != cudaSuccess) return e;
+    if (plain) {   // the chunk alone; the host loops
+        cudaGraphNode_t last;
+        e = capture_into(stream, g, nullptr, [&] { body(ctx, stream); }, &last);
+        if (e == cudaSuccess) e = cudaGraphInstantiate(exec, g, 0);
+        cudaGraphDestroy(g);
+        return e;
+    }
     cudaGraphConditionalHandle hw;
     cudaGraphNode_t wnode, last;
     cudaGraph_t wbody = nullptr;

@@ -13,6 +13,7 @@ struct GearState {
     double gamma_cur, rr_cur;       // r.u and r.r of the current FP32 r and u (the update kernel's sums)
     double tol, maxr, delta, residual;
     int nits, maxit, done, status, first, y_reset, final_check, nupdates, passes, max_passes;
+    int ru_due;                     // the last product asked for a reliable update
     unsigned ticket[kRedTickets];
 };
 
@@ -53,7 +54,11 @@ cudaError_t launch_gear_init(const GearBuffers &B, const double *D64, unsigned *
 // node) over `chunk` iterations, each the FP32 product with its dot products,
 // a conditional reliable update, and the vector update; the loop ends when the
 // state says done.  Graph construction uses `stream` for capture.
-cudaError_t build_gear_graph(const GearBuffers &B, const GearLayouts &L, int chunk, cudaStream_t stream,
+// With `plain` the graph is one chunk of iterations without conditional
+// nodes (the reliable-update kernels run every iteration and return at once
+// unless due) and the host relaunches it until the state says done: for
+// profilers that do not see kernels inside conditional graph nodes.
+cudaError_t build_gear_graph(const GearBuffers &B, const GearLayouts &L, int chunk, bool plain, cudaStream_t stream,
                              cudaGraphExec_t *exec, int *kernels_per_iteration);
 // x += y at the end of a solve, unless a reliable update folded y last.
 cudaError_t launch_gear_fold(const GearBuffers &B, cudaStream_t s);
@@ -62,6 +67,6 @@ cudaError_t launch_gear_fold(const GearBuffers &B, cudaStream_t s);
 // conditional WHILE loop until st->done, at most st->max_passes passes (then
 // st->status = kStatusPassLimit): one graph launch runs a whole solve.
 cudaError_t build_pcg_loop_graph(cudaStream_t stream, void (*body)(void *ctx, cudaStream_t s), void *ctx,
-                                 PcgState *st, cudaGraphExec_t *exec);
+                                 PcgState *st, bool plain, cudaGraphExec_t *exec);
 
 }  // namespace phgb

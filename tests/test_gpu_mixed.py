@@ -204,3 +204,23 @@ def test_krylov_solvers_on_each_fp64_layout(gpu, oracle, layout, param):
     s.close()
     for a, b in zip(its["csr"], its[layout]):
         assert abs(a - b) <= max(3, a // 20), its
+
+
+def test_plain_graphs_same_solves(gpu, monkeypatch):
+    """$PHG_GPU_PLAIN_GRAPHS=1 builds the solver graphs without conditional
+    nodes (for profilers) and relaunches them from the host: the same kernels
+    in the same order, so the same iterations and the same bits."""
+    G = load_golden("p2_m6_sine")
+    args = (G["rows_ptr"], G["rows_cols"], G["rows_vals"], G["rhs"])
+    out = []
+    for plain in ("0", "1"):
+        monkeypatch.setenv("PHG_GPU_PLAIN_GRAPHS", plain)
+        s = gpu.Solver(0)
+        s.set_matrix(*args)
+        x64, n64, r64 = s.solve_pcg(rtol=1e-10, btol=0.0, atol=0.0)
+        xm, nm, rm, nu = s.solve_pcg_mixed(rtol=1e-10, btol=0.0, atol=0.0)
+        out.append((x64, n64, r64, xm, nm, rm, nu))
+        s.close()
+    a, b = out
+    assert a[1] == b[1] and a[2] == b[2] and np.array_equal(a[0], b[0])
+    assert a[4] == b[4] and a[5] == b[5] and a[6] == b[6] and np.array_equal(a[3], b[3])
