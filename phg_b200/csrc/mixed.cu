@@ -91,7 +91,10 @@ __device__ __forceinline__ bool gear_final(GearState *st, double gamma, double d
 // kGearBlocksPerSM blocks of 256 threads per SM.
 constexpr int kGearBlocksPerSM = 8;
 
-template <class L, bool AFTER_RU>
+// COND: the graph has conditional nodes and K1 sets the reliable update's
+// condition (a kernel that sets a graph condition is one that profilers do
+// not see, so the plain graphs launch an instance without the call).
+template <class L, bool AFTER_RU, bool COND = true>
 __global__ void __launch_bounds__(kVecThreads, kGearBlocksPerSM)
 gear_spmv_kernel(const L lay, const GearBuffers B, cudaGraphConditionalHandle hif) {
     GearState *st = B.st;
@@ -119,7 +122,7 @@ gear_spmv_kernel(const L lay, const GearBuffers B, cudaGraphConditionalHandle hi
         const bool ru = gear_final<AFTER_RU>(st, st->gamma_cur, delta, st->rr_cur);
         if (!AFTER_RU) {
             st->ru_due = ru ? 1 : 0;
-            if (hif != 0) cudaGraphSetConditional(hif, ru ? 1u : 0u);
+            if constexpr (COND) cudaGraphSetConditional(hif, ru ? 1u : 0u);
         }
     }
 }
@@ -395,10 +398,10 @@ static cudaError_t build_body(const GearBuffers &B, const L32 &l32, const L64 &l
             cudaGraphNode_t k2;
             const cudaGraphConditionalHandle none{};
             cudaError_t e = capture_into(stream, body, prev, [&] {
-                gear_spmv_kernel<typename L32::Dev, false><<<sb, kVecThreads, 0, stream>>>(l32.dev, B, none);
+                gear_spmv_kernel<typename L32::Dev, false, false><<<sb, kVecThreads, 0, stream>>>(l32.dev, B, none);
                 gear_fold_ru_kernel<<<vec_blocks(B.n), kVecThreads, 0, stream>>>(B);
                 gear_reliable_kernel<L64><<<rb, kVecThreads, 0, stream>>>(l64, B);
-                gear_spmv_kernel<typename L32::Dev, true><<<sb, kVecThreads, 0, stream>>>(l32.dev, B, none);
+                gear_spmv_kernel<typename L32::Dev, true, false><<<sb, kVecThreads, 0, stream>>>(l32.dev, B, none);
                 gear_update_kernel<kUpdateV><<<ub, kVecThreads, 0, stream>>>(B);
             }, &k2);
             if (e != cudaSuccess) return e;
