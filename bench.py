@@ -410,7 +410,7 @@ def impl_ours(args):
                 "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "kernel": "FP32 SpMV (%s layout, unroll %d)" % (tune.get("fp32_layout"), tune.get("fp32_unroll", 0)),
                      "achieved": round(ach32, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
-                     "frac": round(ach32 / peak, 4), "traffic": committed_traffic("spmv32_p2_m64"),
+                     "frac": round(ach32 / peak, 4), "traffic": committed_traffic("spmv32_p2_m64") if m == 64 else None,
                      "algorithmic_bytes": int(b32), "launch_ms": round(spmv32_ms, 5),
                      "layout_bytes": int(lb32),
                      "layout_gbs": round(lb32 / (spmv32_ms * 1e-3) / 1e9, 1),
@@ -419,7 +419,7 @@ def impl_ours(args):
                              "layout_bytes (16-bit column offsets), so achieved can exceed the copy peak"},
         "fp64": {"ms": round(ms64, 3), "mixed_over_fp64": round(ms / ms64, 4), "nits": int(nits64),
                  "spmv_ms": round(spmv64_ms, 5), "spmv_gbs": round(ach64, 1),
-                 "spmv_frac": round(ach64 / peak, 4), "traffic": committed_traffic("spmv64_p2_m64"),
+                 "spmv_frac": round(ach64 / peak, 4), "traffic": committed_traffic("spmv64_p2_m64") if m == 64 else None,
                  "layout_bytes": int(lb64)},
         "gpu_launches": int(launches),
         "clocks": clock_info,

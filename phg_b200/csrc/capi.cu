@@ -1408,8 +1408,8 @@ int phgGpuSolverPCGMixed(phgGpuSystem *s, double rtol, double btol, double atol,
         CK(cudaStreamSynchronize(s->stream));
         GearState &hg = *s->h_gst_mixed;
         if (plain_limit) hg.status = GEAR_PASS_LIMIT;
-        if (s->plain_graphs) s->launches += 5 * (int64_t)kGraphChunk * plain_passes + 1;
-        else s->launches += 2 * (int64_t)hg.nits + 3 * (int64_t)hg.nupdates + hg.passes + 1;
+        if (s->plain_graphs) s->launches += 4 * (int64_t)kGraphChunk * plain_passes + 1;
+        else s->launches += 2 * (int64_t)hg.nits + 2 * (int64_t)hg.nupdates + hg.passes + 1;
         nits_total += hg.nits;
         nupd += hg.nupdates;
         if (hg.status == PCG_NONFINITE) return fail(PHG_GPU_ERR_NAN, "mixed PCG: non-finite residual");

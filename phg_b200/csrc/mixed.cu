@@ -10,20 +10,22 @@
 // (solver-phg.c:485-604).  An iteration is two kernels, each with one grid
 // sum in its epilogue:
 //   K1  w = A u (FP32 values and vectors) and delta = w.u in FP64; the last
-//       block decides the step's alpha and beta from delta and the gamma
-//       K2 left, or that a reliable update is due (on the r.r K2 left)
+//       block takes the step's alpha and beta from delta and the gamma the
+//       update left
 //   K2  the vector update above, and the next gamma = r.u and r.r in FP64
-//       from the new r and u while they are in registers
+//       from the new r and u while they are in registers; the last block
+//       tests the FP32 residual and decides whether a reliable update is due
 // A reliable update (the FP32 residual has fallen tenfold since the last one,
-// or the iteration looks converged) runs inside a conditional graph node:
+// or the iteration looks converged) runs inside a conditional graph node
+// after K2, before the next product:
 //   R0  x += y (FP64)
 //   R1  rtrue = b - A x with the FP64 matrix values (the explicit residual of
 //       the FP64 iterate), r = (float) rtrue, u = D^-1 r, ||rtrue||^2 -> the
 //       stopping test (the reference's rule, get_tol solver-phg.c:104), and
 //       r.u, r.r for the next step
-//   R2  K1 again on the new u
-// and the next K2 restarts y.  The stopping test thus sees the residual of
-// the iterate it returns, not a recurrence that may have drifted from it.
+// and the next K1 takes its product on the new u; the K2 after it restarts
+// y.  The stopping test thus sees the residual of the iterate it returns,
+// not a recurrence that may have drifted from it.
 // The iterations run in a conditional WHILE loop of `chunk` iterations per
 // pass, so a solve is one graph launch and the host waits once.
 #include "common.cuh"
@@ -44,37 +46,24 @@ __device__ __forceinline__ void gear_breakdown(GearState *st) {
     st->nits += 1;   // the reference counts the step it breaks down in (solver-phg.c:537)
 }
 
-// gamma = r.u, delta = w.u, rr = r.r of the current vectors.  AFTER_RU: the
-// product that follows a reliable update (the stopping test was just done on
-// the FP64 residual).  Returns whether a reliable update is due.
-template <bool AFTER_RU>
-__device__ __forceinline__ bool gear_final(GearState *st, double gamma, double delta, double rr) {
-    const double res = sqrt(rr);
-    if (!(isfinite(res) && isfinite(gamma) && isfinite(delta))) {
+// The step from gamma = r.u (the update kernel's, or the reliable update's)
+// and delta = w.u.
+__device__ __forceinline__ void gear_step(GearState *st, double gamma, double delta) {
+    if (!(isfinite(gamma) && isfinite(delta))) {
         st->done = 1;
         st->status = PCG_NONFINITE;
-        st->residual = res;
-        return false;
-    }
-    if (!AFTER_RU) {
-        st->y_reset = 0;   // the previous update kernel has consumed it
-        st->residual = res;
-        const bool conv = !(res > st->tol) || st->nits >= st->maxit;
-        if (conv || res < st->delta * st->maxr) {
-            st->final_check = conv ? 1 : 0;
-            return true;
-        }
+        return;
     }
     double alpha, beta;
     if (st->first) {
-        if (delta == 0.0) { gear_breakdown(st); return false; }
+        if (delta == 0.0) { gear_breakdown(st); return; }
         beta = 0.0;
         alpha = gamma / delta;
     } else {
-        if (st->gamma_prev == 0.0) { gear_breakdown(st); return false; }
+        if (st->gamma_prev == 0.0) { gear_breakdown(st); return; }
         beta = gamma / st->gamma_prev;
         const double den = delta - beta * gamma / st->alpha_prev;
-        if (den == 0.0) { gear_breakdown(st); return false; }
+        if (den == 0.0) { gear_breakdown(st); return; }
         alpha = gamma / den;
     }
     st->alpha = alpha;
@@ -83,22 +72,35 @@ __device__ __forceinline__ bool gear_final(GearState *st, double gamma, double d
     st->alpha_prev = alpha;
     st->first = 0;
     st->nits += 1;
-    return false;
+}
+
+// After an update: the FP32 recurrence's residual (rr = r.r) against the
+// tolerance and the last reliable update.  Returns whether a reliable
+// update is due.
+__device__ __forceinline__ bool gear_check(GearState *st, double rr) {
+    const double res = sqrt(rr);
+    st->residual = res;
+    st->y_reset = 0;   // this update restarted y if it had to
+    if (!isfinite(res)) {
+        st->done = 1;
+        st->status = PCG_NONFINITE;
+        return false;
+    }
+    const bool conv = !(res > st->tol) || st->nits >= st->maxit;
+    st->final_check = conv ? 1 : 0;
+    return conv || res < st->delta * st->maxr;
 }
 
 // ---------------------------------------------------------------------------
-// K1 / R2: w = A u and delta = w.u.  Grid-stride over slices on a grid of
+// K1: w = A u and delta = w.u.  Grid-stride over slices on a grid of
 // kGearBlocksPerSM blocks of 256 threads per SM.
 constexpr int kGearBlocksPerSM = 8;
 
-// COND: the graph has conditional nodes and K1 sets the reliable update's
-// condition (a kernel that sets a graph condition is one that profilers do
-// not see, so the plain graphs launch an instance without the call).
-template <class L, bool AFTER_RU, bool COND = true>
+template <class L>
 __global__ void __launch_bounds__(kVecThreads, kGearBlocksPerSM)
-gear_spmv_kernel(const L lay, const GearBuffers B, cudaGraphConditionalHandle hif) {
+gear_spmv_kernel(const L lay, const GearBuffers B) {
     GearState *st = B.st;
-    if (st->done || (AFTER_RU && !st->ru_due)) return;
+    if (st->done) return;
     grid_sum_init();
     const int lane = threadIdx.x & 31;
     const int warp = (int)((blockIdx.x * kVecThreads + threadIdx.x) >> 5);
@@ -118,13 +120,7 @@ gear_spmv_kernel(const L lay, const GearBuffers B, cudaGraphConditionalHandle hi
             delta += (double)acc * (double)uf;
         }
     }
-    if (grid_sum2(delta, dummy, B.partials, st->ticket)) {
-        const bool ru = gear_final<AFTER_RU>(st, st->gamma_cur, delta, st->rr_cur);
-        if (!AFTER_RU) {
-            st->ru_due = ru ? 1 : 0;
-            if constexpr (COND) cudaGraphSetConditional(hif, ru ? 1u : 0u);
-        }
-    }
+    if (grid_sum2(delta, dummy, B.partials, st->ticket)) gear_step(st, st->gamma_cur, delta);
 }
 
 // R0: x += y before the explicit residual.
@@ -213,9 +209,12 @@ template <int V> __device__ __forceinline__ void fstore(float *p, const FArr<V> 
 
 constexpr int kUpdateV = 4;
 
-template <int V>
+// COND: the graph has conditional nodes and K2 sets the reliable update's
+// condition (a kernel that sets a graph condition is one that profilers do
+// not see, so the plain graphs launch an instance without the call).
+template <int V, bool COND = true>
 __global__ void __launch_bounds__(kVecThreads, V == 2 ? 5 : 4)
-gear_update_kernel(const GearBuffers B) {
+gear_update_kernel(const GearBuffers B, cudaGraphConditionalHandle hif) {
     GearState *st = B.st;
     if (st->done) return;
     grid_sum_init();
@@ -227,7 +226,9 @@ gear_update_kernel(const GearBuffers B) {
     double ru = 0.0, rr = 0.0;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nfull; c += stride) {
         const int i = V * c;
-        FArr<V> u = fload<V>(B.u + i), p = fload<V>(B.p + i), w = fload_ro<V>(B.w + i), s = fload<V>(B.s + i);
+        // u = r / D is not read: the stored u is that same correctly rounded
+        // quotient (K2, R1 and the set-up all form it so), recomputed here
+        FArr<V> p = fload<V>(B.p + i), w = fload_ro<V>(B.w + i), s = fload<V>(B.s + i);
         FArr<V> y;
         if (reset) {
 #pragma unroll
@@ -235,11 +236,11 @@ gear_update_kernel(const GearBuffers B) {
         } else {
             y = fload<V>(B.y + i);
         }
-        FArr<V> r = fload<V>(B.r + i);
+        FArr<V> r = fload<V>(B.r + i), u;
         const FArr<V> d = fload_ro<V>(B.D + i);
 #pragma unroll
         for (int q = 0; q < V; q++) {
-            p.v[q] = u.v[q] + b * p.v[q];
+            p.v[q] = r.v[q] / d.v[q] + b * p.v[q];
             s.v[q] = w.v[q] + b * s.v[q];
             y.v[q] = y.v[q] + a * p.v[q];
             r.v[q] = r.v[q] - a * s.v[q];
@@ -255,7 +256,7 @@ gear_update_kernel(const GearBuffers B) {
     }
     for (int64_t i = (int64_t)nfull * V + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const float p = B.u[i] + b * B.p[i], s = B.w[i] + b * B.s[i];
+        const float p = B.r[i] / B.D[i] + b * B.p[i], s = B.w[i] + b * B.s[i];
         B.p[i] = p;
         B.s[i] = s;
         B.y[i] = (reset ? 0.0f : B.y[i]) + a * p;
@@ -268,6 +269,9 @@ gear_update_kernel(const GearBuffers B) {
     if (grid_sum2(ru, rr, B.partials, st->ticket)) {
         st->gamma_cur = ru;
         st->rr_cur = rr;
+        const bool due = gear_check(st, rr);
+        st->ru_due = due ? 1 : 0;
+        if constexpr (COND) cudaGraphSetConditional(hif, due ? 1u : 0u);
     }
 }
 
@@ -393,19 +397,18 @@ static cudaError_t build_body(const GearBuffers &B, const L32 &l32, const L64 &l
     const int rb = sb < 148 * 6 ? sb : 148 * 6;   // the reliable kernel holds 6 blocks per SM
     const int ub = update_blocks(B.n);
     cudaGraphNode_t prev = nullptr;
-    if (plain) {   // every kernel every iteration; R0-R2 return unless K1 asked for them
+    if (plain) {   // every kernel every iteration; R0 and R1 return unless K2 asked for them
         for (int i = 0; i < chunk; i++) {
-            cudaGraphNode_t k2;
+            cudaGraphNode_t last;
             const cudaGraphConditionalHandle none{};
             cudaError_t e = capture_into(stream, body, prev, [&] {
-                gear_spmv_kernel<typename L32::Dev, false, false><<<sb, kVecThreads, 0, stream>>>(l32.dev, B, none);
+                gear_spmv_kernel<typename L32::Dev><<<sb, kVecThreads, 0, stream>>>(l32.dev, B);
+                gear_update_kernel<kUpdateV, false><<<ub, kVecThreads, 0, stream>>>(B, none);
                 gear_fold_ru_kernel<<<vec_blocks(B.n), kVecThreads, 0, stream>>>(B);
                 gear_reliable_kernel<L64><<<rb, kVecThreads, 0, stream>>>(l64, B);
-                gear_spmv_kernel<typename L32::Dev, true, false><<<sb, kVecThreads, 0, stream>>>(l32.dev, B, none);
-                gear_update_kernel<kUpdateV><<<ub, kVecThreads, 0, stream>>>(B);
-            }, &k2);
+            }, &last);
             if (e != cudaSuccess) return e;
-            prev = k2;
+            prev = last;
         }
         return cudaSuccess;
     }
@@ -413,26 +416,22 @@ static cudaError_t build_body(const GearBuffers &B, const L32 &l32, const L64 &l
         cudaGraphConditionalHandle hif;
         cudaError_t e = cudaGraphConditionalHandleCreate(&hif, body, 0, 0);
         if (e != cudaSuccess) return e;
-        cudaGraphNode_t k1, ifn, k2;
+        cudaGraphNode_t k2, ifn;
         e = capture_into(stream, body, prev, [&] {
-            gear_spmv_kernel<typename L32::Dev, false><<<sb, kVecThreads, 0, stream>>>(l32.dev, B, hif);
-        }, &k1);
+            gear_spmv_kernel<typename L32::Dev><<<sb, kVecThreads, 0, stream>>>(l32.dev, B);
+            gear_update_kernel<kUpdateV><<<ub, kVecThreads, 0, stream>>>(B, hif);
+        }, &k2);
         if (e != cudaSuccess) return e;
         cudaGraph_t ifbody;
-        e = add_conditional(body, k1, hif, cudaGraphCondTypeIf, &ifn, &ifbody);
+        e = add_conditional(body, k2, hif, cudaGraphCondTypeIf, &ifn, &ifbody);
         if (e != cudaSuccess) return e;
-        cudaGraphNode_t r2;
+        cudaGraphNode_t r1;
         e = capture_into(stream, ifbody, nullptr, [&] {
             gear_fold_ru_kernel<<<vec_blocks(B.n), kVecThreads, 0, stream>>>(B);
             gear_reliable_kernel<L64><<<rb, kVecThreads, 0, stream>>>(l64, B);
-            gear_spmv_kernel<typename L32::Dev, true><<<sb, kVecThreads, 0, stream>>>(l32.dev, B, hif);
-        }, &r2);
+        }, &r1);
         if (e != cudaSuccess) return e;
-        e = capture_into(stream, body, ifn, [&] {
-            gear_update_kernel<kUpdateV><<<ub, kVecThreads, 0, stream>>>(B);
-        }, &k2);
-        if (e != cudaSuccess) return e;
-        prev = k2;
+        prev = ifn;
     }
     cudaGraphNode_t lk;
     return capture_into(stream, body, prev, [&] { gear_loop_kernel<<<1, 1, 0, stream>>>(B.st, hwhile); }, &lk);

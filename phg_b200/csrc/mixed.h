@@ -13,7 +13,7 @@ struct GearState {
     double gamma_cur, rr_cur;       // r.u and r.r of the current FP32 r and u (the update kernel's sums)
     double tol, maxr, delta, residual;
     int nits, maxit, done, status, first, y_reset, final_check, nupdates, passes, max_passes;
-    int ru_due;                     // the last product asked for a reliable update
+    int ru_due;                     // the last update asked for a reliable update
     unsigned ticket[kRedTickets];
 };
 
