@@ -312,22 +312,23 @@ element_lanes_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo
     constexpr int N = D::N, QK = D::QK, QR = D::QR, W = 4;
     constexpr int EPW = 32 / N;                  // elements per warp
     constexpr int CS = QK * N;                   // component stride of the gk table
-    // gradient component c at point q of basis b at [q * 3 + c][b]; each
+    // gradient component c at point q of basis b at [b][q * 3 + c]: a basis'
+    // gradients are one row of RW doubles, read with 16-byte loads; each
     // element's table is padded so that the EPW elements of a warp start in
-    // different banks (a lane reads its element's entry while the other
-    // elements' lanes read theirs: unpadded, elements 0 and 2 of a P2 warp
-    // shared banks and every read took two wavefronts)
-    constexpr int GW = QK * 3 * N;                      // doubles of one element's table
-    constexpr int WANT = (32 / EPW) & ~1;               // bank offset (words) between elements
-    constexpr int GPAD = (((WANT - 2 * GW) % 32 + 32) % 32) / 2;
-    __shared__ double s_g[W][EPW][GW + GPAD];
+    // different banks (a lane reads its element's row while the other
+    // elements' lanes read theirs)
+    constexpr int RW = (QK * 3 + 1) & ~1;               // doubles per basis row (even: 16-byte loads)
+    constexpr int GW = RW * N;                          // doubles of one element's table
+    constexpr int WANT = (32 / EPW) & ~3;               // bank offset (words) between elements
+    constexpr int GPAD = ((((WANT - 2 * GW) % 32 + 32) % 32) / 2 + 1) & ~1;   // even: rows stay 16-byte aligned
+    __shared__ __align__(16) double s_g[W][EPW][GW + GPAD];
     __shared__ double s_f[W][EPW][N];
     __shared__ double s_fq[W][EPW][QR];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int sub = lane / N, b = lane - sub * N;
     const bool lane_ok = sub < EPW;
     const int sl = lane_ok ? sub : 0;
-    double(*G)[N] = reinterpret_cast<double(*)[N]>(s_g[w][sl]);
+    double(*G)[RW] = reinterpret_cast<double(*)[RW]>(s_g[w][sl]);
     double *fl = s_f[w][sl], *fq = s_fq[w][sl];
 
     for (int64_t e0 = ((int64_t)blockIdx.x * W + w) * EPW; e0 < nelem; e0 += (int64_t)gridDim.x * W * EPW) {
@@ -372,7 +373,7 @@ element_lanes_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo
 #pragma unroll
             for (int q = 0; q < QK; q++)
 #pragma unroll
-                for (int c = 0; c < 3; c++) G[q * 3 + c][b] = g[q][c];
+                for (int c = 0; c < 3; c++) G[b][q * 3 + c] = g[q][c];
             fl[b] = fv;
         }
         __syncwarp();
@@ -387,11 +388,18 @@ element_lanes_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo
         const double vol = act ? J[16] : 0.0;
         // column b of the element matrix
         for (int a = 0; a < N; a++) {
+            double ga[RW];   // basis a's gradients, RW / 2 16-byte loads
+#pragma unroll
+            for (int k = 0; k < RW; k += 2) {
+                const double2 t2 = *reinterpret_cast<const double2 *>(&G[a][k]);
+                ga[k] = t2.x;
+                ga[k + 1] = t2.y;
+            }
             double d = 0.;
 #pragma unroll
             for (int q = 0; q < QK; q++) {
-                const double d0 = rn_add(0., rn_add(rn_add(rn_mul(g[q][0], G[q * 3][a]), rn_mul(g[q][1], G[q * 3 + 1][a])),
-                                                    rn_mul(g[q][2], G[q * 3 + 2][a])));
+                const double d0 = rn_add(0., rn_add(rn_add(rn_mul(g[q][0], ga[q * 3]), rn_mul(g[q][1], ga[q * 3 + 1])),
+                                                    rn_mul(g[q][2], ga[q * 3 + 2])));
                 const double t = rn_mul(d0, Wt.wk[q]);
                 d = rn_add(d, kappa != nullptr ? rn_mul(t, kap) : t);
             }
