@@ -254,11 +254,13 @@ int phgGpuAdjointGradient(phgGpuSystem *sys, const double *u,
 			  double *grad, double *J, int *nits);
 
 /* Mixed-precision Jacobi-PCG on the assembled system: FP32 matrix values,
- * Krylov vectors and SpMV with FP64-accumulated dot products, inside FP64
- * refinement -- the FP64 solution x and FP64 residual b - A x are updated
- * ("reliable updates") whenever the FP32 residual has fallen tenfold, and the
- * search direction is kept across updates, so the iteration converges like
- * the FP64 one.  The stopping rule is the reference's (get_tol,
+ * Krylov vectors and SpMV (products and sums rounded one by one) with
+ * FP64-accumulated dot products, in the single-reduction (Chronopoulos-Gear)
+ * form of PCG, inside FP64 refinement -- the FP64 solution x is brought up
+ * to date and the explicit FP64 residual b - A x recomputed ("reliable
+ * updates") whenever the FP32 residual has fallen tenfold, and the search
+ * direction is kept across updates, so the iteration converges like the
+ * FP64 one.  The stopping rule is the reference's (get_tol,
  * src/solver-phg.c:104, on the initial residual) applied to the FP64
  * residual; on return *residual is ||b - A x||_2 computed in FP64.  Extends
  * the reference (its FLOAT is fixed at build time, configure.in:627-671).
