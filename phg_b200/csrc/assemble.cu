@@ -1233,6 +1233,7 @@ static cudaError_t value_walk(const WalkArgs &A, cudaStream_t s) {
     value_walk_kernel<N, WalkCfg<N>><<<blocks, W * 32, 0, s>>>(
         A.ndof, A.inc_ptr, A.inc, A.bdry, A.Ke, A.Re, A.g, A.slot, A.tmap, A.dpos, A.ptr, A.bptr, A.bcols, A.vals,
         A.bvals, A.rhs, A.diag, A.status, A.over_list, A.nover);
+    // rows longer than the walk's table (listed by the recording walk)
     value_walk_kernel<N, LongWalkCfg<N>><<<148 * 4, 32, 0, s>>>(
         A.ndof, A.inc_ptr, A.inc, A.bdry, A.Ke, A.Re, A.g, A.slot, A.tmap, A.dpos, A.ptr, A.bptr, A.bcols, A.vals,
         A.bvals, A.rhs, A.diag, A.status, A.over_list, A.nover);

@@ -67,6 +67,7 @@ cudaError_t launch_compact(int N, const WalkArgs &a, cudaStream_t s);
 // (ptr, cols, bptr, bcols as the recording build left them); a changed
 // pattern sets PHGB_DEV_PATTERN_CHANGED.
 cudaError_t launch_value_walk(int p, const WalkArgs &a, cudaStream_t s);
+
 // Longest row the walk assembles (its second pass); longer rows are
 // PHG_GPU_ERR_LIMIT.
 int row_walk_max_row(int p);

@@ -162,6 +162,7 @@ struct phgGpuSystem_ {
     DevBuf<int32_t> elems;
     bool have_mesh = false;
     bool geometry_given = false;           // s->geo holds PHG's geometry (phgGpuSetGeometry)
+    bool geometry_valid = false;           // s->geo holds this mesh's geometry, checked by a build
 
     // DOF layout
     int order = 0, N = 0;
@@ -877,6 +878,7 @@ int phgGpuSetMesh(phgGpuSystem *s, int64_t nvert, const double *verts, int64_t n
     s->pattern_state = 0;
     s->have_mesh = true;
     s->geometry_given = false;
+    s->geometry_valid = false;
     s->have_dofs = false;
     s->assembled = false;
     return PHG_GPU_OK;
@@ -951,9 +953,11 @@ static int element_pass(phgGpuSystem *s, const double *kappa, double mass, const
     ea.kappa = dk; ea.f = df; ea.mass = mass;
     ea.gk = s->gk.p; ea.br = s->br.p; ea.brt = s->brt.p; ea.wk_host = s->wk.data(); ea.wr_host = s->wr.data();
     ea.Ke = s->Ke.p; ea.Re = s->Re.p; ea.geo = s->geo.p; ea.status = s->status.p;
-    ea.geometry_given = s->geometry_given;
+    // the geometry is computed once per mesh (a build that succeeded has
+    // checked its vertex indices and coordinates)
+    ea.geometry_given = s->geometry_given || s->geometry_valid;
     CK(launch_element_kernel(s->order, ea, s->stream));
-    s->launches += s->geometry_given ? 1 : 2;
+    s->launches += ea.geometry_given ? 1 : 2;
     return PHG_GPU_OK;
 }
 
@@ -1000,6 +1004,7 @@ static int build_system(phgGpuSystem *s, const double *kappa, double mass, const
             s->pattern_state = 1;
         } else {
             CHECK_RC(check_status(s, "phgGpuBuildLinearSystem"));
+            s->geometry_valid = true;
             CHECK_RC(refresh_layout_values(s));
             s->mass = mass;
             return PHG_GPU_OK;
@@ -1028,6 +1033,7 @@ static int build_system(phgGpuSystem *s, const double *kappa, double mass, const
     CK(launch_scan(ndof, s->cnt_bdry.p, s->brp.p, s->scan_ws.p, s->stream));
     CK(cudaMemcpyAsync(&tot[1], s->brp.p + ndof, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream));
     CHECK_RC(check_status(s, "phgGpuBuildLinearSystem (rows)"));
+    s->geometry_valid = true;
     if (tot[0] < 0 || tot[1] < 0) return fail(PHG_GPU_ERR_LIMIT, "matrix has more than 2^31 entries");
     s->nnz = tot[0];
     s->bnnz = tot[1];
@@ -1039,6 +1045,7 @@ static int build_system(phgGpuSystem *s, const double *kappa, double mass, const
     wa.bptr = s->brp.p; wa.bcols = s->bci.p; wa.bvals = s->bva.p;
     CK(launch_compact(s->N, wa, s->stream));   // sets no status: the check above covers the build
     s->launches += 1;
+
     s->n = ndof;
     s->assembled = true;
     s->have_bdry_cols = true;
@@ -1061,6 +1068,7 @@ int phgGpuElementMatrices(phgGpuSystem *s, const double *kappa, double mass_coef
     CHECK_RC(set_device(s));
     CHECK_RC(element_pass(s, kappa, mass_coef, f));
     CHECK_RC(check_status(s, "phgGpuElementMatrices"));
+    s->geometry_valid = true;
     const size_t N = (size_t)s->N;
     if (Ke != nullptr) CHECK_RC(copy_out(s, Ke, s->Ke.p, (size_t)s->nelem * N * N));
     if (Re != nullptr) CHECK_RC(copy_out(s, Re, s->Re.p, (size_t)s->nelem * N));

@@ -358,3 +358,25 @@ def test_given_geometry_on_unrefined_mesh(gpu, name):
         b.set_geometry(G["geom"][:-1])
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("name", ["p2_corner_refined", "p3_corner_refined", "p1_corner_refined", "p3_m3_mass"])
+def test_rebuild_on_recorded_pattern_refined(gpu, name):
+    """Builds two and three on one mesh and DOF map (the second records the
+    pattern and its contribution lists, the third gathers over them) give the
+    first build's rows bit for bit, on PHG-refined meshes whose rows reach
+    past the walk's table (P3: 281 entries) and past the gather's staging
+    (high-valence vertices), with the reference's golden rows."""
+    G = load_golden(name)
+    args = (gpu, int(G["order"]), G["verts"], G["elems"], G["e2l"], G["bdry"], G["f"], G["g"],
+            G.get("kappa"), float(G.get("mass", 0.0)), phg_geometry(name, G))
+    s = build(*args)
+    for _ in range(2):
+        s.build_linear_system(kappa=G.get("kappa"), f=G["f"], g=G["g"], mass=float(G.get("mass", 0.0)))
+        ptr, cols, vals = s.get_matrix()
+        assert np.array_equal(ptr, G["rows_ptr"]) and np.array_equal(cols, G["rows_cols"])
+        assert np.array_equal(vals, G["rows_vals"])
+        bptr, bcols, bvals = s.get_bdry_columns()
+        assert np.array_equal(bcols, G["bdry_rows_cols"]) and np.array_equal(bvals, G["bdry_rows_vals"])
+        assert np.array_equal(s.get_rhs(), G["rhs"]) and np.array_equal(s.get_diagonal(), G["diag"])
+    s.close()
