@@ -226,3 +226,18 @@ def test_plain_graphs_same_solves(gpu, monkeypatch):
     a, b = out
     assert a[1] == b[1] and a[2] == b[2] and np.array_equal(a[0], b[0])
     assert a[4] == b[4] and a[5] == b[5] and a[6] == b[6] and np.array_equal(a[3], b[3])
+
+
+def test_mixed_maxit_stops_with_fp64_residual(gpu, oracle):
+    """maxit ends the mixed solve after exactly maxit steps (the reliable
+    update that follows makes the last FP64 residual test), and the residual
+    it reports is the FP64 ||b - A x|| of the iterate it returns."""
+    G = load_golden("p2_m6_sine")
+    s = gpu.Solver(0)
+    s.set_matrix(G["rows_ptr"], G["rows_cols"], G["rows_vals"], G["rhs"])
+    x, nits, res, nupd = s.solve_pcg_mixed(rtol=1e-12, btol=0.0, atol=0.0, maxit=10)
+    assert nits == 10 and nupd >= 1
+    r = G["rhs"] - oracle.spmv(G["rows_ptr"], G["rows_cols"], G["rows_vals"], x)
+    assert abs(res - np.linalg.norm(r)) <= 1e-10 * np.linalg.norm(G["rhs"])
+    assert res > 1e-12 * np.linalg.norm(G["rhs"])
+    s.close()
