@@ -423,6 +423,156 @@ element_lanes_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo
     }
 }
 
+// Element matrices and vectors with N / 2 lanes per element (P2: six
+// elements a warp): lane j owns the columns j and j + N / 2, so that each
+// row of basis gradients it reads from shared memory serves two entries.
+// Every entry takes the operations of element_lanes_kernel in the same order
+// (round-to-nearest, no contraction) but one, so the matrices are the same
+// bits: the dot products' leading "0 +" is left out, since it only turns a
+// -0 into +0, and a -0 term added to the running sum (which starts at +0 and
+// so never is -0) leaves the same sum.
+template <int P>
+__global__ void __launch_bounds__(128, 4)   // 128 registers, no spills (5 blocks: 96 registers, 1% slower)
+element_cols2_kernel(int64_t nelem, int64_t ndof, const double *__restrict__ geo, const int32_t *__restrict__ e2l,
+                     const double *__restrict__ kappa, const double mass, const double *__restrict__ f,
+                     const ElemWeights Wt, const double *__restrict__ gk, const double *__restrict__ br,
+                     const double *__restrict__ brt, double *__restrict__ Ke, double *__restrict__ Re, int *status) {
+    using D = ElemDims<P>;
+    constexpr int N = D::N, QK = D::QK, QR = D::QR, W = 4, H = N / 2;
+    static_assert(N % 2 == 0, "columns are paired");
+    constexpr int EPW = 32 / H;                  // elements per warp
+    constexpr int CS = QK * N;                   // component stride of the gk table
+    constexpr int RW = (QK * 3 + 1) & ~1;        // doubles per basis row (even: 16-byte loads)
+    constexpr int GW = RW * N;
+    constexpr int WANT = (32 / EPW) & ~3;
+    constexpr int GPAD = ((((WANT - 2 * GW) % 32 + 32) % 32) / 2 + 1) & ~1;
+    __shared__ __align__(16) double s_g[W][EPW][GW + GPAD];
+    __shared__ double s_f[W][EPW][N];
+    __shared__ double s_fq[W][EPW][QR];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int sub = lane / H, j = lane - sub * H;
+    const bool lane_ok = sub < EPW;
+    const int sl = lane_ok ? sub : 0;
+    const int b1 = j, b2 = j + H;
+    double(*G)[RW] = reinterpret_cast<double(*)[RW]>(s_g[w][sl]);
+    double *fl = s_f[w][sl], *fq = s_fq[w][sl];
+
+    // gradients of basis b at the stiffness points (as element_lanes_kernel)
+    auto grad = [&](const double *J, bool act, int b, double (&g)[QK][3]) {
+#pragma unroll
+        for (int q = 0; q < QK; q++) {
+            if (P == 1) {
+#pragma unroll
+                for (int c = 0; c < 3; c++) g[q][c] = act ? J[4 * b + c] : 0.0;
+            } else if (b < 4) {
+                const double d = gk[(b * QK + q) * N + b];
+#pragma unroll
+                for (int c = 0; c < 3; c++) g[q][c] = rn_mul(d, act ? J[4 * b + c] : 0.0);
+            } else {
+                const double *Gk = gk + q * N + b;
+                const double g0 = Gk[0], g1 = Gk[CS], g2 = Gk[2 * CS], g3 = Gk[3 * CS];
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    const double j0 = act ? J[c] : 0.0, j1 = act ? J[4 + c] : 0.0;
+                    const double j2 = act ? J[8 + c] : 0.0, j3 = act ? J[12 + c] : 0.0;
+                    g[q][c] = rn_add(rn_add(rn_add(rn_mul(g0, j0), rn_mul(g1, j1)), rn_mul(g2, j2)), rn_mul(g3, j3));
+                }
+            }
+        }
+    };
+
+    for (int64_t e0 = ((int64_t)blockIdx.x * W + w) * EPW; e0 < nelem; e0 += (int64_t)gridDim.x * W * EPW) {
+        const int64_t e = e0 + sub;
+        const bool act = lane_ok && e < nelem;
+        const double *J = geo + (size_t)(act ? e : 0) * kGeo;
+        double kap = 0.0;
+        if (act && kappa != nullptr) {
+            kap = kappa[e];
+            if (j == 0 && !isfinite(kap)) atomicExch(status, PHGB_DEV_NONFINITE);
+        }
+        double g1[QK][3], g2[QK][3];
+        grad(J, act, b1, g1);
+        grad(J, act, b2, g2);
+        double fv1 = 0.0, fv2 = 0.0;
+        if (act && f != nullptr) {
+            const int32_t d1 = e2l[(size_t)e * N + b1], d2 = e2l[(size_t)e * N + b2];
+            if (d1 < 0 || d1 >= ndof) atomicExch(status, PHGB_DEV_BAD_INDEX);
+            else fv1 = f[d1];
+            if (d2 < 0 || d2 >= ndof) atomicExch(status, PHGB_DEV_BAD_INDEX);
+            else fv2 = f[d2];
+            if (!isfinite(fv1) || !isfinite(fv2)) atomicExch(status, PHGB_DEV_NONFINITE);
+        }
+        if (lane_ok) {
+#pragma unroll
+            for (int q = 0; q < QK; q++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    G[b1][q * 3 + c] = g1[q][c];
+                    G[b2][q * 3 + c] = g2[q][c];
+                }
+            fl[b1] = fv1;
+            fl[b2] = fv2;
+        }
+        __syncwarp();
+        // f_h at the RHS points (phgDofEval_: sum over the element's nodes)
+        if (lane_ok)
+            for (int q = j; q < QR; q += H) {
+                double v = 0.0;
+                for (int k = 0; k < N; k++) v = rn_add(v, rn_mul(brt[k * QR + q], fl[k]));
+                fq[q] = v;
+            }
+        __syncwarp();
+        const double vol = act ? J[16] : 0.0;
+        double *Ke_e = Ke + (size_t)(act ? e : 0) * N * N;
+        // columns b1 and b2 of the element matrix
+        for (int a = 0; a < N; a++) {
+            double ga[RW];
+#pragma unroll
+            for (int k = 0; k < RW; k += 2) {
+                const double2 t2 = *reinterpret_cast<const double2 *>(&G[a][k]);
+                ga[k] = t2.x;
+                ga[k + 1] = t2.y;
+            }
+            double d1 = 0., d2 = 0.;
+#pragma unroll
+            for (int q = 0; q < QK; q++) {
+                const double x1 = rn_add(rn_add(rn_mul(g1[q][0], ga[q * 3]), rn_mul(g1[q][1], ga[q * 3 + 1])),
+                                         rn_mul(g1[q][2], ga[q * 3 + 2]));
+                const double x2 = rn_add(rn_add(rn_mul(g2[q][0], ga[q * 3]), rn_mul(g2[q][1], ga[q * 3 + 1])),
+                                         rn_mul(g2[q][2], ga[q * 3 + 2]));
+                const double t1 = rn_mul(x1, Wt.wk[q]), t2 = rn_mul(x2, Wt.wk[q]);
+                d1 = rn_add(d1, kappa != nullptr ? rn_mul(t1, kap) : t1);
+                d2 = rn_add(d2, kappa != nullptr ? rn_mul(t2, kap) : t2);
+            }
+            double v1 = rn_mul(d1, vol), v2 = rn_mul(d2, vol);
+            if (mass != 0.0) {
+                double m1 = 0., m2 = 0.;
+                for (int q = 0; q < QR; q++) {
+                    const double ba = br[q * N + a];
+                    m1 = rn_add(m1, rn_mul(rn_mul(br[q * N + b1], ba), Wt.wr[q]));
+                    m2 = rn_add(m2, rn_mul(rn_mul(br[q * N + b2], ba), Wt.wr[q]));
+                }
+                v1 = rn_add(v1, rn_mul(mass, rn_mul(m1, vol)));
+                v2 = rn_add(v2, rn_mul(mass, rn_mul(m2, vol)));
+            }
+            if (act) {
+                Ke_e[a * N + b1] = v1;
+                Ke_e[a * N + b2] = v2;
+            }
+        }
+        if (act) {
+            double r1 = 0.0, r2 = 0.0;
+            for (int q = 0; q < QR; q++) {
+                r1 = rn_add(r1, rn_mul(rn_mul(br[q * N + b1], Wt.wr[q]), fq[q]));
+                r2 = rn_add(r2, rn_mul(rn_mul(br[q * N + b2], Wt.wr[q]), fq[q]));
+            }
+            Re[(size_t)e * N + b1] = rn_mul(r1, vol);
+            Re[(size_t)e * N + b2] = rn_mul(r2, vol);
+        }
+        __syncwarp();
+    }
+}
+
 // ---------------------------------------------------------------------------
 // DOF -> (element, basis) incidence lists.
 
@@ -1159,10 +1309,15 @@ static void elem_launch(const ElemArgs &A, cudaStream_t s) {
     ElemWeights Wt{};
     for (int q = 0; q < ElemDims<P>::QK; q++) Wt.wk[q] = A.wk_host[q];
     for (int q = 0; q < ElemDims<P>::QR; q++) Wt.wr[q] = A.wr_host[q];
-    if constexpr (P <= 2) {   // a lane per basis function
+    if constexpr (P == 1) {   // a lane per basis function
         constexpr int EPB = 4 * (32 / ElemDims<P>::N);   // elements per block
         const int blocks = grid_for(A.nelem, EPB, 148 * 64);
         element_lanes_kernel<P><<<blocks, 128, 0, s>>>(A.nelem, A.ndof, A.geo, A.e2l, A.kappa, A.mass, A.f, Wt,
+                                                       A.gk, A.br, A.brt, A.Ke, A.Re, A.status);
+    } else if constexpr (P == 2) {   // a lane per two basis functions
+        constexpr int EPB = 4 * (32 / (ElemDims<P>::N / 2));
+        const int blocks = grid_for(A.nelem, EPB, 148 * 64);
+        element_cols2_kernel<P><<<blocks, 128, 0, s>>>(A.nelem, A.ndof, A.geo, A.e2l, A.kappa, A.mass, A.f, Wt,
                                                        A.gk, A.br, A.brt, A.Ke, A.Re, A.status);
     } else {          // P3: a warp per element
         const int blocks = grid_for(A.nelem, W, 148 * 64);
