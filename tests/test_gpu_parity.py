@@ -380,3 +380,37 @@ def test_rebuild_on_recorded_pattern_refined(gpu, name):
         assert np.array_equal(bcols, G["bdry_rows_cols"]) and np.array_equal(bvals, G["bdry_rows_vals"])
         assert np.array_equal(s.get_rhs(), G["rhs"]) and np.array_equal(s.get_diagonal(), G["diag"])
     s.close()
+
+
+@pytest.mark.parametrize("p,k", [(1, 3), (2, 1), (2, 5), (3, 2)])
+def test_ragged_element_counts(gpu, oracle, p, k):
+    """Element counts that leave the element kernels' warps part-filled (P1
+    takes 8 elements a warp, P2 6, P3 one; every Kuhn cube has 6 m^3): the
+    4^3 cube without its last k elements.  The first build, rebuilds on the
+    recorded pattern with new kappas and one with a mass term are bit for bit
+    the oracle's, and the PCG solve matches the oracle's."""
+    v, e = gpu.kuhn_cube(4)
+    e = np.ascontiguousarray(e[:-k])
+    e2l, bdry, nodes = gpu.lagrange_dofs(v, e, p)
+    f = gpu.sine_source(nodes)
+    rng = np.random.default_rng(10 * p + k)
+    cases = [(None, 0.0), (np.exp(rng.standard_normal(len(e))), 0.0),
+             (np.exp(rng.standard_normal(len(e))), 0.0), (None, 2.5)]
+    with gpu.Solver(0) as s:
+        s.set_mesh(v, e)
+        s.set_dof_map(p, e2l, bdry)
+        for i, (kappa, mass) in enumerate(cases):
+            s.build_linear_system(kappa=kappa, f=f, mass=mass)
+            o = oracle.assemble(p, v, e, e2l, bdry, f, kappa=kappa, mass=mass)
+            ptr, cols, vals = s.get_matrix()
+            assert np.array_equal(ptr, o["ptr"]) and np.array_equal(cols, o["cols"]), i
+            assert np.array_equal(vals, o["vals"]), i
+            bp, bc, bv = s.get_bdry_columns()
+            assert np.array_equal(bc, o["bcols"]) and np.array_equal(bv, o["bvals"]), i
+            assert np.array_equal(s.get_rhs(), o["rhs"]) and np.array_equal(s.get_diagonal(), o["diag"]), i
+            if i == 1:
+                x, nits, _ = s.solve_pcg(rtol=1e-10, btol=0.0, atol=0.0)
+                xo, no, _, _ = oracle.pcg(o["ptr"], o["cols"], o["vals"], o["diag"], o["rhs"], rtol=1e-10,
+                                          btol=0.0, atol=0.0)
+                assert abs(nits - no) <= 2
+                assert np.linalg.norm(x - xo) <= solution_tol(1e-10) * np.linalg.norm(xo)
