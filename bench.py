@@ -437,7 +437,7 @@ def impl_ours(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_leg(args, m)
-        # the checker: the FP64 oracle PCG (the reference's recurrence restated
+        # the FP64 oracle PCG (the reference's recurrence restated
         # on the CPU) on this matrix, which the parity tests show is the
         # oracle's own bit for bit; the mixed solution's distance to it
         line["pcg"].update(oracle_check(s, xm))
@@ -468,7 +468,7 @@ def cpu_baseline_leg(args, m):
 
 def oracle_check(s, xm):
     """Relative L2 distance of the mixed solution to the FP64 oracle PCG
-    solution of the same system (test infrastructure, run as the checker)."""
+    solution of the same system (test infrastructure, run as a comparison)."""
     try:
         from oracle import pho
         ptr, cols, vals = s.get_matrix()

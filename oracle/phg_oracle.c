@@ -2,7 +2,7 @@
  * phg_oracle.c -- CPU restatement of the reference (PHG 0.9.7) arithmetic
  * for the P1/P2/P3 element assembly + Jacobi-PCG path.
  *
- * TEST INFRASTRUCTURE ONLY: the checker for tests/, smoke() and bench.py's
+ * TEST INFRASTRUCTURE ONLY: the oracle of tests/, smoke() and bench.py's
  * CPU-baseline leg.  The product never links, loads or calls it.
  *
  * Compiled with -ffp-contract=off: every expression below is evaluated with

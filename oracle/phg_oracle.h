@@ -2,8 +2,8 @@
  * phg_oracle -- CPU restatement of the reference (PHG 0.9.7) arithmetic for
  * the element-assembly + Jacobi-PCG path.
  *
- * TEST INFRASTRUCTURE ONLY.  This library is the checker used by tests/,
- * by __graft_entry__.smoke() and by bench.py's CPU-baseline leg.  The product
+ * TEST INFRASTRUCTURE ONLY.  This library is the oracle that tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline leg compare with.  The product
  * (phg_b200/) never links, loads or calls it.
  *
  * Every routine follows one reference routine operation by operation (same

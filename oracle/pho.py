@@ -1,7 +1,7 @@
 """ctypes binding of the CPU restatement in oracle/phg_oracle.c.
 
-TEST INFRASTRUCTURE ONLY: used by tests/, smoke() and bench.py's
-CPU-baseline leg as the checker; the product never imports it.
+TEST INFRASTRUCTURE ONLY: the oracle that tests/, smoke() and bench.py's
+CPU-baseline leg compare with; the product never imports it.
 """
 import ctypes as C
 import os
